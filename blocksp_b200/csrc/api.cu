@@ -1,0 +1,354 @@
+// api.cu — C ABI glue: handles, matrices, bsmv and vector reductions.
+#include <algorithm>
+#include <cstring>
+#include "reduce.cuh"
+
+namespace bsp {
+
+static thread_local std::string g_last_error;
+void record_error(const std::string& msg) { g_last_error = msg; }
+
+int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha,
+                const void* x, double beta, const void* z, void* y, cudaStream_t s);
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+static int check_device_present() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    record_error("no CUDA device visible: the BlockSp B200 path has no CPU fallback");
+    return BSP_NO_DEVICE;
+  }
+  return BSP_OK;
+}
+
+static int validate_structure(int n_rows, int n_cols, int bs, int64_t nnzb, const int* row_ptr,
+                              const int* col_idx) {
+  if (n_rows < 0 || n_cols < 0 || bs < 1 || bs > 64 || nnzb < 0) {
+    record_error("matrix: bad sizes");
+    return BSP_INVALID;
+  }
+  if (!row_ptr || (nnzb > 0 && !col_idx)) {
+    record_error("matrix: null structure pointer");
+    return BSP_INVALID;
+  }
+  if (row_ptr[0] != 0 || row_ptr[n_rows] != nnzb) {
+    record_error("matrix: row_ptr must start at 0 and end at nnzb");
+    return BSP_INVALID;
+  }
+  if (nnzb > INT32_MAX) {
+    record_error("matrix: more than 2^31-1 blocks");
+    return BSP_INVALID;
+  }
+  std::vector<unsigned char> seen;
+  for (int i = 0; i < n_rows; ++i) {
+    if (row_ptr[i + 1] < row_ptr[i]) {
+      record_error("matrix: row_ptr not monotone");
+      return BSP_INVALID;
+    }
+    for (int t = row_ptr[i]; t < row_ptr[i + 1]; ++t)
+      if (col_idx[t] < 0 || col_idx[t] >= n_cols) {
+        record_error("matrix: column index out of range in row " + std::to_string(i));
+        return BSP_INVALID;
+      }
+    // duplicate columns within a row are not representable in the reference
+    // container (operator() finds the existing entry, containers.hpp:156-157)
+    if (row_ptr[i + 1] - row_ptr[i] > 1) {
+      std::vector<int> c(col_idx + row_ptr[i], col_idx + row_ptr[i + 1]);
+      std::sort(c.begin(), c.end());
+      if (std::adjacent_find(c.begin(), c.end()) != c.end()) {
+        record_error("matrix: duplicate column in row " + std::to_string(i));
+        return BSP_INVALID;
+      }
+    }
+  }
+  return BSP_OK;
+}
+
+}  // namespace bsp
+
+using namespace bsp;
+
+extern "C" {
+
+int bsp_abi_version(void) { return BSP_ABI_VERSION; }
+
+const char* bsp_status_string(int s) {
+  switch (s) {
+    case BSP_OK: return "ok";
+    case BSP_ZERO_PIVOT: return "zero pivot in a diagonal block";
+    case BSP_NOT_SPD: return "block Cholesky met a non-positive pivot";
+    case BSP_BREAKDOWN: return "Krylov breakdown";
+    case BSP_MAXIT: return "maximum iterations reached";
+    case BSP_NAN: return "NaN or Inf in residual";
+    case BSP_TIMEOUT: return "bounded device wait timed out";
+    case BSP_CUDA_ERROR: return "CUDA error";
+    case BSP_INVALID: return "invalid argument";
+    case BSP_NO_DEVICE: return "no CUDA device";
+    case BSP_OUT_OF_MEMORY: return "out of device memory";
+    default: return "unknown status";
+  }
+}
+
+const char* bsp_last_error(bsp_handle_t h) {
+  if (h) {
+    h->last_error = g_last_error;
+    return h->last_error.c_str();
+  }
+  return g_last_error.c_str();
+}
+
+int bsp_device_count(int* count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  if (count) *count = n;
+  return n > 0 ? BSP_OK : BSP_NO_DEVICE;
+}
+
+int bsp_handle_create(int device, void* stream, bsp_handle_t* out) {
+  if (!out) return BSP_INVALID;
+  *out = nullptr;
+  BSP_TRY(check_device_present());
+  BSP_CUDA_TRY(cudaSetDevice(device));
+  auto h = std::make_unique<bsp_handle_s>();
+  h->device = device;
+  cudaDeviceProp prop;
+  BSP_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  h->num_sms = prop.multiProcessorCount;
+  if (stream) {
+    h->stream = (cudaStream_t)stream;
+  } else {
+    BSP_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  BSP_TRY(h->ws.partials.alloc((size_t)kRedSlots * kRedBlocks * 4));
+  BSP_TRY(h->ws.tickets.alloc(kRedSlots));
+  BSP_TRY(h->ws.scalars.alloc(256));
+  BSP_TRY(h->ws.status.alloc(1));
+  BSP_CUDA_TRY(cudaMemset(h->ws.tickets.get(), 0, kRedSlots * sizeof(unsigned)));
+  BSP_CUDA_TRY(cudaMemset(h->ws.scalars.get(), 0, 256 * sizeof(double)));
+  BSP_CUDA_TRY(cudaMemset(h->ws.status.get(), 0, sizeof(DevStatus)));
+  *out = h.release();
+  return BSP_OK;
+}
+
+int bsp_handle_destroy(bsp_handle_t h) {
+  if (!h) return BSP_OK;
+  {
+    DeviceGuard g(h->device);
+    cudaStreamSynchronize(h->stream);
+    h->ws = Workspace{};
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+  }
+  delete h;
+  return BSP_OK;
+}
+
+int bsp_handle_sync(bsp_handle_t h) {
+  if (!h) return BSP_INVALID;
+  DeviceGuard g(h->device);
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+void* bsp_handle_stream(bsp_handle_t h) { return h ? (void*)h->stream : nullptr; }
+
+static int matrix_create_common(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
+                                const int* row_ptr, const int* col_idx, bsp_matrix_t* out,
+                                std::unique_ptr<bsp_matrix_s>& A) {
+  BSP_TRY(validate_structure(n_rows, n_cols, bs, nnzb, row_ptr, col_idx));
+  A = std::make_unique<bsp_matrix_s>();
+  A->h = h;
+  A->n_rows = n_rows;
+  A->n_cols = n_cols;
+  A->bs = bs;
+  A->nnzb = nnzb;
+  A->h_row_ptr.assign(row_ptr, row_ptr + n_rows + 1);
+  A->h_col_idx.assign(col_idx, col_idx + nnzb);
+  BSP_TRY(A->row_ptr.alloc(n_rows + 1));
+  BSP_TRY(A->col_idx.alloc(nnzb > 0 ? nnzb : 1));
+  BSP_TRY(A->vals.alloc(nnzb > 0 ? (size_t)nnzb * bs * bs : 1));
+  BSP_CUDA_TRY(cudaMemcpy(A->row_ptr.get(), row_ptr, (n_rows + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  if (nnzb > 0)
+    BSP_CUDA_TRY(cudaMemcpy(A->col_idx.get(), col_idx, nnzb * sizeof(int), cudaMemcpyHostToDevice));
+  (void)out;
+  return BSP_OK;
+}
+
+int bsp_matrix_create(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
+                      const int* row_ptr, const int* col_idx, const double* vals,
+                      bsp_matrix_t* out) {
+  if (!h || !out) return BSP_INVALID;
+  *out = nullptr;
+  DeviceGuard g(h->device);
+  std::unique_ptr<bsp_matrix_s> A;
+  BSP_TRY(matrix_create_common(h, n_rows, n_cols, bs, nnzb, row_ptr, col_idx, out, A));
+  if (nnzb > 0) {
+    if (!vals) return BSP_INVALID;
+    BSP_CUDA_TRY(cudaMemcpy(A->vals.get(), vals, (size_t)nnzb * bs * bs * sizeof(double),
+                            cudaMemcpyHostToDevice));
+  }
+  *out = A.release();
+  return BSP_OK;
+}
+
+int bsp_matrix_create_dev(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
+                          const int* d_row_ptr, const int* d_col_idx, const double* d_vals,
+                          bsp_matrix_t* out) {
+  if (!h || !out) return BSP_INVALID;
+  *out = nullptr;
+  DeviceGuard g(h->device);
+  if (n_rows < 0 || nnzb < 0) return BSP_INVALID;
+  std::vector<int> rp(n_rows + 1), ci(nnzb);
+  BSP_CUDA_TRY(cudaMemcpy(rp.data(), d_row_ptr, (n_rows + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  if (nnzb > 0)
+    BSP_CUDA_TRY(cudaMemcpy(ci.data(), d_col_idx, nnzb * sizeof(int), cudaMemcpyDeviceToHost));
+  std::unique_ptr<bsp_matrix_s> A;
+  BSP_TRY(matrix_create_common(h, n_rows, n_cols, bs, nnzb, rp.data(), ci.data(), out, A));
+  if (nnzb > 0)
+    BSP_CUDA_TRY(cudaMemcpy(A->vals.get(), d_vals, (size_t)nnzb * bs * bs * sizeof(double),
+                            cudaMemcpyDeviceToDevice));
+  *out = A.release();
+  return BSP_OK;
+}
+
+int bsp_matrix_destroy(bsp_matrix_t A) {
+  if (!A) return BSP_OK;
+  {
+    DeviceGuard g(A->h->device);
+    cudaStreamSynchronize(A->h->stream);
+  }
+  delete A;
+  return BSP_OK;
+}
+
+int bsp_matrix_info(bsp_matrix_t A, int* n_rows, int* n_cols, int* bs, int64_t* nnzb) {
+  if (!A) return BSP_INVALID;
+  if (n_rows) *n_rows = A->n_rows;
+  if (n_cols) *n_cols = A->n_cols;
+  if (bs) *bs = A->bs;
+  if (nnzb) *nnzb = A->nnzb;
+  return BSP_OK;
+}
+
+int bsp_matrix_device_ptrs(bsp_matrix_t A, const int** row_ptr, const int** col_idx,
+                           const double** vals) {
+  if (!A) return BSP_INVALID;
+  if (row_ptr) *row_ptr = A->row_ptr.get();
+  if (col_idx) *col_idx = A->col_idx.get();
+  if (vals) *vals = A->vals.get();
+  return BSP_OK;
+}
+
+}  // extern "C"
+
+namespace bsp {
+__global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+__global__ void k_to_bf16(int64_t n, const double* __restrict__ a, __nv_bfloat16* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16_rn((float)a[i]);  // double -> float -> bf16, both round-to-nearest-even
+}
+__global__ void k_axpy(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = fma(a, x[i], y[i]);
+}
+int grid_for(const bsp_handle_s* h, int64_t n, int threads) {
+  int64_t g = ceil_div(n, threads);
+  int64_t cap = (int64_t)h->num_sms * 8;
+  return (int)std::max<int64_t>(1, std::min(g, cap));
+}
+}  // namespace bsp
+
+extern "C" {
+
+int bsp_matrix_make_lowp(bsp_matrix_t A, int dtype) {
+  if (!A) return BSP_INVALID;
+  DeviceGuard g(A->h->device);
+  const int64_t n = A->nnzb * A->bs * A->bs;
+  if (dtype == BSP_F32) {
+    if (A->vals32.get()) return BSP_OK;
+    BSP_TRY(A->vals32.alloc(n > 0 ? n : 1));
+    if (n > 0) k_to_f32<<<grid_for(A->h, n, 256), 256, 0, A->h->stream>>>(n, A->vals.get(), A->vals32.get());
+  } else if (dtype == BSP_BF16) {
+    if (A->vals16.get()) return BSP_OK;
+    BSP_TRY(A->vals16.alloc(n > 0 ? n : 1));
+    if (n > 0) k_to_bf16<<<grid_for(A->h, n, 256), 256, 0, A->h->stream>>>(n, A->vals.get(), A->vals16.get());
+  } else if (dtype != BSP_F64) {
+    return BSP_INVALID;
+  }
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+int bsp_bsmv_dev(bsp_handle_t h, bsp_matrix_t A, int nrhs, int transpose, int dtype,
+                 double alpha, const void* x, double beta, const void* z, void* y) {
+  if (!h || !A || !x || !y) return BSP_INVALID;
+  if (beta != 0.0 && !z) return BSP_INVALID;
+  DeviceGuard g(h->device);
+  return bsmv_launch(A, nrhs, transpose, dtype, alpha, x, beta, z, y, h->stream);
+}
+
+int bsp_bsmv(bsp_handle_t h, bsp_matrix_t A, int nrhs, int transpose, double alpha,
+             const double* x, double beta, double* y) {
+  if (!h || !A || !x || !y) return BSP_INVALID;
+  DeviceGuard g(h->device);
+  const int64_t nx = (int64_t)(transpose ? A->n_rows : A->n_cols) * A->bs * nrhs;
+  const int64_t ny = (int64_t)(transpose ? A->n_cols : A->n_rows) * A->bs * nrhs;
+  BSP_TRY(h->stage(nx > 0 ? nx : 1, ny > 0 ? ny : 1));
+  double* dx = h->stage_in.get();
+  double* dy = h->stage_out.get();
+  BSP_CUDA_TRY(cudaMemcpyAsync(dx, x, nx * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (beta != 0.0)
+    BSP_CUDA_TRY(cudaMemcpyAsync(dy, y, ny * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  BSP_TRY(bsmv_launch(A, nrhs, transpose, BSP_F64, alpha, dx, beta, dy, dy, h->stream));
+  BSP_CUDA_TRY(cudaMemcpyAsync(y, dy, ny * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+int bsp_dot_dev(bsp_handle_t h, int64_t n, const double* x, const double* y, double* out_dev) {
+  if (!h || n < 0 || !out_dev) return BSP_INVALID;
+  DeviceGuard g(h->device);
+  return launch_reduce<1>(h, 0, n, DotBody{x, y}, StoreFin{out_dev});
+}
+
+int bsp_dot(bsp_handle_t h, int64_t n, const double* x_dev, const double* y_dev, double* out_host) {
+  if (!out_host) return BSP_INVALID;
+  BSP_TRY(bsp_dot_dev(h, n, x_dev, y_dev, h->ws.scalars.get()));
+  BSP_CUDA_TRY(cudaMemcpyAsync(out_host, h->ws.scalars.get(), sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+int bsp_axpy_dev(bsp_handle_t h, int64_t n, double a, const double* x, double* y) {
+  if (!h || n < 0) return BSP_INVALID;
+  DeviceGuard g(h->device);
+  if (n == 0) return BSP_OK;
+  k_axpy<<<grid_for(h, n, 256), 256, 0, h->stream>>>(n, a, x, y);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,223 @@
+/*
+ * blocksp_b200.h — C ABI of the B200-native BlockSp solve path.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (BSP_OK == 0) and never aborts the process.  Compute runs on the GPU only:
+ * there is no CPU fallback, and every call fails with BSP_NO_DEVICE when no
+ * CUDA device is present.
+ *
+ * Conventions shared with the reference library (BlockSp v1.0):
+ *   - A block-sparse matrix is block CSR: n_rows block rows, block size bs,
+ *     row_ptr[n_rows+1], col_idx[nnzb], vals[nnzb*bs*bs].  Each bs x bs block is
+ *     stored row-major, as blitz::TinyMatrix<T,N,N>::data() is
+ *     (blocksp_containers.hpp:52-53, blocksp_dense_multiply.hpp:65).
+ *     Columns inside a row may appear in any order (the reference keeps
+ *     insertion order, blocksp_containers.hpp:156-163); each column at most once.
+ *   - A vector with n elements, block size B and D dimensions is n*B*D
+ *     contiguous values in (element, dim, b) order, which is the memory layout
+ *     of solArray<T,B,D> (blocksp_containers.hpp:581) and of util::tvConcat
+ *     (blocksp_utility.hpp:257-265).
+ *   - "Coupled" bsmv multiplies BlockSp<T,B*D> by solArray<T,B,D>
+ *     (blocksp_multiply.hpp:209-246); "multi-RHS" bsmv multiplies BlockSp<T,B>
+ *     by solArray<T,B,D> dimension by dimension (blocksp_multiply.hpp:170-205).
+ *
+ * Functions whose name ends in _dev take device pointers and run
+ * stream-ordered on the handle's stream; the others take host buffers and
+ * copy them in and out (the drop-in path used by solve(A, b)).
+ */
+#ifndef BLOCKSP_B200_H
+#define BLOCKSP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSP_ABI_VERSION 1
+
+/* ---- status codes (the reference ignores LAPACK info and calls std::exit
+ *      on a singular diagonal, blocksp_preconditioners.hpp:47-51; here every
+ *      failure is returned) ---- */
+enum bsp_status {
+  BSP_OK = 0,
+  BSP_ZERO_PIVOT = 1,    /* singular diagonal block in Diag/SOR/ILU0          */
+  BSP_NOT_SPD = 2,       /* non-positive pivot in the IChol0 block Cholesky    */
+  BSP_BREAKDOWN = 3,     /* Krylov breakdown (p'Ap <= 0 in pCG, H(j+1,j)=0 ...) */
+  BSP_MAXIT = 4,         /* iteration limit reached before the tolerance      */
+  BSP_NAN = 5,           /* NaN or Inf met in a residual                      */
+  BSP_TIMEOUT = 6,       /* a bounded device-side wait gave up                */
+  BSP_CUDA_ERROR = 7,    /* a CUDA runtime call failed                        */
+  BSP_INVALID = 8,       /* bad argument (size, pointer, unsupported shape)   */
+  BSP_NO_DEVICE = 9,     /* no CUDA device visible                            */
+  BSP_OUT_OF_MEMORY = 10
+};
+
+enum bsp_dtype { BSP_F64 = 0, BSP_F32 = 1, BSP_BF16 = 2 };
+
+/* Preconditioner kinds (blocksp_preconditioners.hpp:66-538). */
+enum bsp_precond_kind {
+  BSP_PC_NONE = 0,       /* NoPre, :66-71                                     */
+  BSP_PC_DIAG_LU = 1,    /* Diag<dense::LUFactor>, :75-111                    */
+  BSP_PC_DIAG_CHOL = 2,  /* Diag<dense::CholeskyFactor>, :75-111              */
+  BSP_PC_SOR_LU = 3,     /* SOR<dense::LUFactor> (SOR_pGMRES), :116-240       */
+  BSP_PC_SOR_CHOL = 4,   /* SOR<dense::CholeskyFactor> (SOR_pCG), :116-240    */
+  BSP_PC_ILU0 = 5,       /* ILU0, :246-357                                    */
+  BSP_PC_ICHOL0 = 6,     /* IChol0, :364-538                                  */
+  BSP_PC_LEARNED_LLT = 7,/* learned factor L, applied as L L^T (no reference) */
+  BSP_PC_LEARNED_LU = 8  /* learned factors L,U, applied as (LU) (no reference) */
+};
+
+/* Arithmetic of the inner work (bsmv + preconditioner apply). */
+enum bsp_precision {
+  BSP_PREC_F64 = 0,      /* everything in FP64: the reference's method         */
+  BSP_PREC_F32 = 1,      /* FP32 bsmv/apply inside FP64 iterative refinement   */
+  BSP_PREC_BF16 = 2      /* BF16 storage, FP32 accumulate, inside FP64 IR      */
+};
+
+/* Stopping rule. */
+enum bsp_stop_rule {
+  BSP_STOP_REFERENCE = 0,  /* the reference's own test: pCG compares the
+                              recursive ||r|| with tol*||M^-1 b||
+                              (blocksp_solvers.hpp:61-69); pGMRES compares the
+                              preconditioned least-squares residual with
+                              tol*||M^-1 b|| (blocksp_solvers.hpp:167-232)     */
+  BSP_STOP_TRUE_RESIDUAL = 1 /* FP64 true residual ||b-Ax||/||b|| <= tol       */
+};
+
+typedef struct bsp_handle_s* bsp_handle_t;
+typedef struct bsp_matrix_s* bsp_matrix_t;
+typedef struct bsp_precond_s* bsp_precond_t;
+
+typedef struct {
+  int kind;            /* bsp_precond_kind                                     */
+  double sor_w;        /* SOR damping w (reference default 1.6, solvers.hpp:363) */
+  int sor_nu;          /* sweeps per direction (default 3)                      */
+  int sor_type;        /* <0 backward only, 0 symmetric, >0 forward only        */
+  int precision;       /* bsp_precision of the stored factors                  */
+} bsp_precond_params;
+
+typedef struct {
+  double tol;          /* relative tolerance                                   */
+  int max_iters;       /* maxIters (pCG default 1000, pGMRES 500, structs 5000) */
+  int restart;         /* pGMRES restart length, <0 = never (solvers.hpp:239)   */
+  int k;               /* deflated-restart size k (deflated_restart.hpp:38)     */
+  int print_iters;     /* print "pCG iters N" / "pGMRES iters N"                */
+  int stop_rule;       /* bsp_stop_rule                                         */
+  int precision;       /* bsp_precision of the inner work                       */
+  double inner_tol;    /* mixed precision: relative tolerance of each inner solve */
+  int max_outer;       /* mixed precision: max refinement steps                 */
+} bsp_solve_opts;
+
+typedef struct {
+  int status;          /* bsp_status of the solve                              */
+  int iters;           /* the reference's printed count ("pCG iters N")        */
+  int n_hist;          /* entries written to the residual history              */
+  int n_restarts;      /* pGMRES restarts performed                             */
+  int n_outer;         /* mixed precision: refinement steps taken               */
+  int inner_iters;     /* mixed precision: total inner iterations               */
+  double res0;         /* ||M^-1 b||, the reference's res_mag[0]                */
+  double final_res;    /* last history entry                                    */
+  double true_rel_res; /* FP64 ||b - A x|| / ||b|| computed on the GPU         */
+  double setup_ms;     /* preconditioner build time (device events)           */
+  double solve_ms;     /* solve time (device events)                            */
+} bsp_solve_info;
+
+/* ---------------- handle ---------------- */
+/* One handle per CUDA stream; a handle is not thread-safe (the reference is
+ * single-threaded, blocksp_solvers.hpp has no synchronisation). stream may be
+ * NULL (the handle creates its own non-blocking stream). */
+int bsp_handle_create(int device, void* stream, bsp_handle_t* out);
+int bsp_handle_destroy(bsp_handle_t h);
+int bsp_handle_sync(bsp_handle_t h);
+void* bsp_handle_stream(bsp_handle_t h);
+const char* bsp_status_string(int status);
+const char* bsp_last_error(bsp_handle_t h);
+int bsp_device_count(int* count);
+int bsp_abi_version(void);
+
+/* ---------------- matrix ----------------
+ * Replaces the packing of BlockSp<T,N> = Sp::CSR<TinyMatrix<T,N,N>>
+ * (blocksp_containers.hpp:52-53, 92-496): the caller hands over the CSR arrays
+ * once; the handle keeps the device copy.  vals are FP64; lower-precision
+ * copies are made on demand for mixed precision. */
+int bsp_matrix_create(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
+                      const int* row_ptr, const int* col_idx, const double* vals,
+                      bsp_matrix_t* out);
+/* Same, from arrays already in device memory (copied). */
+int bsp_matrix_create_dev(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
+                          const int* d_row_ptr, const int* d_col_idx, const double* d_vals,
+                          bsp_matrix_t* out);
+int bsp_matrix_destroy(bsp_matrix_t A);
+int bsp_matrix_info(bsp_matrix_t A, int* n_rows, int* n_cols, int* bs, int64_t* nnzb);
+/* Device pointers of the packed matrix (row_ptr, col_idx, FP64 vals). */
+int bsp_matrix_device_ptrs(bsp_matrix_t A, const int** row_ptr, const int** col_idx,
+                           const double** vals);
+/* Build the FP32 or BF16 copy of the values (idempotent). */
+int bsp_matrix_make_lowp(bsp_matrix_t A, int dtype);
+
+/* ---------------- bsmv ----------------
+ * y = alpha * op(A) * x + beta * z   (z may alias y; z == NULL means 0)
+ * nrhs == 1: BlockSp<T,N> x solArray with N = bs (coupled form when the
+ *            solArray has D > 1 and N = B*D; blocksp_multiply.hpp:209-246).
+ * nrhs == D > 1: BlockSp<T,B> x solArray<T,B,D>, the same block applied to
+ *            each dimension (blocksp_multiply.hpp:170-205, 252-285).
+ * transpose != 0: op(A) = A^T (blocksp_multiply.hpp:196-204, 280-284).
+ * The reference's void bsmv(b, A, x) (multiply.hpp:386-390, accumulating)
+ * is alpha = 1, beta = 1, z = y; bsmv(A, x) returning a new array is beta = 0.
+ * dtype selects the stored copy of A (BSP_F64 or, after bsp_matrix_make_lowp,
+ * BSP_F32/BSP_BF16, which take and return FP32 vectors). */
+int bsp_bsmv_dev(bsp_handle_t h, bsp_matrix_t A, int nrhs, int transpose, int dtype,
+                 double alpha, const void* x, double beta, const void* z, void* y);
+/* Host-buffer form (FP64): copies x (and y when beta != 0) in, y out. */
+int bsp_bsmv(bsp_handle_t h, bsp_matrix_t A, int nrhs, int transpose,
+             double alpha, const double* x, double beta, double* y);
+
+/* ---------------- vector reductions (FP64, deterministic) ----------------
+ * dot (blocksp_containers.hpp:974-996), twoNorm (998-1012), axpy (857-864). */
+int bsp_dot_dev(bsp_handle_t h, int64_t n, const double* x, const double* y, double* out_dev);
+int bsp_dot(bsp_handle_t h, int64_t n, const double* x_dev, const double* y_dev, double* out_host);
+int bsp_axpy_dev(bsp_handle_t h, int64_t n, double a, const double* x, double* y);
+
+/* ---------------- preconditioners ----------------
+ * Construction = the reference constructor: makeADInv (preconditioners.hpp:22-63),
+ * ILU0::factor (:274-291), IChol0::factor (:393-429).  A must outlive pc, as
+ * A_Ptr must in the reference (:80, :120). */
+int bsp_precond_create(bsp_handle_t h, bsp_matrix_t A, const bsp_precond_params* params,
+                       bsp_precond_t* out);
+int bsp_precond_destroy(bsp_precond_t pc);
+/* r <- M^{-1} r in place, as operator()(solArray&) (preconditioners.hpp:541-556).
+ * nrhs as for bsmv (1 unless the matrix is BlockSp<T,B> with D dims). */
+int bsp_precond_apply_dev(bsp_handle_t h, bsp_precond_t pc, double* r);
+int bsp_precond_apply(bsp_handle_t h, bsp_precond_t pc, double* r_host);
+/* Copy the factored blocks back (ILU0: LU in A's layout; IChol0: L in the
+ * layout of A.lowTri(); Diag/SOR: inverted diagonal blocks, n*bs*bs). */
+int bsp_precond_export(bsp_precond_t pc, double* vals_host, int64_t capacity);
+int bsp_precond_info(bsp_precond_t pc, int* kind, int* n_levels_lower, int* n_levels_upper,
+                     int64_t* factor_nnzb);
+
+/* ---------------- Krylov solvers ----------------
+ * pCG  (blocksp_solvers.hpp:51-105)  and  pGMRES with Morgan deflated restart
+ * (blocksp_solvers.hpp:156-295, blocksp_deflated_restart.hpp:38-269).
+ * pc may be NULL (NoPre).  x is the output (the reference starts from x = 0).
+ * hist (host, may be NULL) receives up to hist_cap residual magnitudes: the
+ * reference's res_mag sequence.  b, x are device pointers for _dev. */
+int bsp_pcg_dev(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+                const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info);
+int bsp_pgmres_dev(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+                   const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info);
+/* Host-buffer forms: upload b, solve, download x (solve(A,b) of the solver
+ * structs, solvers.hpp:378-381, 422-425, 455-458, 489-492). */
+int bsp_pcg(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+            const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info);
+int bsp_pgmres(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+               const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info);
+/* FP64 true relative residual ||b - A x|| / ||b|| on the device. */
+int bsp_true_residual_dev(bsp_handle_t h, bsp_matrix_t A, const double* b, const double* x,
+                          double* rel_res_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLOCKSP_B200_H */

@@ -1,0 +1,30 @@
+"""Shared fixtures: the ``gpu`` marker, the repo on sys.path, and a GPU handle."""
+import os
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+
+
+@pytest.fixture(scope="session")
+def handle():
+    import blocksp_b200 as bsp
+    h = bsp.Handle(0)
+    yield h
+    h.close()
+
+
+@pytest.fixture(scope="session")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a visible CUDA device")
+    return torch
