@@ -182,6 +182,7 @@ def run_gpu(args, world, rank, local):
         "e2e_bsmv_ms": e2e_ms, "n": n, "bs": bs, "nnzb": nnzb,
         "peak": peak, "peak_kind": peak_kind, "clocks": clocks, "launches": reps,
     }
+    A.close()
     h.close()
     return res
 

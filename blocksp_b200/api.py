@@ -12,7 +12,7 @@ one-call forms (blocksp_solvers.hpp:344-649).  Compute always runs through
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
+import weakref
 
 import numpy as np
 
@@ -39,6 +39,10 @@ class Handle:
         check(self.lib.bsp_handle_create(device, stream, C.byref(h)), "bsp_handle_create")
         self.h = h
         self.device = device
+        self._children = weakref.WeakSet()  # objects that must be released first
+
+    def adopt(self, obj) -> None:
+        self._children.add(obj)
 
     def sync(self) -> None:
         check(self.lib.bsp_handle_sync(self.h), "bsp_handle_sync", self.h)
@@ -49,6 +53,8 @@ class Handle:
 
     def close(self) -> None:
         if getattr(self, "h", None):
+            for child in list(self._children):
+                child.close()
             self.lib.bsp_handle_destroy(self.h)
             self.h = None
 
@@ -88,6 +94,7 @@ class Matrix:
                                     _ptr(row_ptr), _ptr(col_idx), _ptr(vals), C.byref(m)),
               "bsp_matrix_create", self.handle.h)
         self.m = m
+        self.handle.adopt(self)
 
     @classmethod
     def from_system(cls, s, handle: Handle | None = None) -> "Matrix":
@@ -143,3 +150,221 @@ def dot_dev(handle: Handle, x, y) -> float:
     check(handle.lib.bsp_dot(handle.h, int(x.numel()), _ptr(x), _ptr(y), C.byref(out)), "bsp_dot",
           handle.h)
     return out.value
+
+
+# ---------------------------------------------------------------- preconditioners
+
+class Precond:
+    """A preconditioner built on the GPU (preConditioners::* in the reference).
+
+    Calling it on a device tensor applies M^{-1} in place, like the reference's
+    ``operator()(solArray&)`` (blocksp_preconditioners.hpp:541-556).
+    """
+
+    def __init__(self, A: Matrix, kind: int, w: float = 1.6, nu: int = 3, type_: int = 0,
+                 precision: int = _lib.PREC_F64):
+        self.A = A
+        self.handle = A.handle
+        self.kind = kind
+        params = PrecondParams(kind, float(w), int(nu), int(type_), int(precision))
+        p = C.c_void_p()
+        check(self.handle.lib.bsp_precond_create(self.handle.h, A.m, C.byref(params), C.byref(p)),
+              "bsp_precond_create", self.handle.h)
+        self.p = p
+        self.handle.adopt(self)
+
+    def __call__(self, r) -> None:
+        check(self.handle.lib.bsp_precond_apply_dev(self.handle.h, self.p, _ptr(r)),
+              "bsp_precond_apply_dev", self.handle.h)
+
+    def apply_host(self, r: np.ndarray) -> np.ndarray:
+        out = np.array(r, dtype=np.float64, copy=True)
+        check(self.handle.lib.bsp_precond_apply(self.handle.h, self.p, _ptr(out)),
+              "bsp_precond_apply", self.handle.h)
+        return out
+
+    def info(self) -> dict:
+        kind, lo, up, nnz = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        check(self.handle.lib.bsp_precond_info(self.p, C.byref(kind), C.byref(lo), C.byref(up),
+                                               C.byref(nnz)), "bsp_precond_info")
+        return {"kind": kind.value, "levels_lower": lo.value, "levels_upper": up.value,
+                "factor_nnzb": nnz.value}
+
+    def export(self) -> np.ndarray:
+        inf = self.info()
+        bs = self.A.bs
+        nblk = inf["factor_nnzb"] if self.kind in (_lib.PC_ILU0, _lib.PC_ICHOL0) else self.A.n_rows
+        out = np.zeros((nblk, bs, bs))
+        check(self.handle.lib.bsp_precond_export(self.p, _ptr(out), out.size), "bsp_precond_export")
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "p", None):
+            self.handle.lib.bsp_precond_destroy(self.p)
+            self.p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def NoPre(A: Matrix) -> None:
+    """preConditioners::NoPre: no preconditioning (solvers take None)."""
+    return None
+
+
+def Diag(A: Matrix, inv: str = "LU", precision: int = _lib.PREC_F64) -> Precond:
+    """Block-Jacobi: Diag<dense::LUFactor|CholeskyFactor> (preconditioners.hpp:75-111)."""
+    return Precond(A, _lib.PC_DIAG_LU if inv == "LU" else _lib.PC_DIAG_CHOL, precision=precision)
+
+
+def SOR(A: Matrix, w: float, nu: int, type_: int = 0, inv: str = "LU",
+        precision: int = _lib.PREC_F64) -> Precond:
+    """Block SOR from x = 0 (preconditioners.hpp:116-240); type <0 backward, 0 symmetric, >0 forward."""
+    return Precond(A, _lib.PC_SOR_LU if inv == "LU" else _lib.PC_SOR_CHOL, w=w, nu=nu, type_=type_,
+                   precision=precision)
+
+
+def ILU0(A: Matrix, precision: int = _lib.PREC_F64) -> Precond:
+    """Block ILU(0), natural order, no pivoting across blocks (preconditioners.hpp:246-357)."""
+    return Precond(A, _lib.PC_ILU0, precision=precision)
+
+
+def IChol0(A: Matrix, precision: int = _lib.PREC_F64) -> Precond:
+    """Block IC(0) on A.lowTri() (preconditioners.hpp:364-538)."""
+    return Precond(A, _lib.PC_ICHOL0, precision=precision)
+
+
+# ---------------------------------------------------------------- solvers
+
+def _opts(tol, max_iters, restart=-1, k=-1, print_iters=False, stop_rule=_lib.STOP_REFERENCE,
+          precision=_lib.PREC_F64, inner_tol=1e-4, max_outer=50) -> SolveOpts:
+    return SolveOpts(float(tol), int(max_iters), int(restart), int(k), int(bool(print_iters)),
+                     int(stop_rule), int(precision), float(inner_tol), int(max_outer))
+
+
+def _info_dict(info: SolveInfo) -> dict:
+    return {f: getattr(info, f) for f, _ in SolveInfo._fields_}
+
+
+def _solve(fn_dev, fn_host, A: Matrix, b, pc, opts: SolveOpts, return_info: bool):
+    lib = A.handle.lib
+    cap = max(4, opts.max_iters + 64 + (opts.max_iters // max(opts.restart, 1) if opts.restart > 0 else 0))
+    hist = np.zeros(cap)
+    info = SolveInfo()
+    pcp = pc.p if pc is not None else None
+    if hasattr(b, "data_ptr"):
+        import torch
+        x = torch.empty_like(b)
+        st = getattr(lib, fn_dev)(A.handle.h, A.m, pcp, _ptr(b), _ptr(x), C.byref(opts), _ptr(hist),
+                                  cap, C.byref(info))
+    else:
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(bb)
+        st = getattr(lib, fn_host)(A.handle.h, A.m, pcp, _ptr(bb), _ptr(x), C.byref(opts), _ptr(hist),
+                                   cap, C.byref(info))
+    if st not in (_lib.BSP_OK, 4, 3, 5):  # MAXIT / BREAKDOWN / NAN still return x
+        check(st, fn_dev, A.handle.h)
+    if return_info:
+        d = _info_dict(info)
+        return x, d, hist[: info.n_hist].copy()
+    return x
+
+
+def pCG(A: Matrix, b, tol: float, preCond: Precond | None = None, maxIters: int = 1000,
+        printIters: bool = False, return_info: bool = False, stop_rule: int = _lib.STOP_REFERENCE):
+    """Preconditioned CG (blocksp_solvers.hpp:51-105); x_0 = 0."""
+    return _solve("bsp_pcg_dev", "bsp_pcg", A, b, preCond,
+                  _opts(tol, maxIters, print_iters=printIters, stop_rule=stop_rule), return_info)
+
+
+def pGMRES(A: Matrix, b, tol: float, preCond: Precond | None = None, maxIters: int = 500,
+           restart: int = -1, k: int = -1, printIters: bool = False, return_info: bool = False,
+           stop_rule: int = _lib.STOP_REFERENCE):
+    """Left-preconditioned GMRES with optional deflated restart (blocksp_solvers.hpp:156-295)."""
+    return _solve("bsp_pgmres_dev", "bsp_pgmres", A, b, preCond,
+                  _opts(tol, maxIters, restart, k, printIters, stop_rule=stop_rule), return_info)
+
+
+class SOR_pGMRES:
+    """pGMRES with block SOR / LU block inversion (blocksp_solvers.hpp:344-391)."""
+
+    def __init__(self, A: Matrix, w: float = 1.6, nu: int = 3, SORtype: int = 0, tol: float = 1e-8,
+                 maxIters: int = 5000, restart: int = -1, k: int = -1, printIters: bool = False):
+        self.SOR_pre = SOR(A, w, nu, SORtype, "LU")
+        self.tol, self.maxIters, self.restart, self.k, self.printIters = tol, maxIters, restart, k, printIters
+
+    def solve(self, A: Matrix, b, return_info: bool = False):
+        return pGMRES(A, b, self.tol, self.SOR_pre, self.maxIters, self.restart, self.k,
+                      self.printIters, return_info)
+
+
+class SOR_pCG:
+    """pCG with symmetric block SOR / Cholesky block inversion (blocksp_solvers.hpp:395-431)."""
+
+    def __init__(self, A: Matrix, w: float = 1.6, nu: int = 3, tol: float = 1e-8, maxIters: int = 5000,
+                 printIters: bool = False):
+        self.SOR_pre = SOR(A, w, nu, 0, "Chol")
+        self.tol, self.maxIters, self.printIters = tol, maxIters, printIters
+
+    def solve(self, A: Matrix, b, return_info: bool = False):
+        return pCG(A, b, self.tol, self.SOR_pre, self.maxIters, self.printIters, return_info)
+
+
+class ILU0_pGMRES:
+    """pGMRES with block ILU0 (blocksp_solvers.hpp:434-467)."""
+
+    def __init__(self, A: Matrix, tol: float = 1e-8, maxIters: int = 5000, restart: int = -1,
+                 k: int = -1, printIters: bool = False):
+        self.ILU0_pre = ILU0(A)
+        self.tol, self.maxIters, self.restart, self.k, self.printIters = tol, maxIters, restart, k, printIters
+
+    def solve(self, A: Matrix, b, return_info: bool = False):
+        return pGMRES(A, b, self.tol, self.ILU0_pre, self.maxIters, self.restart, self.k,
+                      self.printIters, return_info)
+
+
+class IChol0_pCG:
+    """pCG with block IChol0 (blocksp_solvers.hpp:471-498)."""
+
+    def __init__(self, A: Matrix, tol: float = 1e-8, maxIters: int = 5000, printIters: bool = False):
+        self.IChol0_pre = IChol0(A)
+        self.tol, self.maxIters, self.printIters = tol, maxIters, printIters
+
+    def solve(self, A: Matrix, b, return_info: bool = False):
+        return pCG(A, b, self.tol, self.IChol0_pre, self.maxIters, self.printIters, return_info)
+
+
+class ez:
+    """One-call solvers with the reference's packaged defaults (blocksp_solvers.hpp:508-649):
+    tolerance 1e-8 (FP64), maxIters 5000, SOR w = 1.6 (0.6 robust), nu = 3."""
+
+    @staticmethod
+    def sor_pGMRES(A, b, printIters=False):
+        return SOR_pGMRES(A, 1.6, 3, 0, 1e-8, 5000, -1, -1, printIters).solve(A, b)
+
+    @staticmethod
+    def sor_pGMRES_robust(A, b, printIters=False):
+        return SOR_pGMRES(A, 0.6, 3, 0, 1e-8, 5000, -1, -1, printIters).solve(A, b)
+
+    @staticmethod
+    def sor_pGMRES_dr(A, b, printIters=False):
+        return SOR_pGMRES(A, 1.6, 3, 0, 1e-8, 5000, 30, 10, printIters).solve(A, b)
+
+    @staticmethod
+    def ilu0_pGMRES(A, b, printIters=False):
+        return ILU0_pGMRES(A, 1e-8, 5000, -1, -1, printIters).solve(A, b)
+
+    @staticmethod
+    def ilu0_pGMRES_dr(A, b, printIters=False):
+        return ILU0_pGMRES(A, 1e-8, 5000, 30, 10, printIters).solve(A, b)
+
+    @staticmethod
+    def sor_pCG(A, b, printIters=False):
+        return SOR_pCG(A, 1.6, 3, 1e-8, 5000, printIters).solve(A, b)
+
+    @staticmethod
+    def ichol0_pCG(A, b, printIters=False):
+        return IChol0_pCG(A, 1e-8, 5000, printIters).solve(A, b)

@@ -175,6 +175,7 @@ static int matrix_create_common(bsp_handle_t h, int n_rows, int n_cols, int bs, 
   BSP_TRY(validate_structure(n_rows, n_cols, bs, nnzb, row_ptr, col_idx));
   A = std::make_unique<bsp_matrix_s>();
   A->h = h;
+  A->device = h->device;
   A->n_rows = n_rows;
   A->n_cols = n_cols;
   A->bs = bs;
@@ -229,11 +230,10 @@ int bsp_matrix_create_dev(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_
 }
 
 int bsp_matrix_destroy(bsp_matrix_t A) {
+  // Does not touch A->h: the handle may already be gone.  cudaFree in the
+  // buffer destructors synchronises the device before releasing memory.
   if (!A) return BSP_OK;
-  {
-    DeviceGuard g(A->h->device);
-    cudaStreamSynchronize(A->h->stream);
-  }
+  DeviceGuard g(A->device);
   delete A;
   return BSP_OK;
 }

@@ -1,0 +1,739 @@
+// krylov.cu — pCG and pGMRES with deflated restart on sm_100a.
+//
+// Reference: blocksp_solvers.hpp:51-105 (pCG), :107-136 (one_arnoldi),
+// :156-295 (pGMRES), blocksp_deflated_restart.hpp:38-269 (Morgan GMRES-DR).
+//
+// All vectors, scalars, the Hessenberg matrix and its least-squares state
+// live on the GPU in FP64.  Per iteration the host enqueues kernels and reads
+// back one small status word; no vector or Hessenberg data crosses PCIe.
+//   * dots/norms are deterministic fused grid reductions (reduce.cuh),
+//   * the Arnoldi step is modified Gram-Schmidt with each axpy fused into the
+//     next dot (j+2 passes for column j),
+//   * the least-squares problem is kept in Givens-QR form and updated by one
+//     column per iteration (the reference re-solves it with gels each time;
+//     both give the minimiser of the same problem),
+//   * the deflated restart (harmonic Ritz values, Schur form, selection,
+//     invariant subspace, P_{k+1}, c_r, H_new) runs on one GPU thread in
+//     small_dense.h, and Qn <- Qn P_{k+1} is a tall-skinny in-place kernel.
+#include <algorithm>
+#include <vector>
+#include "reduce.cuh"
+#include "small_dense.h"
+
+struct bsp_precond_s;
+
+namespace bsp {
+
+int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha,
+                const void* x, double beta, const void* z, void* y, cudaStream_t s);
+int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z);
+int precond_check_status(bsp_precond_s* pc);
+int grid_for(const bsp_handle_s* h, int64_t n, int threads);
+
+constexpr double kEps = 2.220446049250313e-16;
+
+enum { DONE_RUNNING = 0, DONE_CONVERGED = 1, DONE_MAXIT = 2, DONE_BREAKDOWN = 3, DONE_NAN = 4 };
+
+// Status word read back by the host every iteration.
+struct KHead {
+  int done;
+  int j;          // current Arnoldi column (pGMRES) / iteration count (pCG)
+  int tot;        // pGMRES totIters
+  int keff;       // columns kept by the last deflated restart
+  int n_hist;
+  int restarted;
+  int breakdown;
+  int pad;
+  double res0, tolerance, res, zero_thresh;
+  // pCG scalars
+  double rz, pAp, alpha, beta;
+};
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_copy(int64_t n, const double* __restrict__ a, double* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+// q = v / *h unless |*h| < zero_thresh (breakdown: the reference does not
+// extend the basis, blocksp_solvers.hpp:133)
+__global__ void k_div(int64_t n, const double* __restrict__ v, const double* __restrict__ h,
+                      const KHead* __restrict__ head, double* __restrict__ q) {
+  const double d = *h;
+  if (fabs(d) < head->zero_thresh) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    q[i] = v[i] / d;
+}
+// p = z + beta p
+__global__ void k_cg_p(int64_t n, const double* __restrict__ z, const KHead* __restrict__ head,
+                       double* __restrict__ p) {
+  const double beta = head->beta;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+// ---- reduction bodies / finalisers (pCG) ----
+struct CgInitBody {  // sums p.p and r.z  (z == p initially)
+  const double *p, *r;
+  __device__ void setup() {}
+  __device__ void operator()(int64_t i, double (&a)[2]) const {
+    a[0] = fma(p[i], p[i], a[0]);
+    a[1] = fma(r[i], p[i], a[1]);
+  }
+};
+struct CgInitFin {
+  KHead* head;
+  double tol;
+  double* hist;
+  __device__ void operator()(const double (&s)[2]) const {
+    const double res0 = sqrt(s[0]);  // res_mag[0] = sqrt(dot(p, p))
+    head->res0 = res0;
+    head->res = res0;
+    head->tolerance = res0 * tol;
+    head->rz = s[1];
+    head->j = 0;
+    hist[0] = res0;
+    head->n_hist = 1;
+    head->done = (res0 > head->tolerance) ? DONE_RUNNING : DONE_CONVERGED;
+    if (!isfinite(res0)) head->done = DONE_NAN;
+  }
+};
+struct CgPApBody {
+  const double *p, *Ap;
+  __device__ void setup() {}
+  __device__ void operator()(int64_t i, double (&a)[1]) const { a[0] = fma(p[i], Ap[i], a[0]); }
+};
+struct CgPApFin {
+  KHead* head;
+  __device__ void operator()(const double (&s)[1]) const {
+    head->pAp = s[0];
+    head->alpha = head->rz / s[0];  // alpha = rz / dot(p, Ap)
+  }
+};
+struct CgUpdBody {  // x += alpha p; r -= alpha Ap; sum r.r
+  double *x, *r;
+  const double *p, *Ap;
+  const KHead* head;
+  double alpha;
+  __device__ void setup() { alpha = head->alpha; }
+  __device__ void operator()(int64_t i, double (&a)[1]) {
+    x[i] += alpha * p[i];
+    const double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    a[0] = fma(ri, ri, a[0]);
+  }
+};
+struct CgUpdFin {
+  KHead* head;
+  double* hist;
+  int hist_cap;
+  __device__ void operator()(const double (&s)[1]) const {
+    const double res = sqrt(s[0]);
+    head->res = res;
+    if (head->n_hist < hist_cap) hist[head->n_hist] = res;
+    head->n_hist++;
+    if (!isfinite(res) || !isfinite(head->alpha)) head->done = DONE_NAN;
+    else if (!(res > head->tolerance)) head->done = DONE_CONVERGED;
+  }
+};
+struct CgRzBody {
+  const double *r, *z;
+  __device__ void setup() {}
+  __device__ void operator()(int64_t i, double (&a)[1]) const { a[0] = fma(r[i], z[i], a[0]); }
+};
+struct CgRzFin {
+  KHead* head;
+  int max_iters;
+  __device__ void operator()(const double (&s)[1]) const {
+    head->beta = s[0] / head->rz;  // beta = dot(r, z) / rz
+    head->rz = s[0];
+    head->j++;
+    if (head->j > max_iters) head->done = DONE_MAXIT;
+  }
+};
+
+// ---- reduction bodies (pGMRES) ----
+struct NormFin {  // ||v|| into *out
+  double* out;
+  __device__ void operator()(const double (&s)[1]) const { *out = sqrt(fabs(s[0])); }
+};
+// pass i of MGS for column j: v -= H(i-1, j) q_{i-1} (i > 0); H(i, j) = q_i . v
+struct MgsBody {
+  double* v;
+  const double *qprev, *qi;
+  const double* hprev_ptr;
+  double hprev;
+  __device__ void setup() { hprev = qprev ? *hprev_ptr : 0.0; }
+  __device__ void operator()(int64_t e, double (&a)[1]) {
+    double ve = v[e];
+    if (qprev) {
+      ve = fma(-hprev, qprev[e], ve);
+      v[e] = ve;
+    }
+    a[0] = fma(qi[e], ve, a[0]);
+  }
+};
+// last pass: v -= H(j, j) q_j; H(j+1, j) = ||v||
+struct MgsLastBody {
+  double* v;
+  const double* qj;
+  const double* h_ptr;
+  double h;
+  __device__ void setup() { h = *h_ptr; }
+  __device__ void operator()(int64_t e, double (&a)[1]) {
+    const double ve = fma(-h, qj[e], v[e]);
+    v[e] = ve;
+    a[0] = fma(ve, ve, a[0]);
+  }
+};
+
+struct GPtrs {
+  KHead* head;
+  int m;  // leading dimension / capacity in columns
+  double *H, *R, *g, *rhs, *y;
+  sd::Rot* rots;
+  int* nrot;
+  double* hist;
+  int hist_cap;
+  // deflated restart work
+  double *Hn, *Z, *P, *w, *work, *wr, *wi, *resv, *Hnew;
+  int *perm, *sel;
+};
+
+__global__ void k_gm_init(GPtrs g, double tol) {
+  KHead* h = g.head;
+  const double res0 = h->res0;  // written by the norm reduction
+  h->res = res0;
+  h->tolerance = res0 * tol;
+  h->zero_thresh = fmin(res0 * kEps, kEps);
+  h->j = 0;
+  h->tot = 0;
+  h->restarted = 0;
+  h->breakdown = 0;
+  h->keff = 0;
+  g.hist[0] = res0;
+  h->n_hist = 1;
+  for (int i = 0; i <= g.m; ++i) {
+    g.g[i] = 0.0;
+    g.rhs[i] = 0.0;
+  }
+  g.g[0] = res0;
+  g.rhs[0] = res0;
+  *g.nrot = 0;
+  h->done = (res0 > h->tolerance) ? DONE_RUNNING : DONE_CONVERGED;
+  if (!isfinite(res0)) h->done = DONE_NAN;
+}
+
+// Least-squares update after column j was built (H(0..j+1, j) in place).
+__global__ void k_gm_ls(GPtrs g, int max_iters) {
+  KHead* h = g.head;
+  const int j = h->j;
+  const double hsub = g.H[(j + 1) * g.m + j];
+  if (fabs(hsub) < h->zero_thresh) h->breakdown = 1;
+  int nrot = *g.nrot;
+  const double res = sd::ls_add_column(g.H, g.m, j, j + 1, g.R, g.rots, nrot, g.g);
+  *g.nrot = nrot;
+  h->res = res;
+  if (h->n_hist < g.hist_cap) g.hist[h->n_hist] = res;
+  h->n_hist++;
+  h->j = j + 1;
+  h->tot++;
+  if (!isfinite(res)) h->done = DONE_NAN;
+  else if (!(res > h->tolerance)) h->done = DONE_CONVERGED;
+  else if (h->tot > max_iters) h->done = DONE_MAXIT;
+  else if (h->breakdown) h->done = DONE_BREAKDOWN;
+}
+
+// y = R^{-1} g over the current n = j columns
+__global__ void k_gm_y(GPtrs g) { sd::back_solve(g.R, g.m, g.g, g.head->j, g.y); }
+
+// x += sum_i y_i q_i  (in the reference's order: x = x0 + y0 q0 + y1 q1 + ...)
+__global__ void k_gm_combine(int64_t len, double* __restrict__ x, double* const* __restrict__ Q,
+                             const double* __restrict__ y, const KHead* __restrict__ head) {
+  const int n = head->j;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
+    double xe = x[e];
+    for (int i = 0; i < n; ++i) xe += y[i] * Q[i][e];
+    x[e] = xe;
+  }
+}
+
+// Deflated restart (deflated_restart.hpp:38-269) on one thread.
+// Input: H ((n+1) x n, n = head->j), rhs, y (current LS solution), k.
+// Output: P_{k+1} in g.P ((n+1) x (keff+1), ld = m+1), H_new, c_r, new LS state.
+__global__ void k_gm_deflate(GPtrs g, int k_req, int max_keep) {
+  KHead* h = g.head;
+  const int n = h->j, m1 = n + 1, ld = g.m;
+  int k = k_req > n ? n : k_req;
+  // residual vector res_vec = rhs - H y (solvers.hpp:202-203, 226-227)
+  for (int i = 0; i < m1; ++i) {
+    double s = 0.0;
+    for (int t = 0; t < n; ++t) s += g.H[i * ld + t] * g.y[t];
+    g.resv[i] = g.rhs[i] - s;
+  }
+  const double zero_thresh = 10.0 * n * n * kEps;
+  // (1) H_tilde = H_n + |h_mn|^2 H_n^{-T} e_n e_n^T
+  const int ldn = g.m;
+  for (int i = 0; i < n; ++i)
+    for (int t = 0; t < n; ++t) g.Hn[i * ldn + t] = g.H[i * ld + t];
+  const double hmn = g.H[n * ld + n - 1];
+  for (int i = 0; i < n; ++i) g.w[i] = 0.0;
+  g.w[n - 1] = 1.0;
+  sd::solve_transposed(g.Hn, ldn, n, g.w, g.work, g.perm);
+  for (int i = 0; i < n; ++i) g.Hn[i * ldn + n - 1] += hmn * hmn * g.w[i];
+  // (2) real Schur form, selection of the k smallest harmonic Ritz values
+  sd::hessenberg(g.Hn, ldn, n, g.Z, ldn, g.work);
+  const bool conv = sd::francis_qr(g.Hn, ldn, n, g.Z, ldn);
+  sd::schur_eigs(g.Hn, ldn, n, g.wr, g.wi);
+  sd::select_smallest(g.wr, g.wi, n, k, zero_thresh, g.perm, g.sel);
+  // (3) orthonormal basis P_k of the selected invariant subspace
+  const int ldp = g.m + 1;
+  const int keff = sd::invariant_basis(g.Hn, ldn, n, g.Z, ldn, g.wr, g.wi, g.sel, g.P, ldp, g.work);
+  k = keff;
+  if (!conv || k < 1 || k + 1 > max_keep) {
+    h->done = DONE_BREAKDOWN;  // the Qn update below is skipped (keff = -1)
+    h->keff = -1;
+    return;
+  }
+  // (4) P_{k+1}: [P_k; 0] and res_vec orthogonalised (classical GS as in :211-232)
+  for (int t = 0; t < k; ++t) g.P[n * ldp + t] = 0.0;
+  for (int i = 0; i < m1; ++i) g.P[i * ldp + k] = g.resv[i];
+  for (int c = 0; c < k; ++c) {
+    double d = 0.0;
+    for (int i = 0; i < m1; ++i) d += g.P[i * ldp + c] * g.P[i * ldp + k];
+    for (int i = 0; i < m1; ++i) g.P[i * ldp + k] -= d * g.P[i * ldp + c];
+  }
+  {
+    double nrm = 0.0;
+    for (int i = 0; i < m1; ++i) nrm += g.P[i * ldp + k] * g.P[i * ldp + k];
+    nrm = sqrt(nrm);
+    for (int i = 0; i < m1; ++i) g.P[i * ldp + k] /= nrm;
+  }
+  // (5) c_r = P_{k+1}^T res_vec
+  for (int c = 0; c <= k; ++c) {
+    double s = 0.0;
+    for (int i = 0; i < m1; ++i) s += g.P[i * ldp + c] * g.resv[i];
+    g.rhs[c] = s;
+  }
+  for (int i = k + 1; i <= g.m; ++i) g.rhs[i] = 0.0;
+  // (6) H_new = P_{k+1}^T H P_k  ((k+1) x k)
+  for (int i = 0; i < m1; ++i)  // W = H P_k -> Hnew as scratch ((n+1) x k, ld = m)
+    for (int c = 0; c < k; ++c) {
+      double s = 0.0;
+      for (int t = 0; t < n; ++t) s += g.H[i * ld + t] * g.P[t * ldp + c];
+      g.Hnew[i * ld + c] = s;
+    }
+  for (int r = 0; r <= k; ++r)
+    for (int c = 0; c < k; ++c) {
+      double s = 0.0;
+      for (int i = 0; i < m1; ++i) s += g.P[i * ldp + r] * g.Hnew[i * ld + c];
+      g.work[r * ld + c] = s;
+    }
+  for (int i = 0; i <= g.m; ++i)
+    for (int c = 0; c < g.m; ++c) g.H[i * ld + c] = 0.0;
+  for (int r = 0; r <= k; ++r)
+    for (int c = 0; c < k; ++c) g.H[r * ld + c] = g.work[r * ld + c];
+  // (8) restart the least-squares state from H_new and c_r
+  int nrot = 0;
+  for (int i = 0; i <= g.m; ++i) g.g[i] = g.rhs[i];
+  double res = 0.0;
+  for (int c = 0; c < k; ++c) res = sd::ls_add_column(g.H, ld, c, k, g.R, g.rots, nrot, g.g);
+  *g.nrot = nrot;
+  (void)res;
+  h->keff = k;
+  h->j = k;
+  h->restarted = 1;
+}
+
+// Qout[0..k] <- Qn[0..m1-1] P_{k+1} (deflated_restart.hpp:250-258), written to
+// spare vectors; the host then swaps the pointer tables.
+__global__ void k_gm_qn_update(int64_t len, double* const* __restrict__ Q, double* const* __restrict__ Qout,
+                               const double* __restrict__ P, int ldp, const KHead* __restrict__ head,
+                               int m1) {
+  const int kp1 = head->keff + 1;  // <= the spare count, checked by k_gm_deflate
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
+    for (int c = 0; c < kp1; ++c) {
+      double s = 0.0;
+      for (int i = 0; i < m1; ++i) s += Q[i][e] * P[i * ldp + c];
+      Qout[c][e] = s;
+    }
+  }
+}
+
+// Pure restart (k = 0): q_0 = r_0 / ||r_0||, rhs = ||r_0|| e_1 (solvers.hpp:255-262)
+__global__ void k_gm_pure_restart(GPtrs g) {
+  KHead* h = g.head;
+  const double r = h->res0;  // holds ||r_0|| of the new residual here
+  if (h->n_hist < g.hist_cap) g.hist[h->n_hist] = r;
+  h->n_hist++;
+  for (int i = 0; i <= g.m; ++i) {
+    g.g[i] = 0.0;
+    g.rhs[i] = 0.0;
+  }
+  g.g[0] = r;
+  g.rhs[0] = r;
+  *g.nrot = 0;
+  h->j = 0;
+  h->keff = 0;
+  h->restarted = 0;
+  h->res = r;
+  if (!(r > h->tolerance)) h->done = DONE_CONVERGED;
+}
+
+// ------------------------------------------------------------------ host helpers
+struct Vec {  // device vector pool entry
+  DevBuf<double> b;
+};
+
+static int read_head(bsp_handle_s* h, const KHead* d, KHead* out) {
+  BSP_CUDA_TRY(cudaMemcpyAsync(out, d, sizeof(KHead), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+static int status_of(int done) {
+  switch (done) {
+    case DONE_CONVERGED: return BSP_OK;
+    case DONE_MAXIT: return BSP_MAXIT;
+    case DONE_BREAKDOWN: return BSP_BREAKDOWN;
+    case DONE_NAN: return BSP_NAN;
+    default: return BSP_OK;
+  }
+}
+
+int true_residual(bsp_handle_s* h, bsp_matrix_s* A, const double* b, const double* x, double* work,
+                  double* out_host) {
+  const int64_t len = (int64_t)A->n_rows * A->bs;
+  BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, -1.0, x, 1.0, b, work, h->stream));
+  double* s = h->ws.scalars.get();
+  BSP_TRY(launch_reduce<1>(h, 1, len, DotBody{work, work}, StoreFin{s}));
+  BSP_TRY(launch_reduce<1>(h, 2, len, DotBody{b, b}, StoreFin{s + 1}));
+  double v[2];
+  BSP_CUDA_TRY(cudaMemcpyAsync(v, s, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out_host = v[1] > 0 ? sqrt(v[0]) / sqrt(v[1]) : sqrt(v[0]);
+  return BSP_OK;
+}
+
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+  }
+  double stop_ms() {
+    float ms = 0;
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EventTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+// ------------------------------------------------------------------ pCG
+int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b, double* x,
+              const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info) {
+  const int64_t len = (int64_t)A->n_rows * A->bs;
+  const int hcap = std::max(2, o->max_iters + 3);
+  DevBuf<double> vr, vp, vz, vAp, dhist;
+  DevBuf<KHead> dhead;
+  BSP_TRY(vr.alloc(len));
+  BSP_TRY(vp.alloc(len));
+  BSP_TRY(vz.alloc(len));
+  BSP_TRY(vAp.alloc(len));
+  BSP_TRY(dhist.alloc(hcap));
+  BSP_TRY(dhead.alloc(1));
+  BSP_CUDA_TRY(cudaMemsetAsync(dhead.get(), 0, sizeof(KHead), h->stream));
+  EventTimer tm(h->stream);
+  const int g = grid_for(h, len, 256);
+  KHead* hd = dhead.get();
+  BSP_CUDA_TRY(cudaMemsetAsync(x, 0, len * sizeof(double), h->stream));      // x = 0
+  k_copy<<<g, 256, 0, h->stream>>>(len, b, vr.get());                         // r = b
+  if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, b, vp.get()));              // p = M^-1 b
+  else k_copy<<<g, 256, 0, h->stream>>>(len, b, vp.get());
+  k_copy<<<g, 256, 0, h->stream>>>(len, vp.get(), vz.get());                  // z = p
+  BSP_TRY(launch_reduce<2>(h, 3, len, CgInitBody{vp.get(), vr.get()}, CgInitFin{hd, o->tol, dhist.get()}));
+  KHead st;
+  BSP_TRY(read_head(h, hd, &st));
+  while (st.done == DONE_RUNNING) {
+    BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, vp.get(), 0.0, nullptr, vAp.get(), h->stream));
+    BSP_TRY(launch_reduce<1>(h, 4, len, CgPApBody{vp.get(), vAp.get()}, CgPApFin{hd}));
+    BSP_TRY(launch_reduce<1>(h, 5, len, CgUpdBody{x, vr.get(), vp.get(), vAp.get(), hd, 0.0},
+                             CgUpdFin{hd, dhist.get(), hcap}));
+    BSP_TRY(read_head(h, hd, &st));
+    if (st.done != DONE_RUNNING) break;
+    if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, vr.get(), vz.get()));
+    else k_copy<<<g, 256, 0, h->stream>>>(len, vr.get(), vz.get());
+    BSP_TRY(launch_reduce<1>(h, 6, len, CgRzBody{vr.get(), vz.get()}, CgRzFin{hd, o->max_iters}));
+    k_cg_p<<<g, 256, 0, h->stream>>>(len, vz.get(), hd, vp.get());
+    BSP_CUDA_TRY(cudaPeekAtLastError());
+    BSP_TRY(read_head(h, hd, &st));
+  }
+  const double solve_ms = tm.stop_ms();
+  if (pc) BSP_TRY(precond_check_status(pc));
+  const int nh = std::min(st.n_hist, hcap);
+  if (hist && hist_cap > 0)
+    BSP_CUDA_TRY(cudaMemcpy(hist, dhist.get(), std::min(nh, hist_cap) * sizeof(double), cudaMemcpyDeviceToHost));
+  if (info) {
+    info->status = status_of(st.done);
+    info->iters = st.j;
+    info->n_hist = nh;
+    info->n_restarts = 0;
+    info->res0 = st.res0;
+    info->final_res = st.res;
+    info->solve_ms = solve_ms;
+    BSP_TRY(true_residual(h, A, b, x, vAp.get(), &info->true_rel_res));
+  }
+  if (o->print_iters) {
+    printf("pCG iters %d\n", st.j);  // solvers.hpp:99-103
+    if (st.j > o->max_iters) printf("maximum pCG iterations reached\n");
+  }
+  return status_of(st.done);
+}
+
+// ------------------------------------------------------------------ pGMRES
+int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b, double* x,
+                 const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info) {
+  const int64_t len = (int64_t)A->n_rows * A->bs;
+  const int restart = o->restart;
+  const int k_req = o->k;
+  const int m = restart > 0 ? restart : std::max(1, o->max_iters + 1);
+  if (restart > 256) {
+    record_error("pGMRES restart length above 256 is not supported");
+    return BSP_INVALID;
+  }
+  // Basis vectors.  Restarted: m+1 vectors plus k+2 spares for the deflated
+  // restart, allocated once.  Unrestarted: grown in chunks as the space grows.
+  constexpr int kChunk = 16;
+  const int n_spare = restart > 0 ? std::min(k_req, m) + 2 : 0;
+  std::vector<DevBuf<double>> chunks;
+  std::vector<double*> qptr, spare;
+  DevBuf<double*> dq, dspare;
+  BSP_TRY(dq.alloc(m + 1));
+  BSP_TRY(dspare.alloc(std::max(n_spare, 1)));
+  auto upload_tables = [&]() -> int {
+    const int cnt = std::min<int>((int)qptr.size(), m + 1);
+    BSP_CUDA_TRY(cudaMemcpyAsync(dq.get(), qptr.data(), cnt * sizeof(double*), cudaMemcpyHostToDevice, h->stream));
+    if (n_spare > 0)
+      BSP_CUDA_TRY(cudaMemcpyAsync(dspare.get(), spare.data(), n_spare * sizeof(double*), cudaMemcpyHostToDevice, h->stream));
+    return BSP_OK;
+  };
+  auto ensure_basis = [&](int count) -> int {
+    bool grew = false;
+    while ((int)qptr.size() < count) {
+      const int nv = restart > 0 ? (m + 1 + n_spare) : kChunk;
+      DevBuf<double> c;
+      BSP_TRY(c.alloc((size_t)nv * len));
+      for (int t = 0; t < nv; ++t) {
+        double* ptr = c.get() + (size_t)t * len;
+        if (restart > 0 && t > m) spare.push_back(ptr);
+        else qptr.push_back(ptr);
+      }
+      chunks.push_back(std::move(c));
+      grew = true;
+    }
+    if (grew) BSP_TRY(upload_tables());
+    return BSP_OK;
+  };
+  DevBuf<double> vv, vx0, vr0;
+  BSP_TRY(vv.alloc(len));
+  BSP_TRY(vx0.alloc(len));
+  BSP_TRY(vr0.alloc(len));
+  // small dense state
+  const int hcap = std::max(4, o->max_iters + 2 + (restart > 0 ? o->max_iters / restart + 2 : 0));
+  const size_t HM = (size_t)(m + 1) * m;
+  const size_t nrot_cap = (size_t)(m + 1) * (m + 2) / 2 + m + 8;
+  DevBuf<double> dsm;
+  size_t dr = restart > 0 ? (size_t)m * m * 3 + (size_t)(m + 1) * (m + 2) + 8 * (size_t)m + 64 + HM : 0;
+  const size_t total = 2 * HM + 3 * (size_t)(m + 2) + hcap + dr;
+  BSP_TRY(dsm.alloc(total));
+  DevBuf<sd::Rot> drots;
+  BSP_TRY(drots.alloc(nrot_cap));
+  DevBuf<int> dint;
+  BSP_TRY(dint.alloc(1 + 2 * (size_t)m + 8));
+  DevBuf<KHead> dhead;
+  BSP_TRY(dhead.alloc(1));
+  BSP_CUDA_TRY(cudaMemsetAsync(dsm.get(), 0, total * sizeof(double), h->stream));
+  BSP_CUDA_TRY(cudaMemsetAsync(dhead.get(), 0, sizeof(KHead), h->stream));
+  GPtrs gp{};
+  gp.head = dhead.get();
+  gp.m = m;
+  double* base = dsm.get();
+  gp.H = base; base += HM;
+  gp.R = base; base += HM;
+  gp.g = base; base += m + 2;
+  gp.rhs = base; base += m + 2;
+  gp.y = base; base += m + 2;
+  gp.hist = base; base += hcap;
+  gp.hist_cap = hcap;
+  if (restart > 0) {
+    gp.Hn = base; base += (size_t)m * m;
+    gp.Z = base; base += (size_t)m * m;
+    gp.work = base; base += (size_t)m * m + 4 * (size_t)m + 32;
+    gp.P = base; base += (size_t)(m + 1) * (m + 2);
+    gp.w = base; base += m + 1;
+    gp.wr = base; base += m + 1;
+    gp.wi = base; base += m + 1;
+    gp.resv = base; base += m + 2;
+    gp.Hnew = base; base += HM;
+  }
+  gp.rots = drots.get();
+  gp.nrot = dint.get();
+  gp.perm = dint.get() + 1;
+  gp.sel = dint.get() + 1 + m;
+  KHead* hd = dhead.get();
+  const int g = grid_for(h, len, 256);
+
+  EventTimer tm(h->stream);
+  BSP_TRY(ensure_basis(restart > 0 ? m + 1 : 2));
+  BSP_CUDA_TRY(cudaMemsetAsync(vx0.get(), 0, len * sizeof(double), h->stream));  // x_0 = 0
+  // r_0 = M^-1 b; res_mag[0] = ||r_0||; q_0 = r_0 / res_mag[0]
+  if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, b, vr0.get()));
+  else k_copy<<<g, 256, 0, h->stream>>>(len, b, vr0.get());
+  BSP_TRY(launch_reduce<1>(h, 7, len, DotBody{vr0.get(), vr0.get()}, NormFin{&hd->res0}));
+  k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
+  k_gm_init<<<1, 1, 0, h->stream>>>(gp, o->tol);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  KHead st;
+  BSP_TRY(read_head(h, hd, &st));
+  int n_restarts = 0;
+  // first Arnoldi steps reuse the zeroed memset of q_0 normalisation guard
+  while (st.done == DONE_RUNNING) {
+    const int j = st.j;
+    BSP_TRY(ensure_basis(j + 2));
+    // v = M^-1 A q_j
+    BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, qptr[j], 0.0, nullptr, vv.get(), h->stream));
+    if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, vv.get(), vv.get()));
+    // MGS: j+2 fused passes
+    for (int i = 0; i <= j; ++i) {
+      MgsBody body{vv.get(), i > 0 ? qptr[i - 1] : nullptr, qptr[i],
+                   i > 0 ? gp.H + (size_t)(i - 1) * m + j : nullptr, 0.0};
+      BSP_TRY(launch_reduce<1>(h, 8 + (i & 1), len, body, StoreFin{gp.H + (size_t)i * m + j}));
+    }
+    BSP_TRY(launch_reduce<1>(h, 10, len, MgsLastBody{vv.get(), qptr[j], gp.H + (size_t)j * m + j, 0.0},
+                             NormFin{gp.H + (size_t)(j + 1) * m + j}));
+    k_div<<<g, 256, 0, h->stream>>>(len, vv.get(), gp.H + (size_t)(j + 1) * m + j, hd, qptr[j + 1]);
+    k_gm_ls<<<1, 1, 0, h->stream>>>(gp, o->max_iters);
+    BSP_CUDA_TRY(cudaPeekAtLastError());
+    BSP_TRY(read_head(h, hd, &st));
+    if (st.done != DONE_RUNNING) break;
+    if (restart > 0 && st.j == restart) {
+      // x_0 = x_0 + Q y
+      k_gm_y<<<1, 1, 0, h->stream>>>(gp);
+      k_gm_combine<<<g, 256, 0, h->stream>>>(len, vx0.get(), dq.get(), gp.y, hd);
+      ++n_restarts;
+      if (k_req == 0) {
+        // r_0 = M^-1 (b - A x_0), pure restart
+        BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, -1.0, vx0.get(), 1.0, b, vr0.get(), h->stream));
+        if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, vr0.get(), vr0.get()));
+        BSP_TRY(launch_reduce<1>(h, 7, len, DotBody{vr0.get(), vr0.get()}, NormFin{&hd->res0}));
+        k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
+        k_gm_pure_restart<<<1, 1, 0, h->stream>>>(gp);
+      } else {
+        k_gm_deflate<<<1, 1, 0, h->stream>>>(gp, k_req, n_spare);
+        k_gm_qn_update<<<g, 256, 0, h->stream>>>(len, dq.get(), dspare.get(), gp.P, m + 1, hd, st.j + 1);
+      }
+      BSP_CUDA_TRY(cudaPeekAtLastError());
+      BSP_TRY(read_head(h, hd, &st));
+      if (k_req != 0 && st.done == DONE_RUNNING) {
+        if (st.keff + 1 > n_spare) {
+          record_error("deflated restart kept more vectors than reserved");
+          return BSP_BREAKDOWN;
+        }
+        for (int c = 0; c <= st.keff; ++c) std::swap(qptr[c], spare[c]);
+        BSP_TRY(upload_tables());
+      }
+    }
+  }
+  // x = x_0 + Q y
+  k_gm_y<<<1, 1, 0, h->stream>>>(gp);
+  BSP_CUDA_TRY(cudaMemcpyAsync(x, vx0.get(), len * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  k_gm_combine<<<g, 256, 0, h->stream>>>(len, x, dq.get(), gp.y, hd);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  const double solve_ms = tm.stop_ms();
+  if (pc) BSP_TRY(precond_check_status(pc));
+  const int nh = std::min(st.n_hist, hcap);
+  if (hist && hist_cap > 0)
+    BSP_CUDA_TRY(cudaMemcpy(hist, gp.hist, std::min(nh, hist_cap) * sizeof(double), cudaMemcpyDeviceToHost));
+  if (info) {
+    info->status = status_of(st.done);
+    info->iters = st.tot;
+    info->n_hist = nh;
+    info->n_restarts = n_restarts;
+    info->res0 = st.res0;
+    info->final_res = st.res;
+    info->solve_ms = solve_ms;
+    BSP_TRY(true_residual(h, A, b, x, vv.get(), &info->true_rel_res));
+  }
+  if (o->print_iters) {
+    printf("pGMRES iters %d\n", st.tot);  // solvers.hpp:266-270
+    if (st.tot > o->max_iters) printf("maximum pGMRES iterations reached\n");
+  }
+  return status_of(st.done);
+}
+
+}  // namespace bsp
+
+// ================================================================== C ABI
+using namespace bsp;
+
+static int solve_common(bool gmres, bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc,
+                        const double* b, double* x, const bsp_solve_opts* opts, double* hist,
+                        int hist_cap, bsp_solve_info* info) {
+  if (!h || !A || !b || !x || !opts) return BSP_INVALID;
+  if (A->n_rows != A->n_cols) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  if (info) *info = bsp_solve_info{};
+  return gmres ? pgmres_solve(h, A, pc, b, x, opts, hist, hist_cap, info)
+               : pcg_solve(h, A, pc, b, x, opts, hist, hist_cap, info);
+}
+
+static int solve_host(bool gmres, bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc,
+                      const double* b, double* x, const bsp_solve_opts* opts, double* hist,
+                      int hist_cap, bsp_solve_info* info) {
+  if (!h || !A || !b || !x) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  const size_t len = (size_t)A->n_rows * A->bs;
+  BSP_TRY(h->stage(len, len));
+  BSP_CUDA_TRY(cudaMemcpyAsync(h->stage_in.get(), b, len * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const int s = solve_common(gmres, h, A, pc, h->stage_in.get(), h->stage_out.get(), opts, hist,
+                             hist_cap, info);
+  if (s != BSP_OK && s != BSP_MAXIT && s != BSP_BREAKDOWN && s != BSP_NAN) return s;
+  BSP_CUDA_TRY(cudaMemcpyAsync(x, h->stage_out.get(), len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return s;
+}
+
+extern "C" {
+
+int bsp_pcg_dev(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+                const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info) {
+  return solve_common(false, h, A, pc, b, x, opts, hist, hist_cap, info);
+}
+int bsp_pgmres_dev(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+                   const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info) {
+  return solve_common(true, h, A, pc, b, x, opts, hist, hist_cap, info);
+}
+int bsp_pcg(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+            const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info) {
+  return solve_host(false, h, A, pc, b, x, opts, hist, hist_cap, info);
+}
+int bsp_pgmres(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, double* x,
+               const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info) {
+  return solve_host(true, h, A, pc, b, x, opts, hist, hist_cap, info);
+}
+int bsp_true_residual_dev(bsp_handle_t h, bsp_matrix_t A, const double* b, const double* x,
+                          double* rel_res_host) {
+  if (!h || !A || !b || !x || !rel_res_host) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  DevBuf<double> w;
+  BSP_TRY(w.alloc((size_t)A->n_rows * A->bs));
+  return true_residual(h, A, b, x, w.get(), rel_res_host);
+}
+
+}  // extern "C"

@@ -1,0 +1,1027 @@
+// precond.cu — block Diag / SOR / ILU0 / IChol0 preconditioners on sm_100a.
+//
+// Reference: blocksp_preconditioners.hpp (BlockSp v1.0).
+//   makeADInv            :22-63   -> k_factor mode DIAG (inverted diagonal blocks)
+//   Diag                 :75-111  -> sweep with no off-diagonal entries, POST_D
+//   SOR                  :116-240 -> nu sync-free forward / backward sweeps from x = 0
+//   ILU0::factor         :274-291 -> k_factor mode ILU0 (row-wise, level scheduled)
+//   ILU0::invmul         :294-349 -> unit-L forward sweep + U backward sweep
+//   IChol0::factor       :393-429 -> k_factor mode ICHOL0
+//   IChol0::invmul       :432-489 -> L forward sweep + L^T backward sweep
+//
+// Method preservation: every sweep and factorisation runs in the reference's
+// natural row order.  Rows are only *scheduled* by dependency level (a row
+// starts once every row it reads is final), which changes when a row is
+// computed but not what it computes, so the preconditioner is the same
+// operator as the reference's (no recolouring, no reordering).
+//
+// Sync-free execution: a launch is persistent; each group of lanes claims the
+// next row of the level order with an atomic ticket, waits (bounded spin) on
+// the ready flags of the rows it depends on, computes, publishes its row and
+// raises its own flag.  A row only waits on rows with smaller tickets, which
+// were claimed by groups that are already running, so the launch always
+// progresses without any co-residency requirement.  Flags hold the epoch of
+// the sweep that last wrote them, so they never need clearing.
+//
+// The factorisation is row-oriented (IKJ): row k applies the eliminations of
+// rows i < k in increasing i, exactly the sequence of updates the reference's
+// right-looking loop applies to each block (k, j), so the factors are the same.
+#include <algorithm>
+#include <numeric>
+#include "blockops.cuh"
+#include "reduce.cuh"
+
+namespace bsp {
+
+// ----------------------------------------------------------------- device wait
+__device__ __forceinline__ void wait_flag(const int* f, int epoch, DevStatus* st, int who) {
+  if (ld_acquire(f) == epoch) return;
+  unsigned spins = 0;
+  while (ld_acquire(f) != epoch) {
+    __nanosleep(40);
+    if ((++spins & 255u) == 0u) {
+      if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;  // already failed
+      if (spins > kSpinLimit) {
+        set_status(st, BSP_TIMEOUT, who);
+        return;
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------------- sweeps
+enum { RANGE_LOWER = 0, RANGE_UPPER = 1, RANGE_SPLIT = 2, RANGE_ALL = 3, RANGE_NONE = 4 };
+enum { POST_NONE = 0, POST_D = 1, POST_DT = 2, POST_SOR = 3 };
+
+template <typename VT, typename AT> struct SweepP {
+  int n;
+  const int* order;     // processing order (null: identity)
+  const int* ptr;       // row pointer of the structure swept
+  const int* idx;       // column (transposed structure: source row) of each entry
+  const int64_t* blk;   // block index of each entry (null: the entry index)
+  const int* diag;      // position of the diagonal entry of each row
+  int range;            // RANGE_*
+  int dep_dir;          // RANGE_SPLIT: -1 deps are j < i (forward), +1 deps are j > i
+  const VT* vals;
+  const VT* dinv;
+  const AT* rhs;
+  const AT* xold;       // POST_SOR / RANGE_SPLIT: iterate before the sweep (null: zero)
+  AT* x;
+  AT w;
+  int* flags;
+  int epoch;
+  unsigned* ticket;
+  DevStatus* st;
+};
+
+template <typename VT, typename AT>
+__device__ __forceinline__ void row_range(const SweepP<VT, AT>& p, int i, int& beg, int& end) {
+  switch (p.range) {
+    case RANGE_LOWER: beg = __ldg(p.ptr + i); end = __ldg(p.diag + i); break;
+    case RANGE_UPPER: beg = __ldg(p.diag + i) + 1; end = __ldg(p.ptr + i + 1); break;
+    case RANGE_NONE: beg = end = 0; break;
+    default: beg = __ldg(p.ptr + i); end = __ldg(p.ptr + i + 1); break;
+  }
+}
+
+constexpr int kSweepThreads = 256;
+
+template <int BS, typename VT, typename AT, bool TRANS, int POST>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p) {
+  using M = BlockMap<BS, VT>;
+  using CV = typename Chunk<VT>::vec;
+  constexpr int V = M::V, G = M::G, P = M::P, CPR = M::CPR, RPP = M::RPP, CPB = M::CPB;
+  constexpr int GPC = kSweepThreads / G;
+  __shared__ AT sm_s[GPC][BS];
+  const int gl = threadIdx.x % G;
+  const int gid = threadIdx.x / G;
+  const int lane = threadIdx.x & 31;
+  const int gbase = lane - gl;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
+  const int c0 = (gl % CPR) * V;
+  const CV* vb = reinterpret_cast<const CV*>(p.vals);
+  AT* s = sm_s[gid];
+
+  while (true) {
+    int t = 0;
+    if (gl == 0) t = (int)atomicAdd(p.ticket, 1u);
+    t = __shfl_sync(gmask, t, gbase);
+    if (t >= p.n) break;
+    const int i = p.order ? __ldg(p.order + t) : t;
+    int beg, end;
+    row_range(p, i, beg, end);
+    AT acc[P];
+    AT tac[V];
+#pragma unroll
+    for (int q = 0; q < P; ++q) acc[q] = AT(0);
+#pragma unroll
+    for (int v = 0; v < V; ++v) tac[v] = AT(0);
+    for (int e = beg; e < end; ++e) {
+      const int j = __ldg(p.idx + e);
+      const AT* src;
+      if (p.range == RANGE_SPLIT) {
+        if (j == i) continue;
+        const bool dep = (p.dep_dir < 0) ? (j < i) : (j > i);
+        if (dep) {
+          wait_flag(p.flags + j, p.epoch, p.st, i);
+          src = p.x;
+        } else {
+          if (!p.xold) continue;
+          src = p.xold;
+        }
+      } else {
+        wait_flag(p.flags + j, p.epoch, p.st, i);
+        src = p.x;
+      }
+      const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
+      if constexpr (!TRANS) {
+        AT xv[V];
+        ld_vec_cg<V>(src + (int64_t)j * BS + c0, xv);
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          AT av[V];
+          unpack(ld_stream(vb + b * CPB + q * G + gl), av);
+#pragma unroll
+          for (int v = 0; v < V; ++v) acc[q] = fma(av[v], xv[v], acc[q]);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const int r = q * RPP + gl / CPR;
+          const AT xr = __ldcg(src + (int64_t)j * BS + r);
+          AT av[V];
+          unpack(ld_stream(vb + b * CPB + q * G + gl), av);
+#pragma unroll
+          for (int v = 0; v < V; ++v) tac[v] = fma(av[v], xr, tac[v]);
+        }
+      }
+    }
+    // s = rhs_i - sum  (in shared memory, BS values per group)
+    if constexpr (!TRANS) {
+#pragma unroll
+      for (int q = 0; q < P; ++q) acc[q] = row_reduce<CPR>(acc[q], gmask);
+      if (gl % CPR == 0) {
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const int r = q * RPP + gl / CPR;
+          s[r] = __ldcg(p.rhs + (int64_t)i * BS + r) - acc[q];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int o = CPR; o < G; o <<= 1) tac[v] += __shfl_xor_sync(gmask, tac[v], o);
+      if (gl < CPR) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) s[c0 + v] = __ldcg(p.rhs + (int64_t)i * BS + c0 + v) - tac[v];
+      }
+    }
+    __syncwarp(gmask);
+    // post-operation and write-back of row i
+    if constexpr (POST == POST_NONE) {
+      for (int r = gl; r < BS; r += G) p.x[(int64_t)i * BS + r] = s[r];
+    } else if constexpr (POST == POST_D || POST == POST_SOR) {
+      const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)i * CPB;
+      AT sv[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) sv[v] = s[c0 + v];
+      AT o[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        AT av[V];
+        unpack(ld_stream(db + q * G + gl), av);
+        o[q] = AT(0);
+#pragma unroll
+        for (int v = 0; v < V; ++v) o[q] = fma(av[v], sv[v], o[q]);
+        o[q] = row_reduce<CPR>(o[q], gmask);
+      }
+      if (gl % CPR == 0) {
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const int r = q * RPP + gl / CPR;
+          AT val = o[q];
+          if constexpr (POST == POST_SOR) {
+            // x(im) += -w * x(im) + w * ph   (preconditioners.hpp:161-165)
+            const AT xo = p.xold ? __ldcg(p.xold + (int64_t)i * BS + r) : AT(0);
+            val = xo + (-p.w * xo + p.w * val);
+          }
+          p.x[(int64_t)i * BS + r] = val;
+        }
+      }
+    } else {  // POST_DT: x = D^T s
+      const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)i * CPB;
+      AT o[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) o[v] = AT(0);
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const int r = q * RPP + gl / CPR;
+        const AT sr = s[r];
+        AT av[V];
+        unpack(ld_stream(db + q * G + gl), av);
+#pragma unroll
+        for (int v = 0; v < V; ++v) o[v] = fma(av[v], sr, o[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int off = CPR; off < G; off <<= 1) o[v] += __shfl_xor_sync(gmask, o[v], off);
+      if (gl < CPR) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) p.x[(int64_t)i * BS + c0 + v] = o[v];
+      }
+    }
+    __threadfence();
+    __syncwarp(gmask);
+    if (gl == 0) st_release(p.flags + i, p.epoch);
+    __syncwarp(gmask);
+  }
+}
+
+// Any block size (bs <= 32): one warp per row, lane r computes component r.
+template <typename VT, typename AT, bool TRANS, int POST>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_generic(const SweepP<VT, AT> p, int bs) {
+  __shared__ AT sm_s[kSweepThreads / 32][32];
+  const int lane = threadIdx.x & 31;
+  AT* s = sm_s[threadIdx.x >> 5];
+  const int b2 = bs * bs;
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = (int)atomicAdd(p.ticket, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= p.n) break;
+    const int i = p.order ? __ldg(p.order + t) : t;
+    int beg, end;
+    row_range(p, i, beg, end);
+    AT acc = AT(0);
+    for (int e = beg; e < end; ++e) {
+      const int j = __ldg(p.idx + e);
+      const AT* src;
+      if (p.range == RANGE_SPLIT) {
+        if (j == i) continue;
+        const bool dep = (p.dep_dir < 0) ? (j < i) : (j > i);
+        if (dep) {
+          wait_flag(p.flags + j, p.epoch, p.st, i);
+          src = p.x;
+        } else {
+          if (!p.xold) continue;
+          src = p.xold;
+        }
+      } else {
+        wait_flag(p.flags + j, p.epoch, p.st, i);
+        src = p.x;
+      }
+      const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
+      if (lane < bs) {
+        const VT* a = p.vals + b * b2;
+        for (int c = 0; c < bs; ++c) {
+          const AT m = TRANS ? AT(a[c * bs + lane]) : AT(a[lane * bs + c]);
+          acc = fma(m, __ldcg(src + (int64_t)j * bs + c), acc);
+        }
+      }
+    }
+    if (lane < bs) s[lane] = __ldcg(p.rhs + (int64_t)i * bs + lane) - acc;
+    __syncwarp();
+    if (lane < bs) {
+      AT val = s[lane];
+      if constexpr (POST != POST_NONE) {
+        const VT* d = p.dinv + (int64_t)i * b2;
+        val = AT(0);
+        for (int c = 0; c < bs; ++c) {
+          const AT m = (POST == POST_DT) ? AT(d[c * bs + lane]) : AT(d[lane * bs + c]);
+          val = fma(m, s[c], val);
+        }
+      }
+      if constexpr (POST == POST_SOR) {
+        const AT xo = p.xold ? __ldcg(p.xold + (int64_t)i * bs + lane) : AT(0);
+        val = xo + (-p.w * xo + p.w * val);
+      }
+      p.x[(int64_t)i * bs + lane] = val;
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(p.flags + i, p.epoch);
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------- factorisation
+enum { FACT_ILU0 = 0, FACT_ICHOL0 = 1, FACT_DIAG = 2 };
+
+struct FactorP {
+  int n, bs, mode;
+  const int* order;
+  const int* ptr;
+  const int* col;
+  const int* diag;
+  double* vals;
+  double* dinv;
+  int* flags;
+  int epoch;
+  unsigned* ticket;
+  DevStatus* st;
+};
+
+constexpr int kFactorWarps = 4;
+
+__global__ void __launch_bounds__(kFactorWarps * 32) k_factor(const FactorP p) {
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bs = p.bs, b2 = bs * bs;
+  double* sA = smem + (size_t)warp * 5 * b2;
+  double* sB = sA + b2;
+  double* sC = sB + b2;
+  double* aug = sC + b2;  // 2*b2
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = (int)atomicAdd(p.ticket, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= p.n) break;
+    const int k = p.order ? __ldg(p.order + t) : t;
+    const int beg = __ldg(p.ptr + k), dg = __ldg(p.diag + k), end = __ldg(p.ptr + k + 1);
+    if (p.mode != FACT_DIAG) {
+      for (int e = beg; e < dg; ++e) wait_flag(p.flags + __ldg(p.col + e), p.epoch, p.st, k);
+      for (int e = beg; e < dg; ++e) {
+        const int i = __ldg(p.col + e);
+        warp_copy_in(sA, p.vals + (int64_t)e * b2, b2);
+        warp_copy_in(sB, p.dinv + (int64_t)i * b2, b2);
+        // ILU0: L_ki = A_ki U_ii^{-1};  IChol0: L_ki = A_ki L_ii^{-T}
+        warp_gemm(sC, sA, sB, bs, p.mode == FACT_ICHOL0);
+        warp_copy_out(p.vals + (int64_t)e * b2, sC, b2);
+        if (p.mode == FACT_ILU0) {
+          // A_kj -= L_ki U_ij for every j > i present in both rows
+          const int ui0 = __ldg(p.diag + i) + 1, ui1 = __ldg(p.ptr + i + 1);
+          for (int e2 = e + 1; e2 < end; ++e2) {
+            const int pos = warp_find(p.col, ui0, ui1, __ldg(p.col + e2));
+            if (pos >= 0) {
+              warp_copy_in(sB, p.vals + (int64_t)pos * b2, b2);
+              warp_gemm_sub_global(p.vals + (int64_t)e2 * b2, sC, sB, bs, false);
+            }
+          }
+        } else {
+          // A_kj -= L_ki L_ji^T for i < j <= k with (j, i) in the pattern
+          for (int e2 = e + 1; e2 <= dg; ++e2) {
+            const int j = __ldg(p.col + e2);
+            if (j == k) {
+              warp_gemm_sub_global(p.vals + (int64_t)e2 * b2, sC, sC, bs, true);
+            } else {
+              const int pos = warp_find(p.col, __ldg(p.ptr + j), __ldg(p.diag + j), i);
+              if (pos >= 0) {
+                warp_copy_in(sB, p.vals + (int64_t)pos * b2, b2);
+                warp_gemm_sub_global(p.vals + (int64_t)e2 * b2, sC, sB, bs, true);
+              }
+            }
+          }
+        }
+      }
+    }
+    warp_copy_in(sA, p.vals + (int64_t)dg * b2, b2);
+    if (p.mode == FACT_ICHOL0) {
+      const bool ok = warp_cholesky(sA, bs);
+      if (!ok && lane == 0) set_status(p.st, BSP_NOT_SPD, k);
+      warp_copy_out(p.vals + (int64_t)dg * b2, sA, b2);
+      warp_lower_inverse(sB, sA, bs);
+      warp_copy_out(p.dinv + (int64_t)k * b2, sB, b2);
+    } else {
+      const bool ok = warp_inverse(sB, sA, aug, bs);
+      if (!ok && lane == 0) set_status(p.st, BSP_ZERO_PIVOT, k);
+      warp_copy_out(p.dinv + (int64_t)k * b2, sB, b2);
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0 && p.flags) st_release(p.flags + k, p.epoch);
+    __syncwarp();
+  }
+}
+
+// Gather blocks: dst[e] = src[perm[e]] (bs*bs values each).
+__global__ void k_gather_blocks(int64_t nblk, int b2, const int64_t* __restrict__ perm,
+                                const double* __restrict__ src, double* __restrict__ dst) {
+  const int64_t total = nblk * b2;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / b2;
+    dst[t] = src[perm[e] * b2 + (t % b2)];
+  }
+}
+__global__ void k_scatter_blocks(int64_t nblk, int b2, const int64_t* __restrict__ perm,
+                                 const double* __restrict__ src, double* __restrict__ dst) {
+  const int64_t total = nblk * b2;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / b2;
+    dst[perm[e] * b2 + (t % b2)] = src[t];
+  }
+}
+template <typename T>
+__global__ void k_convert(int64_t n, const double* __restrict__ a, T* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if constexpr (std::is_same<T, float>::value) b[i] = (float)a[i];
+    else b[i] = __float2bfloat16_rn((float)a[i]);
+  }
+}
+
+int grid_for(const bsp_handle_s* h, int64_t n, int threads);
+
+}  // namespace bsp
+
+// ================================================================= host side
+using namespace bsp;
+
+struct bsp_precond_s {
+  bsp_handle_t h = nullptr;
+  int device = 0;
+  bsp_matrix_t A = nullptr;
+  int kind = 0, n = 0, bs = 0, precision = 0;
+  double w = 1.6;
+  int nu = 3, type = 0;
+  // factor storage (ILU0: every block of A; IChol0: A.lowTri()), columns sorted
+  DevBuf<int> f_ptr, f_col, f_diag;
+  DevBuf<double> f_vals;
+  DevBuf<float> f_vals32;
+  DevBuf<__nv_bfloat16> f_vals16;
+  std::vector<int64_t> h_perm;  // factor entry -> block index in A
+  DevBuf<int64_t> d_perm;
+  int64_t f_nnzb = 0;
+  // IChol0 backward sweep: transposed strictly-lower structure of L
+  DevBuf<int> t_ptr, t_row;
+  DevBuf<int64_t> t_blk;
+  // SOR / Diag on A's own structure
+  DevBuf<int> a_diag;
+  // inverted diagonal blocks (U_ii^-1, L_ii^-1 or A_ii^-1)
+  DevBuf<double> dinv;
+  DevBuf<float> dinv32;
+  DevBuf<__nv_bfloat16> dinv16;
+  // level orders
+  DevBuf<int> order_lo, order_up;
+  int n_lev_lo = 0, n_lev_up = 0;
+  // sync-free state
+  DevBuf<int> flags;
+  DevBuf<unsigned> ticket;
+  // SOR ping-pong iterates
+  DevBuf<double> sor_a, sor_b;
+  DevBuf<float> sor_a32, sor_b32;
+};
+
+namespace bsp {
+
+// Level of each row when row i depends on the rows listed in deps(i).
+template <class Deps>
+static int level_order(int n, bool ascending, Deps deps, std::vector<int>& order) {
+  std::vector<int> lvl(n, 0);
+  int maxl = -1;
+  if (ascending) {
+    for (int i = 0; i < n; ++i) {
+      int l = 0;
+      deps(i, [&](int j) { l = std::max(l, lvl[j] + 1); });
+      lvl[i] = l;
+      maxl = std::max(maxl, l);
+    }
+  } else {
+    for (int i = n - 1; i >= 0; --i) {
+      int l = 0;
+      deps(i, [&](int j) { l = std::max(l, lvl[j] + 1); });
+      lvl[i] = l;
+      maxl = std::max(maxl, l);
+    }
+  }
+  // counting sort by level; inside a level rows keep natural sweep order
+  std::vector<int> cnt(maxl + 2, 0);
+  for (int i = 0; i < n; ++i) cnt[lvl[i] + 1]++;
+  for (int l = 0; l <= maxl; ++l) cnt[l + 1] += cnt[l];
+  order.assign(n, 0);
+  if (ascending)
+    for (int i = 0; i < n; ++i) order[cnt[lvl[i]]++] = i;
+  else
+    for (int i = n - 1; i >= 0; --i) order[cnt[lvl[i]]++] = i;
+  return maxl + 1;
+}
+
+template <typename T> static int upload(DevBuf<T>& d, const std::vector<T>& v) {
+  BSP_TRY(d.alloc(v.empty() ? 1 : v.size()));
+  if (!v.empty())
+    BSP_CUDA_TRY(cudaMemcpy(d.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return BSP_OK;
+}
+
+static int read_status(bsp_handle_s* h, DevStatus* out) {
+  BSP_CUDA_TRY(cudaMemcpyAsync(out, h->ws.status.get(), sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                               h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (out->code != 0) {
+    BSP_CUDA_TRY(cudaMemsetAsync(h->ws.status.get(), 0, sizeof(DevStatus), h->stream));
+    BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  return BSP_OK;
+}
+
+// Persistent grid for a kernel: SMs x resident CTAs.
+template <class K> static int persistent_grid(const bsp_handle_s* h, K kernel, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return h->num_sms * per_sm;
+}
+
+static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* ptr, const int* col,
+                      const int* diag, double* vals, int n) {
+  bsp_handle_s* h = pc->h;
+  FactorP fp;
+  fp.n = n;
+  fp.bs = pc->bs;
+  fp.mode = mode;
+  fp.order = order;
+  fp.ptr = ptr;
+  fp.col = col;
+  fp.diag = diag;
+  fp.vals = vals;
+  fp.dinv = pc->dinv.get();
+  fp.flags = pc->flags.get();
+  fp.epoch = ++h->epoch;
+  fp.ticket = pc->ticket.get();
+  fp.st = h->ws.status.get();
+  const size_t smem = (size_t)kFactorWarps * 5 * pc->bs * pc->bs * sizeof(double);
+  BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BSP_CUDA_TRY(cudaMemsetAsync(pc->ticket.get(), 0, sizeof(unsigned), h->stream));
+  const int grid = persistent_grid(h, k_factor, kFactorWarps * 32, smem);
+  k_factor<<<grid, kFactorWarps * 32, smem, h->stream>>>(fp);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  DevStatus st;
+  BSP_TRY(read_status(h, &st));
+  if (st.code != 0) {
+    record_error(std::string("preconditioner set-up: ") + bsp_status_string(st.code) +
+                 " at block row " + std::to_string(st.where));
+    return st.code;
+  }
+  return BSP_OK;
+}
+
+// ---------------------------------------------------------------- sweep launch
+template <int BS, typename VT, typename AT, bool TRANS, int POST>
+static int launch_sweep_t(bsp_handle_s* h, const SweepP<VT, AT>& p) {
+  static int grid = 0;
+  if (!grid) grid = persistent_grid(h, k_sweep<BS, VT, AT, TRANS, POST>, kSweepThreads, 0);
+  k_sweep<BS, VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p);
+  return BSP_OK;
+}
+
+template <typename VT, typename AT, bool TRANS, int POST>
+static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* ticket) {
+  p.epoch = ++h->epoch;
+  p.ticket = ticket;
+  p.st = h->ws.status.get();
+  BSP_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), h->stream));
+  constexpr int V = Chunk<VT>::V;
+  bool done = false;
+#define BSP_SWEEP_CASE(B)                                          \
+  case B:                                                          \
+    if constexpr (B % V == 0) {                                    \
+      launch_sweep_t<B, VT, AT, TRANS, POST>(h, p);                \
+      done = true;                                                 \
+    }                                                              \
+    break;
+  switch (bs) {
+    BSP_SWEEP_CASE(2)
+    BSP_SWEEP_CASE(4)
+    BSP_SWEEP_CASE(8)
+    BSP_SWEEP_CASE(16)
+    BSP_SWEEP_CASE(32)
+    default: break;
+  }
+#undef BSP_SWEEP_CASE
+  if (!done) {
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(h, k_sweep_generic<VT, AT, TRANS, POST>, kSweepThreads, 0);
+    k_sweep_generic<VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p, bs);
+  }
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+// ---------------------------------------------------------------- build
+static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
+  const bsp_matrix_s* A = pc->A;
+  const int n = A->n_rows;
+  std::vector<int> ptr(n + 1, 0), col, diag(n, -1);
+  std::vector<int64_t> perm;
+  col.reserve(A->nnzb);
+  perm.reserve(A->nnzb);
+  std::vector<std::pair<int, int64_t>> row;
+  for (int i = 0; i < n; ++i) {
+    row.clear();
+    for (int t = A->h_row_ptr[i]; t < A->h_row_ptr[i + 1]; ++t) {
+      const int j = A->h_col_idx[t];
+      if (!lower_only || j <= i) row.emplace_back(j, t);
+    }
+    std::sort(row.begin(), row.end());
+    for (auto& pr : row) {
+      if (pr.first == i) diag[i] = (int)col.size();
+      col.push_back(pr.first);
+      perm.push_back(pr.second);
+    }
+    ptr[i + 1] = (int)col.size();
+    if (diag[i] < 0) {
+      record_error("block row " + std::to_string(i) + " has no diagonal block");
+      return BSP_ZERO_PIVOT;
+    }
+  }
+  pc->f_nnzb = (int64_t)col.size();
+  pc->h_perm = perm;
+  BSP_TRY(upload(pc->f_ptr, ptr));
+  BSP_TRY(upload(pc->f_col, col));
+  BSP_TRY(upload(pc->f_diag, diag));
+  BSP_TRY(upload(pc->d_perm, perm));
+  const int b2 = pc->bs * pc->bs;
+  BSP_TRY(pc->f_vals.alloc(pc->f_nnzb * b2));
+  k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
+      pc->f_nnzb, b2, pc->d_perm.get(), A->vals.get(), pc->f_vals.get());
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  // level orders on the sorted structure
+  std::vector<int> order;
+  pc->n_lev_lo = level_order(n, true, [&](int i, auto&& f) {
+    for (int e = ptr[i]; e < diag[i]; ++e) f(col[e]);
+  }, order);
+  BSP_TRY(upload(pc->order_lo, order));
+  if (!lower_only) {
+    pc->n_lev_up = level_order(n, false, [&](int i, auto&& f) {
+      for (int e = diag[i] + 1; e < ptr[i + 1]; ++e) f(col[e]);
+    }, order);
+    BSP_TRY(upload(pc->order_up, order));
+  } else {
+    // L^T backward: row i depends on rows j > i with L_ji present
+    std::vector<int> tp(n + 1, 0);
+    for (int j = 0; j < n; ++j)
+      for (int e = ptr[j]; e < diag[j]; ++e) tp[col[e] + 1]++;
+    for (int i = 0; i < n; ++i) tp[i + 1] += tp[i];
+    std::vector<int> trow(tp[n]);
+    std::vector<int64_t> tblk(tp[n]);
+    std::vector<int> fill(tp.begin(), tp.end() - 1);
+    for (int j = 0; j < n; ++j)
+      for (int e = ptr[j]; e < diag[j]; ++e) {
+        const int i = col[e];
+        trow[fill[i]] = j;
+        tblk[fill[i]] = e;
+        fill[i]++;
+      }
+    pc->n_lev_up = level_order(n, false, [&](int i, auto&& f) {
+      for (int t = tp[i]; t < tp[i + 1]; ++t) f(trow[t]);
+    }, order);
+    BSP_TRY(upload(pc->order_up, order));
+    BSP_TRY(upload(pc->t_ptr, tp));
+    BSP_TRY(upload(pc->t_row, trow));
+    BSP_TRY(upload(pc->t_blk, tblk));
+  }
+  return BSP_OK;
+}
+
+static int build_diag_inverse(bsp_precond_s* pc) {
+  const bsp_matrix_s* A = pc->A;
+  const int n = A->n_rows;
+  std::vector<int> diag(n, -1);
+  for (int i = 0; i < n; ++i) {
+    for (int t = A->h_row_ptr[i]; t < A->h_row_ptr[i + 1]; ++t)
+      if (A->h_col_idx[t] == i) diag[i] = t;
+    if (diag[i] < 0) {
+      record_error("block row " + std::to_string(i) + " has no diagonal block");
+      return BSP_ZERO_PIVOT;
+    }
+  }
+  BSP_TRY(upload(pc->a_diag, diag));
+  if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL) {
+    std::vector<int> order;
+    const auto& rp = A->h_row_ptr;
+    const auto& ci = A->h_col_idx;
+    pc->n_lev_lo = level_order(n, true, [&](int i, auto&& f) {
+      for (int t = rp[i]; t < rp[i + 1]; ++t)
+        if (ci[t] < i) f(ci[t]);
+    }, order);
+    BSP_TRY(upload(pc->order_lo, order));
+    pc->n_lev_up = level_order(n, false, [&](int i, auto&& f) {
+      for (int t = rp[i]; t < rp[i + 1]; ++t)
+        if (ci[t] > i) f(ci[t]);
+    }, order);
+    BSP_TRY(upload(pc->order_up, order));
+  }
+  // makeADInv: invert every diagonal block (rows independent)
+  return run_factor(pc, FACT_DIAG, nullptr, A->row_ptr.get(), A->col_idx.get(), pc->a_diag.get(),
+                    A->vals.get(), n);
+}
+
+static int make_lowp_copies(bsp_precond_s* pc) {
+  if (pc->precision == BSP_PREC_F64) return BSP_OK;
+  const int b2 = pc->bs * pc->bs;
+  const int64_t nd = (int64_t)pc->n * b2;
+  const int64_t nf = pc->f_nnzb * b2;
+  if (pc->precision == BSP_PREC_F32) {
+    BSP_TRY(pc->dinv32.alloc(nd));
+    k_convert<float><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv32.get());
+    if (nf > 0) {
+      BSP_TRY(pc->f_vals32.alloc(nf));
+      k_convert<float><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals32.get());
+    }
+  } else {
+    BSP_TRY(pc->dinv16.alloc(nd));
+    k_convert<__nv_bfloat16><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv16.get());
+    if (nf > 0) {
+      BSP_TRY(pc->f_vals16.alloc(nf));
+      k_convert<__nv_bfloat16><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals16.get());
+    }
+  }
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+int precond_build(bsp_precond_s* pc) {
+  const int n = pc->n, b2 = pc->bs * pc->bs;
+  BSP_TRY(pc->dinv.alloc((size_t)std::max(n, 1) * b2));
+  BSP_TRY(pc->flags.alloc(std::max(n, 1)));
+  BSP_TRY(pc->ticket.alloc(1));
+  BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
+  switch (pc->kind) {
+    case BSP_PC_NONE:
+      return BSP_OK;
+    case BSP_PC_DIAG_LU:
+    case BSP_PC_DIAG_CHOL:
+    case BSP_PC_SOR_LU:
+    case BSP_PC_SOR_CHOL:
+      BSP_TRY(build_diag_inverse(pc));
+      if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL) {
+        BSP_TRY(pc->sor_a.alloc((size_t)n * pc->bs));
+        BSP_TRY(pc->sor_b.alloc((size_t)n * pc->bs));
+      }
+      break;
+    case BSP_PC_ILU0:
+      BSP_TRY(build_factor_structure(pc, false));
+      BSP_TRY(run_factor(pc, FACT_ILU0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(),
+                         pc->f_diag.get(), pc->f_vals.get(), n));
+      break;
+    case BSP_PC_ICHOL0:
+      BSP_TRY(build_factor_structure(pc, true));
+      BSP_TRY(run_factor(pc, FACT_ICHOL0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(),
+                         pc->f_diag.get(), pc->f_vals.get(), n));
+      break;
+    default:
+      record_error("unknown preconditioner kind");
+      return BSP_INVALID;
+  }
+  return make_lowp_copies(pc);
+}
+
+// ---------------------------------------------------------------- apply
+// z = M^{-1} r (z may alias r).  AT = double (FP64) or float (mixed precision).
+template <typename VT, typename AT>
+static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, const VT* dinv,
+                       const VT* avals, AT* sa, AT* sb) {
+  bsp_handle_s* h = pc->h;
+  const bsp_matrix_s* A = pc->A;
+  const int n = pc->n, bs = pc->bs;
+  unsigned* tk = pc->ticket.get();
+  SweepP<VT, AT> p{};
+  p.n = n;
+  p.flags = pc->flags.get();
+  switch (pc->kind) {
+    case BSP_PC_NONE:
+      if (z != r) BSP_CUDA_TRY(cudaMemcpyAsync(z, r, (size_t)n * bs * sizeof(AT), cudaMemcpyDeviceToDevice, h->stream));
+      return BSP_OK;
+    case BSP_PC_DIAG_LU:
+    case BSP_PC_DIAG_CHOL:
+      p.range = RANGE_NONE;
+      p.dinv = dinv;
+      p.rhs = r;
+      p.x = z;
+      p.vals = avals;
+      return launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk);
+    case BSP_PC_SOR_LU:
+    case BSP_PC_SOR_CHOL: {
+      // operator() (preconditioners.hpp:227-234): x = 0; nu backward, or nu
+      // forward + nu backward, or nu forward sweeps; r = x.
+      p.ptr = A->row_ptr.get();
+      p.idx = A->col_idx.get();
+      p.range = RANGE_SPLIT;
+      p.vals = avals;
+      p.dinv = dinv;
+      p.rhs = r;
+      p.w = (AT)pc->w;
+      std::vector<int> dirs;
+      if (pc->type < 0) dirs.assign(pc->nu, +1);
+      else if (pc->type == 0) { dirs.assign(pc->nu, -1); dirs.insert(dirs.end(), pc->nu, +1); }
+      else dirs.assign(pc->nu, -1);
+      const AT* xold = nullptr;
+      AT* bufs[2] = {sa, sb};
+      for (size_t s = 0; s < dirs.size(); ++s) {
+        const bool last = s + 1 == dirs.size();
+        AT* out = last ? z : bufs[s & 1];
+        if (last && z == r && xold == nullptr) out = bufs[s & 1];  // nu == 1 in place: keep rhs intact
+        p.dep_dir = dirs[s];
+        p.order = dirs[s] < 0 ? pc->order_lo.get() : pc->order_up.get();
+        p.xold = xold;
+        p.x = out;
+        BSP_TRY((launch_sweep<VT, AT, false, POST_SOR>(h, bs, p, tk)));
+        xold = out;
+      }
+      if (xold != z)
+        BSP_CUDA_TRY(cudaMemcpyAsync(z, xold, (size_t)n * bs * sizeof(AT), cudaMemcpyDeviceToDevice, h->stream));
+      return BSP_OK;
+    }
+    case BSP_PC_ILU0:
+    case BSP_PC_LEARNED_LU: {
+      p.ptr = pc->f_ptr.get();
+      p.idx = pc->f_col.get();
+      p.diag = pc->f_diag.get();
+      p.vals = fvals;
+      p.dinv = dinv;
+      // forward: unit L
+      p.range = RANGE_LOWER;
+      p.order = pc->order_lo.get();
+      p.rhs = r;
+      p.x = z;
+      BSP_TRY((launch_sweep<VT, AT, false, POST_NONE>(h, bs, p, tk)));
+      // backward: U with inverted diagonal
+      p.range = RANGE_UPPER;
+      p.order = pc->order_up.get();
+      p.rhs = z;
+      p.x = z;
+      return launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk);
+    }
+    case BSP_PC_ICHOL0:
+    case BSP_PC_LEARNED_LLT: {
+      p.ptr = pc->f_ptr.get();
+      p.idx = pc->f_col.get();
+      p.diag = pc->f_diag.get();
+      p.vals = fvals;
+      p.dinv = dinv;
+      p.range = RANGE_LOWER;
+      p.order = pc->order_lo.get();
+      p.rhs = r;
+      p.x = z;
+      BSP_TRY((launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk)));
+      // backward: L^T through the transposed structure, diagonal L_ii^{-T}
+      p.ptr = pc->t_ptr.get();
+      p.idx = pc->t_row.get();
+      p.blk = pc->t_blk.get();
+      p.range = RANGE_ALL;
+      p.order = pc->order_up.get();
+      p.rhs = z;
+      p.x = z;
+      return launch_sweep<VT, AT, true, POST_DT>(h, bs, p, tk);
+    }
+    default:
+      return BSP_INVALID;
+  }
+}
+
+int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z) {
+  if (precision == BSP_PREC_F64) {
+    return apply_typed<double, double>(pc, (const double*)r, (double*)z, pc->f_vals.get(),
+                                       pc->dinv.get(), pc->A->vals.get(), pc->sor_a.get(),
+                                       pc->sor_b.get());
+  }
+  const size_t nv = (size_t)pc->n * pc->bs;
+  if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL) {
+    if (pc->sor_a32.n < nv) {
+      BSP_TRY(pc->sor_a32.alloc(nv));
+      BSP_TRY(pc->sor_b32.alloc(nv));
+    }
+  }
+  if (precision == BSP_PREC_F32) {
+    if (!pc->dinv32.get()) return BSP_INVALID;
+    return apply_typed<float, float>(pc, (const float*)r, (float*)z, pc->f_vals32.get(),
+                                     pc->dinv32.get(), pc->A->vals32.get(), pc->sor_a32.get(),
+                                     pc->sor_b32.get());
+  }
+  if (!pc->dinv16.get()) return BSP_INVALID;
+  return apply_typed<__nv_bfloat16, float>(pc, (const float*)r, (float*)z, pc->f_vals16.get(),
+                                           pc->dinv16.get(), pc->A->vals16.get(),
+                                           pc->sor_a32.get(), pc->sor_b32.get());
+}
+
+int precond_check_status(bsp_precond_s* pc) {
+  DevStatus st;
+  BSP_TRY(read_status(pc->h, &st));
+  if (st.code != 0) {
+    record_error(std::string("preconditioner apply: ") + bsp_status_string(st.code) +
+                 " at block row " + std::to_string(st.where));
+    return st.code;
+  }
+  return BSP_OK;
+}
+
+}  // namespace bsp
+
+// ================================================================= C ABI
+extern "C" {
+
+int bsp_precond_create(bsp_handle_t h, bsp_matrix_t A, const bsp_precond_params* params,
+                       bsp_precond_t* out) {
+  if (!h || !A || !params || !out) return BSP_INVALID;
+  *out = nullptr;
+  if (A->n_rows != A->n_cols) {
+    record_error("preconditioners need a square matrix");
+    return BSP_INVALID;
+  }
+  if (A->bs > 32) {
+    record_error("preconditioners support block sizes up to 32");
+    return BSP_INVALID;
+  }
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  auto pc = std::make_unique<bsp_precond_s>();
+  pc->h = h;
+  pc->device = h->device;
+  pc->A = A;
+  pc->kind = params->kind;
+  pc->n = A->n_rows;
+  pc->bs = A->bs;
+  pc->w = params->sor_w;
+  pc->nu = params->sor_nu;
+  pc->type = params->sor_type;
+  pc->precision = params->precision;
+  if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL) {
+    if (pc->nu < 1) {
+      record_error("SOR needs nu >= 1");
+      return BSP_INVALID;
+    }
+  }
+  if (pc->precision != BSP_PREC_F64) {
+    BSP_TRY(bsp_matrix_make_lowp(A, pc->precision == BSP_PREC_F32 ? BSP_F32 : BSP_BF16));
+  }
+  BSP_TRY(precond_build(pc.get()));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = pc.release();
+  return BSP_OK;
+}
+
+int bsp_precond_destroy(bsp_precond_t pc) {
+  if (!pc) return BSP_OK;
+  cudaSetDevice(pc->device);
+  delete pc;
+  return BSP_OK;
+}
+
+int bsp_precond_apply_dev(bsp_handle_t h, bsp_precond_t pc, double* r) {
+  if (!h || !pc || !r) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  return precond_apply(pc, BSP_PREC_F64, r, r);
+}
+
+int bsp_precond_apply(bsp_handle_t h, bsp_precond_t pc, double* r_host) {
+  if (!h || !pc || !r_host) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  const size_t nv = (size_t)pc->n * pc->bs;
+  BSP_TRY(h->stage(nv, 1));
+  double* d = h->stage_in.get();
+  BSP_CUDA_TRY(cudaMemcpyAsync(d, r_host, nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  BSP_TRY(precond_apply(pc, BSP_PREC_F64, d, d));
+  BSP_CUDA_TRY(cudaMemcpyAsync(r_host, d, nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return precond_check_status(pc);
+}
+
+int bsp_precond_export(bsp_precond_t pc, double* vals_host, int64_t capacity) {
+  if (!pc || !vals_host) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(pc->device));
+  const int b2 = pc->bs * pc->bs;
+  bsp_handle_s* h = pc->h;
+  if (pc->kind == BSP_PC_ILU0 || pc->kind == BSP_PC_ICHOL0) {
+    // blocks in the caller's layout: ILU0 in A's block order; IChol0 in the
+    // order of A.lowTri() (A's rows, blocks with col <= row in stored order)
+    const int64_t nf = pc->f_nnzb;
+    if (capacity < nf * b2) return BSP_INVALID;
+    std::vector<double> f(nf * b2);
+    BSP_CUDA_TRY(cudaMemcpy(f.data(), pc->f_vals.get(), f.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if (pc->kind == BSP_PC_ILU0) {
+      for (int64_t e = 0; e < nf; ++e)
+        std::copy(f.begin() + e * b2, f.begin() + (e + 1) * b2, vals_host + pc->h_perm[e] * b2);
+    } else {
+      // rank of each A block among the lower blocks of its row, in A order
+      std::vector<int64_t> low_pos(pc->A->nnzb, -1);
+      int64_t c = 0;
+      for (int i = 0; i < pc->n; ++i)
+        for (int t = pc->A->h_row_ptr[i]; t < pc->A->h_row_ptr[i + 1]; ++t)
+          if (pc->A->h_col_idx[t] <= i) low_pos[t] = c++;
+      for (int64_t e = 0; e < nf; ++e)
+        std::copy(f.begin() + e * b2, f.begin() + (e + 1) * b2, vals_host + low_pos[pc->h_perm[e]] * b2);
+    }
+  } else {
+    if (capacity < (int64_t)pc->n * b2) return BSP_INVALID;
+    BSP_CUDA_TRY(cudaMemcpy(vals_host, pc->dinv.get(), (size_t)pc->n * b2 * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  (void)h;
+  return BSP_OK;
+}
+
+int bsp_precond_info(bsp_precond_t pc, int* kind, int* n_levels_lower, int* n_levels_upper,
+                     int64_t* factor_nnzb) {
+  if (!pc) return BSP_INVALID;
+  if (kind) *kind = pc->kind;
+  if (n_levels_lower) *n_levels_lower = pc->n_lev_lo;
+  if (n_levels_upper) *n_levels_upper = pc->n_lev_up;
+  if (factor_nnzb) *factor_nnzb = pc->f_nnzb;
+  return BSP_OK;
+}
+
+}  // extern "C"

@@ -36,7 +36,8 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out)
   }
 }
 
-// Body: __device__ void operator()(int64_t i, double (&acc)[NV]) for element i.
+// Body: __device__ void setup() once per thread (loads device scalars), then
+//       __device__ void operator()(int64_t i, double (&acc)[NV]) for element i.
 // Fin:  __device__ void operator()(const double (&sum)[NV]) on one thread.
 template <int NV, class Body, class Fin>
 __global__ void __launch_bounds__(kRedThreads)
@@ -45,7 +46,9 @@ k_reduce(int64_t n, Body body, Fin fin, double* partials, unsigned* ticket) {
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) body(i, acc);
+  Body b = body;
+  b.setup();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) b(i, acc);
   __shared__ double blk[NV];
   block_reduce_store<NV>(acc, blk);
   __shared__ bool last;
@@ -89,6 +92,7 @@ inline int launch_reduce(bsp_handle_s* h, int slot, int64_t n, Body body, Fin fi
 struct DotBody {
   const double* x;
   const double* y;
+  __device__ void setup() {}
   __device__ void operator()(int64_t i, double (&a)[1]) const { a[0] = fma(x[i], y[i], a[0]); }
 };
 struct StoreFin {

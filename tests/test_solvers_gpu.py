@@ -1,0 +1,140 @@
+"""Solver parity: GPU pCG / pGMRES(-DR) against the CPU oracle on the same seeded systems.
+
+Parity criteria (FP64): iteration count equal to the oracle's within +-1
+(pCG, unrestarted pGMRES) or +-2 (deflated restart); the residual history
+normalised by its first entry agrees with the oracle's within 1e-10 absolute
+at every step both histories have; the solution agrees within 1e-8 relative
+(infinity norm); the reported FP64 true residual matches the oracle's x.
+"""
+import numpy as np
+import pytest
+
+from blocksp_b200.systems import grid_system
+import oracle.blocksp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300)
+
+
+def check_parity(x, info, hist, ref, it_slack, x_tol=1e-8, h_tol=1e-10):
+    assert abs(info["iters"] - ref.iters) <= it_slack, (info["iters"], ref.iters)
+    h = np.asarray(hist) / hist[0]
+    r = np.asarray(ref.hist) / ref.hist[0]
+    n = min(len(h), len(r))
+    assert n >= 2
+    assert np.abs(h[:n] - r[:n]).max() <= h_tol
+    assert rel(x, ref.x) <= x_tol
+
+
+def setup_system(handle, dims, bs, skew, seed):
+    import blocksp_b200 as bsp
+    s = grid_system(dims, bs, seed=seed, skew=skew)
+    return s, bsp.Matrix.from_system(s, handle), O.BSR.from_system(s)
+
+
+@pytest.mark.parametrize("dims,bs", [((16, 16), 4), ((10, 10), 2), ((6, 6, 6), 8), ((7, 7), 3)])
+def test_pcg_ichol0(handle, dims, bs):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, dims, bs, 0.0, 21)
+    x, info, hist = bsp.pCG(A, s.b, 1e-10, bsp.IChol0(A), 2000, return_info=True)
+    ref = O.pcg(Ao, s.b, 1e-10, O.IChol0(Ao), 2000)
+    assert info["status"] == 0
+    check_parity(x, info, hist, ref, 1)
+    assert abs(info["true_rel_res"] - O.true_rel_residual(Ao, s.b, x)) <= 1e-12
+
+
+@pytest.mark.parametrize("pre", ["none", "diag", "ssor_chol"])
+def test_pcg_other_preconditioners(handle, pre):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (12, 12), 4, 0.0, 22)
+    if pre == "none":
+        pc, pr = None, O.no_pre
+    elif pre == "diag":
+        pc, pr = bsp.Diag(A, "Chol"), O.Diag(Ao, O.CholeskyFactor)
+    else:
+        pc, pr = bsp.SOR(A, 1.6, 3, 0, "Chol"), O.SOR(Ao, 1.6, 3, 0, O.CholeskyFactor)
+    x, info, hist = bsp.pCG(A, s.b, 1e-10, pc, 2000, return_info=True)
+    ref = O.pcg(Ao, s.b, 1e-10, pr, 2000)
+    check_parity(x, info, hist, ref, 1)
+
+
+@pytest.mark.parametrize("restart,k,slack", [(-1, -1, 1), (30, 10, 2), (10, 4, 2), (8, 0, 1)])
+def test_pgmres_ilu0(handle, restart, k, slack):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (6, 6, 6), 8, 0.3, 23)
+    x, info, hist = bsp.pGMRES(A, s.b, 1e-10, bsp.ILU0(A), 5000, restart, k, return_info=True)
+    ref = O.pgmres(Ao, s.b, 1e-10, O.ILU0(Ao), 5000, restart, k)
+    assert info["status"] == 0
+    assert info["n_restarts"] == ref.restarts or restart > 0 and abs(info["n_restarts"] - ref.restarts) <= 1
+    check_parity(x, info, hist, ref, slack)
+
+
+@pytest.mark.parametrize("restart,k", [(-1, -1), (12, 5)])
+def test_pgmres_sor(handle, restart, k):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (8, 8), 4, 0.3, 24)
+    x, info, hist = bsp.pGMRES(A, s.b, 1e-10, bsp.SOR(A, 1.6, 3, 0), 5000, restart, k, return_info=True)
+    ref = O.pgmres(Ao, s.b, 1e-10, O.SOR(Ao, 1.6, 3, 0), 5000, restart, k)
+    check_parity(x, info, hist, ref, 2)
+
+
+def test_pgmres_bs16_dr(handle):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (4, 4, 4), 16, 0.3, 25)
+    x, info, hist = bsp.pGMRES(A, s.b, 1e-10, bsp.ILU0(A), 5000, 10, 4, return_info=True)
+    ref = O.pgmres(Ao, s.b, 1e-10, O.ILU0(Ao), 5000, 10, 4)
+    check_parity(x, info, hist, ref, 2)
+
+
+def test_device_and_host_paths_agree(handle, torch_cuda):
+    import blocksp_b200 as bsp
+    torch = torch_cuda
+    s, A, Ao = setup_system(handle, (10, 10), 4, 0.0, 26)
+    pc = bsp.IChol0(A)
+    xh = bsp.pCG(A, s.b, 1e-10, pc, 1000)
+    xd = bsp.pCG(A, torch.tensor(s.b, device="cuda"), 1e-10, pc, 1000)
+    assert np.array_equal(xh, xd.cpu().numpy())  # deterministic reductions
+
+
+def test_solver_structs_and_ez(handle):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (6, 6, 5), 8, 0.0, 27)
+    for x in (bsp.ILU0_pGMRES(A, 1e-10, 5000, 30, 10).solve(A, s.b),
+              bsp.IChol0_pCG(A, 1e-10).solve(A, s.b),
+              bsp.SOR_pGMRES(A).solve(A, s.b), bsp.SOR_pCG(A).solve(A, s.b),
+              bsp.ez.ilu0_pGMRES_dr(A, s.b), bsp.ez.sor_pGMRES_robust(A, s.b), bsp.ez.ichol0_pCG(A, s.b)):
+        assert O.true_rel_residual(Ao, s.b, x) < 1e-7
+
+
+def test_maxit_status_and_count(handle):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (16, 16), 4, 0.0, 28)
+    x, info, hist = bsp.pCG(A, s.b, 1e-14, None, 5, return_info=True)
+    ref = O.pcg(Ao, s.b, 1e-14, O.no_pre, 5)
+    assert info["status"] == 4 and info["iters"] == ref.iters == 6
+    x, info, hist = bsp.pGMRES(A, s.b, 1e-14, None, 7, return_info=True)
+    ref = O.pgmres(Ao, s.b, 1e-14, O.no_pre, 7)
+    assert info["status"] == 4 and info["iters"] == ref.iters
+
+
+def test_nan_rhs_is_reported(handle):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (6, 6), 4, 0.0, 29)
+    b = s.b.copy()
+    b[5] = np.nan
+    x, info, hist = bsp.pCG(A, b, 1e-10, bsp.IChol0(A), 100, return_info=True)
+    assert info["status"] == 5  # BSP_NAN
+    x, info, hist = bsp.pGMRES(A, b, 1e-10, bsp.ILU0(A), 100, return_info=True)
+    assert info["status"] == 5
+
+
+def test_zero_rhs_returns_zero(handle):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (6, 6), 4, 0.0, 30)
+    x = bsp.pCG(A, np.zeros_like(s.b), 1e-10, bsp.IChol0(A), 100)
+    assert not np.any(x)
+    x = bsp.pGMRES(A, np.zeros_like(s.b), 1e-10, bsp.ILU0(A), 100)
+    assert not np.any(x)
