@@ -90,8 +90,9 @@ def test_device_apply_in_place(handle, torch_cuda):
 
 def test_zero_diagonal_block_is_reported(handle):
     import blocksp_b200 as bsp
+    # row 0 has no lower neighbours, so its ILU0 pivot block is A_00 itself
     s = grid_system((5, 5), 4, seed=2)
-    d = [t for t in range(s.row_ptr[7], s.row_ptr[8]) if s.col_idx[t] == 7][0]
+    d = [t for t in range(s.row_ptr[0], s.row_ptr[1]) if s.col_idx[t] == 0][0]
     s.vals[d] = 0.0
     A = bsp.Matrix.from_system(s, handle)
     for make in (bsp.ILU0, lambda M: bsp.Diag(M, "LU"), lambda M: bsp.SOR(M, 1.0, 1)):

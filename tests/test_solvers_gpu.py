@@ -1,10 +1,17 @@
 """Solver parity: GPU pCG / pGMRES(-DR) against the CPU oracle on the same seeded systems.
 
 Parity criteria (FP64): iteration count equal to the oracle's within +-1
-(pCG, unrestarted pGMRES) or +-2 (deflated restart); the residual history
-normalised by its first entry agrees with the oracle's within 1e-10 absolute
-at every step both histories have; the solution agrees within 1e-8 relative
-(infinity norm); the reported FP64 true residual matches the oracle's x.
+(pCG, unrestarted pGMRES) or +-2 (deflated restart); the solution agrees within
+1e-8 relative (infinity norm); the reported FP64 true residual matches the
+oracle's x.  Residual history, normalised by its first entry:
+  * pGMRES: within 1e-10 absolute at every step both histories have;
+  * pCG: within 1e-10 absolute plus 30x the oracle's own rounding envelope at
+    that step.  CG's recursive residual is chaotic at rounding level: the
+    oracle run twice with its preconditioner output perturbed by 1e-15
+    relative already moves the normalised history by up to ~1e-8 (relative
+    1e-3 in stagnation phases) while x agrees to 1e-14, so a fixed 1e-10 bound
+    would reject the reference against itself.  The envelope is measured per
+    step from three such perturbed oracle runs.
 """
 import numpy as np
 import pytest
@@ -19,14 +26,40 @@ def rel(a, b):
     return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300)
 
 
-def check_parity(x, info, hist, ref, it_slack, x_tol=1e-8, h_tol=1e-10):
+def check_parity(x, info, hist, ref, it_slack, x_tol=1e-8, h_tol=1e-10, envelope=None):
     assert abs(info["iters"] - ref.iters) <= it_slack, (info["iters"], ref.iters)
     h = np.asarray(hist) / hist[0]
     r = np.asarray(ref.hist) / ref.hist[0]
     n = min(len(h), len(r))
     assert n >= 2
-    assert np.abs(h[:n] - r[:n]).max() <= h_tol
+    allowed = np.full(n, h_tol)
+    if envelope is not None:
+        m = min(n, len(envelope))
+        allowed[:m] += 30.0 * envelope[:m]
+        allowed[m:] += 30.0 * (envelope.max() if len(envelope) else 0.0)
+    dev = np.abs(h[:n] - r[:n])
+    assert np.all(dev <= allowed), (int(np.argmax(dev - allowed)), float(dev.max()))
     assert rel(x, ref.x) <= x_tol
+
+
+def cg_envelope(Ao, b, tol, pre, max_iters, ref, trials=3, eps=1e-15):
+    """Per-step spread of the oracle's normalised pCG history under
+    rounding-level perturbations of its preconditioner output."""
+    r = np.asarray(ref.hist) / ref.hist[0]
+    env = np.zeros(len(r))
+    for t in range(trials):
+        rng = np.random.default_rng(100 + t)
+
+        def pert(v):
+            y = pre(v)
+            return y * (1.0 + eps * rng.standard_normal(y.shape))
+        o = O.pcg(Ao, b, tol, pert, max_iters)
+        h = np.asarray(o.hist) / o.hist[0]
+        n = min(len(h), len(r))
+        env[:n] = np.maximum(env[:n], np.abs(h[:n] - r[:n]))
+        if n < len(r):
+            env[n:] = np.maximum(env[n:], r[n:])
+    return env
 
 
 def setup_system(handle, dims, bs, skew, seed):
@@ -40,9 +73,10 @@ def test_pcg_ichol0(handle, dims, bs):
     import blocksp_b200 as bsp
     s, A, Ao = setup_system(handle, dims, bs, 0.0, 21)
     x, info, hist = bsp.pCG(A, s.b, 1e-10, bsp.IChol0(A), 2000, return_info=True)
-    ref = O.pcg(Ao, s.b, 1e-10, O.IChol0(Ao), 2000)
+    ic = O.IChol0(Ao)
+    ref = O.pcg(Ao, s.b, 1e-10, ic, 2000)
     assert info["status"] == 0
-    check_parity(x, info, hist, ref, 1)
+    check_parity(x, info, hist, ref, 1, envelope=cg_envelope(Ao, s.b, 1e-10, ic, 2000, ref))
     assert abs(info["true_rel_res"] - O.true_rel_residual(Ao, s.b, x)) <= 1e-12
 
 
@@ -58,7 +92,7 @@ def test_pcg_other_preconditioners(handle, pre):
         pc, pr = bsp.SOR(A, 1.6, 3, 0, "Chol"), O.SOR(Ao, 1.6, 3, 0, O.CholeskyFactor)
     x, info, hist = bsp.pCG(A, s.b, 1e-10, pc, 2000, return_info=True)
     ref = O.pcg(Ao, s.b, 1e-10, pr, 2000)
-    check_parity(x, info, hist, ref, 1)
+    check_parity(x, info, hist, ref, 1, envelope=cg_envelope(Ao, s.b, 1e-10, pr, 2000, ref))
 
 
 @pytest.mark.parametrize("restart,k,slack", [(-1, -1, 1), (30, 10, 2), (10, 4, 2), (8, 0, 1)])
