@@ -70,6 +70,7 @@ __device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, i
     int bidx = k;
     if (lane >= k && lane < bs) {
       best = fabs(aug[lane * w + k]);
+      if (best != best) best = -0.5;  // NaN never wins the comparison below
       bidx = lane;
     }
 #pragma unroll
@@ -78,6 +79,11 @@ __device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, i
       const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
       if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
     }
+    // Every lane must take the same pivot: the row swap below is a branch that
+    // contains __syncwarp().  Broadcast lane 0's choice so the control flow is
+    // warp-uniform whatever the values (NaN or Inf from a failed block).
+    best = __shfl_sync(0xffffffffu, best, 0);
+    bidx = __shfl_sync(0xffffffffu, bidx, 0);
     if (!(best > 0.0) || !isfinite(best)) ok = false;
     if (bidx != k) {
       for (int c = lane; c < w; c += 32) {

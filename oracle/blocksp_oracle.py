@@ -366,9 +366,12 @@ class SolveResult:
     restarts: int = 0
 
 
-def pcg(A: BSR, b: np.ndarray, tol: float, pre=no_pre, max_iters: int = 1000) -> SolveResult:
+def pcg(A: BSR, b: np.ndarray, tol: float, pre=no_pre, max_iters: int = 1000,
+        matvec=None) -> SolveResult:
     """pCG (solvers.hpp:51-105), including its mixed stopping test: the first
-    history entry is ||M^-1 b|| and later ones are the recursive ||r||."""
+    history entry is ||M^-1 b|| and later ones are the recursive ||r||.
+    ``matvec`` (default: bsmv with A) lets tests perturb the product."""
+    mv = matvec or (lambda v: bsmv(A, v))
     x = np.zeros_like(b)
     r = b.copy()
     p = pre(r.copy())
@@ -377,7 +380,7 @@ def pcg(A: BSR, b: np.ndarray, tol: float, pre=no_pre, max_iters: int = 1000) ->
     tolerance = res[-1] * tol
     it = 0
     while res[-1] > tolerance:
-        Ap = bsmv(A, p)
+        Ap = mv(p)
         rz = dot(r, z)
         alpha = rz / dot(p, Ap)
         x += alpha * p

@@ -5,13 +5,14 @@ Parity criteria (FP64): iteration count equal to the oracle's within +-1
 1e-8 relative (infinity norm); the reported FP64 true residual matches the
 oracle's x.  Residual history, normalised by its first entry:
   * pGMRES: within 1e-10 absolute at every step both histories have;
-  * pCG: within 1e-10 absolute plus 30x the oracle's own rounding envelope at
-    that step.  CG's recursive residual is chaotic at rounding level: the
-    oracle run twice with its preconditioner output perturbed by 1e-15
-    relative already moves the normalised history by up to ~1e-8 (relative
-    1e-3 in stagnation phases) while x agrees to 1e-14, so a fixed 1e-10 bound
-    would reject the reference against itself.  The envelope is measured per
-    step from three such perturbed oracle runs.
+  * pCG: within 1e-10 absolute plus 10x the oracle's own rounding envelope
+    (its running maximum up to that step).  CG's recursive residual is chaotic
+    at rounding level: the oracle rerun with its matrix product and
+    preconditioner output perturbed by 1e-15 relative already moves the
+    normalised history by up to ~1e-7 with IChol0 (~5e-2 without a
+    preconditioner) while x agrees to 1e-14, so a fixed 1e-10 bound would
+    reject the reference against itself.  The envelope is measured from three
+    such perturbed oracle runs.
 """
 import numpy as np
 import pytest
@@ -35,8 +36,9 @@ def check_parity(x, info, hist, ref, it_slack, x_tol=1e-8, h_tol=1e-10, envelope
     allowed = np.full(n, h_tol)
     if envelope is not None:
         m = min(n, len(envelope))
-        allowed[:m] += 30.0 * envelope[:m]
-        allowed[m:] += 30.0 * (envelope.max() if len(envelope) else 0.0)
+        run = np.maximum.accumulate(envelope) if len(envelope) else envelope
+        allowed[:m] += 10.0 * run[:m]
+        allowed[m:] += 10.0 * (run.max() if len(run) else 0.0)
     dev = np.abs(h[:n] - r[:n])
     assert np.all(dev <= allowed), (int(np.argmax(dev - allowed)), float(dev.max()))
     assert rel(x, ref.x) <= x_tol
@@ -50,10 +52,10 @@ def cg_envelope(Ao, b, tol, pre, max_iters, ref, trials=3, eps=1e-15):
     for t in range(trials):
         rng = np.random.default_rng(100 + t)
 
-        def pert(v):
-            y = pre(v)
+        def jitter(y):
             return y * (1.0 + eps * rng.standard_normal(y.shape))
-        o = O.pcg(Ao, b, tol, pert, max_iters)
+        o = O.pcg(Ao, b, tol, lambda v: jitter(pre(v)), max_iters,
+                  matvec=lambda v: jitter(O.bsmv(Ao, v)))
         h = np.asarray(o.hist) / o.hist[0]
         n = min(len(h), len(r))
         env[:n] = np.maximum(env[:n], np.abs(h[:n] - r[:n]))
