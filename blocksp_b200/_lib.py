@@ -75,6 +75,7 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_dot_dev": (_I, [_P, _I64, _P, _P, _P]),
     "bsp_dot": (_I, [_P, _I64, _P, _P, _PD]),
     "bsp_axpy_dev": (_I, [_P, _I64, _D, _P, _P]),
+    "bsp_dot_noalloc": (_I, [_P, _I64, _P, _P, _P]),
     "bsp_precond_create": (_I, [_P, _P, C.POINTER(PrecondParams), C.POINTER(_P)]),
     "bsp_precond_destroy": (_I, [_P]),
     "bsp_precond_apply_dev": (_I, [_P, _P, _P]),

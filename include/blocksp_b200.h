@@ -179,6 +179,17 @@ int bsp_bsmv(bsp_handle_t h, bsp_matrix_t A, int nrhs, int transpose,
 int bsp_dot_dev(bsp_handle_t h, int64_t n, const double* x, const double* y, double* out_dev);
 int bsp_dot(bsp_handle_t h, int64_t n, const double* x_dev, const double* y_dev, double* out_host);
 int bsp_axpy_dev(bsp_handle_t h, int64_t n, double a, const double* x, double* y);
+/* FP64 dot product that allocates nothing; no counterpart in the reference.
+ * For callers that cannot call cudaMalloc where they need the result (code
+ * handed a stream and device pointers by a framework that owns the
+ * allocator), so cannot create a handle.  Stream-ordered on `stream` on the
+ * current device; writes the result to out_dev.  Scratch is a fixed device
+ * array (about 32 KiB per GPU, held until exit): n is limited to 33,554,432
+ * elements and larger n returns BSP_INVALID.  The first call on a device
+ * resolves the scratch address (cudaGetSymbolAddress), so make it before any
+ * stream capture.  Calls share the scratch: calls that overlap on the GPU
+ * race, so serialise them (one stream, or events). */
+int bsp_dot_noalloc(void* stream, int64_t n, const double* x, const double* y, double* out_dev);
 
 /* ---------------- preconditioners ----------------
  * Construction = the reference constructor: makeADInv (preconditioners.hpp:22-63),
