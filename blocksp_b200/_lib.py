@@ -57,6 +57,7 @@ _PD = C.POINTER(C.c_double)
 # name -> (restype, argtypes); every symbol declared in include/blocksp_b200.h
 SIGNATURES: dict[str, tuple] = {
     "bsp_abi_version": (_I, []),
+    "bsp_launch_count": (C.c_uint64, []),
     "bsp_status_string": (C.c_char_p, [_I]),
     "bsp_last_error": (C.c_char_p, [_P]),
     "bsp_device_count": (_I, [C.POINTER(_I)]),

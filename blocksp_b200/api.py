@@ -274,18 +274,27 @@ def _solve(fn_dev, fn_host, A: Matrix, b, pc, opts: SolveOpts, return_info: bool
 
 
 def pCG(A: Matrix, b, tol: float, preCond: Precond | None = None, maxIters: int = 1000,
-        printIters: bool = False, return_info: bool = False, stop_rule: int = _lib.STOP_REFERENCE):
-    """Preconditioned CG (blocksp_solvers.hpp:51-105); x_0 = 0."""
+        printIters: bool = False, return_info: bool = False, stop_rule: int = _lib.STOP_REFERENCE,
+        precision: int = _lib.PREC_F64, inner_tol: float = 1e-6, max_outer: int = 50):
+    """Preconditioned CG (blocksp_solvers.hpp:51-105); x_0 = 0.
+
+    stop_rule=STOP_TRUE_RESIDUAL or precision != PREC_F64 wraps the solve in
+    FP64 iterative refinement until ||b - A x|| / ||b|| <= tol."""
     return _solve("bsp_pcg_dev", "bsp_pcg", A, b, preCond,
-                  _opts(tol, maxIters, print_iters=printIters, stop_rule=stop_rule), return_info)
+                  _opts(tol, maxIters, print_iters=printIters, stop_rule=stop_rule,
+                        precision=precision, inner_tol=inner_tol, max_outer=max_outer), return_info)
 
 
 def pGMRES(A: Matrix, b, tol: float, preCond: Precond | None = None, maxIters: int = 500,
            restart: int = -1, k: int = -1, printIters: bool = False, return_info: bool = False,
-           stop_rule: int = _lib.STOP_REFERENCE):
-    """Left-preconditioned GMRES with optional deflated restart (blocksp_solvers.hpp:156-295)."""
+           stop_rule: int = _lib.STOP_REFERENCE, precision: int = _lib.PREC_F64,
+           inner_tol: float = 1e-6, max_outer: int = 50):
+    """Left-preconditioned GMRES with optional deflated restart (blocksp_solvers.hpp:156-295).
+
+    stop_rule / precision as for pCG."""
     return _solve("bsp_pgmres_dev", "bsp_pgmres", A, b, preCond,
-                  _opts(tol, maxIters, restart, k, printIters, stop_rule=stop_rule), return_info)
+                  _opts(tol, maxIters, restart, k, printIters, stop_rule=stop_rule,
+                        precision=precision, inner_tol=inner_tol, max_outer=max_outer), return_info)
 
 
 class SOR_pGMRES:

@@ -1,5 +1,6 @@
 // api.cu — C ABI glue: handles, matrices, bsmv and vector reductions.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include "reduce.cuh"
 
@@ -7,6 +8,9 @@ namespace bsp {
 
 static thread_local std::string g_last_error;
 void record_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha,
                 const void* x, double beta, const void* z, void* y, cudaStream_t s);
@@ -84,6 +88,8 @@ using namespace bsp;
 extern "C" {
 
 int bsp_abi_version(void) { return BSP_ABI_VERSION; }
+
+uint64_t bsp_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 const char* bsp_status_string(int s) {
   switch (s) {
@@ -290,11 +296,11 @@ int bsp_matrix_make_lowp(bsp_matrix_t A, int dtype) {
   if (dtype == BSP_F32) {
     if (A->vals32.get()) return BSP_OK;
     BSP_TRY(A->vals32.alloc(n > 0 ? n : 1));
-    if (n > 0) k_to_f32<<<grid_for(A->h, n, 256), 256, 0, A->h->stream>>>(n, A->vals.get(), A->vals32.get());
+    if (n > 0) bsp::count_launch(), k_to_f32<<<grid_for(A->h, n, 256), 256, 0, A->h->stream>>>(n, A->vals.get(), A->vals32.get());
   } else if (dtype == BSP_BF16) {
     if (A->vals16.get()) return BSP_OK;
     BSP_TRY(A->vals16.alloc(n > 0 ? n : 1));
-    if (n > 0) k_to_bf16<<<grid_for(A->h, n, 256), 256, 0, A->h->stream>>>(n, A->vals.get(), A->vals16.get());
+    if (n > 0) bsp::count_launch(), k_to_bf16<<<grid_for(A->h, n, 256), 256, 0, A->h->stream>>>(n, A->vals.get(), A->vals16.get());
   } else if (dtype != BSP_F64) {
     return BSP_INVALID;
   }
@@ -346,7 +352,7 @@ int bsp_axpy_dev(bsp_handle_t h, int64_t n, double a, const double* x, double* y
   if (!h || n < 0) return BSP_INVALID;
   DeviceGuard g(h->device);
   if (n == 0) return BSP_OK;
-  k_axpy<<<grid_for(h, n, 256), 256, 0, h->stream>>>(n, a, x, y);
+  bsp::count_launch(), k_axpy<<<grid_for(h, n, 256), 256, 0, h->stream>>>(n, a, x, y);
   BSP_CUDA_TRY(cudaPeekAtLastError());
   return BSP_OK;
 }

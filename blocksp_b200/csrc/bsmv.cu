@@ -220,7 +220,7 @@ static void launch_fwd(const bsp_matrix_s* A, const VT* vals, const AT* x, AT al
   constexpr int G = BlockMap<BS, VT>::G;
   const int rows_per_cta = kBsmvThreads / G;
   const int grid = (int)ceil_div(A->n_rows, rows_per_cta);
-  k_bsmv<BS, VT, AT, R><<<grid, kBsmvThreads, 0, s>>>(A->n_rows, A->row_ptr.get(),
+  bsp::count_launch(), k_bsmv<BS, VT, AT, R><<<grid, kBsmvThreads, 0, s>>>(A->n_rows, A->row_ptr.get(),
                                                       A->col_idx.get(), vals, x, alpha, beta, z, y);
 }
 template <int BS, typename VT, typename AT, int R>
@@ -229,7 +229,7 @@ static void launch_tr(const bsp_matrix_s* A, const VT* vals, const AT* x, AT alp
   constexpr int G = BlockMap<BS, VT>::G;
   const int per_cta = kBsmvThreads / G;
   const int grid = (int)ceil_div(A->n_cols, per_cta);
-  k_bsmv_tr<BS, VT, AT, R><<<grid, kBsmvThreads, 0, s>>>(
+  bsp::count_launch(), k_bsmv_tr<BS, VT, AT, R><<<grid, kBsmvThreads, 0, s>>>(
       A->n_cols, A->tr_ptr.get(), A->tr_row.get(), A->tr_blk.get(), vals, x, alpha, beta, z, y);
 }
 
@@ -274,11 +274,11 @@ static int bsmv_typed(const bsp_matrix_s* A, int R, bool tr, const VT* vals, con
     const int64_t grid = ceil_div(total, threads);
     if (grid > 0) {
       if (tr)
-        k_bsmv_tr_generic<VT, AT><<<(unsigned)grid, threads, 0, s>>>(
+        bsp::count_launch(), k_bsmv_tr_generic<VT, AT><<<(unsigned)grid, threads, 0, s>>>(
             A->n_cols, A->bs, R, A->tr_ptr.get(), A->tr_row.get(), A->tr_blk.get(), vals, x,
             alpha, beta, z, y);
       else
-        k_bsmv_generic<VT, AT><<<(unsigned)grid, threads, 0, s>>>(
+        bsp::count_launch(), k_bsmv_generic<VT, AT><<<(unsigned)grid, threads, 0, s>>>(
             A->n_rows, A->bs, R, A->row_ptr.get(), A->col_idx.get(), vals, x, alpha, beta, z, y);
     }
   }
@@ -308,6 +308,14 @@ int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alph
       return bsmv_typed<__nv_bfloat16, float>(A, nrhs, tr, A->vals16.get(), (const float*)x,
                                               (float)alpha, (float)beta, (const float*)z,
                                               (float*)y, s);
+    case BSP_F32_STORE:  // FP32 blocks, FP64 vectors and accumulation
+      if (!A->vals32.get()) return BSP_INVALID;
+      return bsmv_typed<float, double>(A, nrhs, tr, A->vals32.get(), (const double*)x, alpha, beta,
+                                       (const double*)z, (double*)y, s);
+    case BSP_BF16_STORE:  // BF16 blocks, FP64 vectors and accumulation
+      if (!A->vals16.get()) return BSP_INVALID;
+      return bsmv_typed<__nv_bfloat16, double>(A, nrhs, tr, A->vals16.get(), (const double*)x, alpha,
+                                               beta, (const double*)z, (double*)y, s);
     default:
       return BSP_INVALID;
   }

@@ -52,12 +52,12 @@ __device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p
 __device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
 __device__ __forceinline__ uint4 ld_stream(const uint4* p) { return __ldcs(p); }
 
-// Unpack a chunk into V accumulator-type values.
+// Unpack a chunk into V accumulator-type values (FP32 or FP64 accumulation).
 __device__ __forceinline__ void unpack(const double2& c, double* v) { v[0] = c.x; v[1] = c.y; }
-__device__ __forceinline__ void unpack(const float4& c, float* v) {
+template <typename AT> __device__ __forceinline__ void unpack(const float4& c, AT* v) {
   v[0] = c.x; v[1] = c.y; v[2] = c.z; v[3] = c.w;
 }
-__device__ __forceinline__ void unpack(const uint4& c, float* v) {
+template <typename AT> __device__ __forceinline__ void unpack(const uint4& c, AT* v) {
   const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&c);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -68,10 +68,15 @@ __device__ __forceinline__ void unpack(const uint4& c, float* v) {
 }
 
 // Load V consecutive accumulator-type vector entries (16-byte aligned).
+// FP64 vectors next to FP64 (V = 2), FP32 (V = 4) or BF16 (V = 8) blocks.
 template <int V> __device__ __forceinline__ void ld_vec(const double* p, double* v) {
-  static_assert(V == 2, "double chunks hold 2 values");
-  double2 t = __ldg(reinterpret_cast<const double2*>(p));
-  v[0] = t.x; v[1] = t.y;
+  static_assert(V == 2 || V == 4 || V == 8, "chunks hold 2, 4 or 8 values");
+#pragma unroll
+  for (int k = 0; k < V / 2; ++k) {
+    double2 t = __ldg(reinterpret_cast<const double2*>(p) + k);
+    v[2 * k] = t.x;
+    v[2 * k + 1] = t.y;
+  }
 }
 template <int V> __device__ __forceinline__ void ld_vec(const float* p, float* v) {
   static_assert(V == 4 || V == 8, "float chunks hold 4 (fp32) or 8 (bf16) values");
@@ -85,8 +90,12 @@ template <int V> __device__ __forceinline__ void ld_vec(const float* p, float* v
 // Same, coherent at L2 (bypasses L1): used for vector entries written by other
 // warps during the same launch (sync-free triangular sweeps).
 template <int V> __device__ __forceinline__ void ld_vec_cg(const double* p, double* v) {
-  double2 t = __ldcg(reinterpret_cast<const double2*>(p));
-  v[0] = t.x; v[1] = t.y;
+#pragma unroll
+  for (int k = 0; k < V / 2; ++k) {
+    double2 t = __ldcg(reinterpret_cast<const double2*>(p) + k);
+    v[2 * k] = t.x;
+    v[2 * k + 1] = t.y;
+  }
 }
 template <int V> __device__ __forceinline__ void ld_vec_cg(const float* p, float* v) {
   float4 t = __ldcg(reinterpret_cast<const float4*>(p));
@@ -133,6 +142,9 @@ __device__ __forceinline__ AT row_reduce(AT v, unsigned mask) {
 }
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Process-wide count of kernel launches made by this library (bsp_launch_count).
+void count_launch();
 
 }  // namespace bsp
 

@@ -436,8 +436,15 @@ struct EventTimer {
 };
 
 // ------------------------------------------------------------------ pCG
+// Stored copy the inner operator reads: FP64 for the reference method, FP32
+// blocks (FP64 vectors, FP64 accumulation) for both mixed modes; the BF16
+// mode keeps A in FP32 and stores only the preconditioner factors in BF16.
+static int op_dtype_of(int op_prec) { return op_prec == BSP_PREC_F64 ? BSP_F64 : BSP_F32_STORE; }
+
 int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b, double* x,
-              const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info) {
+              const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info,
+              int op_prec = BSP_PREC_F64, bool want_true = true) {
+  const int op_dtype = op_dtype_of(op_prec);
   const int64_t len = (int64_t)A->n_rows * A->bs;
   const int hcap = std::max(2, o->max_iters + 3);
   DevBuf<double> vr, vp, vz, vAp, dhist;
@@ -453,24 +460,24 @@ int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double*
   const int g = grid_for(h, len, 256);
   KHead* hd = dhead.get();
   BSP_CUDA_TRY(cudaMemsetAsync(x, 0, len * sizeof(double), h->stream));      // x = 0
-  k_copy<<<g, 256, 0, h->stream>>>(len, b, vr.get());                         // r = b
-  if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, b, vp.get()));              // p = M^-1 b
-  else k_copy<<<g, 256, 0, h->stream>>>(len, b, vp.get());
-  k_copy<<<g, 256, 0, h->stream>>>(len, vp.get(), vz.get());                  // z = p
+  bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, b, vr.get());                         // r = b
+  if (pc) BSP_TRY(precond_apply(pc, op_prec,b, vp.get()));              // p = M^-1 b
+  else bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, b, vp.get());
+  bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, vp.get(), vz.get());                  // z = p
   BSP_TRY(launch_reduce<2>(h, 3, len, CgInitBody{vp.get(), vr.get()}, CgInitFin{hd, o->tol, dhist.get()}));
   KHead st;
   BSP_TRY(read_head(h, hd, &st));
   while (st.done == DONE_RUNNING) {
-    BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, vp.get(), 0.0, nullptr, vAp.get(), h->stream));
+    BSP_TRY(bsmv_launch(A, 1, 0, op_dtype, 1.0,vp.get(), 0.0, nullptr, vAp.get(), h->stream));
     BSP_TRY(launch_reduce<1>(h, 4, len, CgPApBody{vp.get(), vAp.get()}, CgPApFin{hd}));
     BSP_TRY(launch_reduce<1>(h, 5, len, CgUpdBody{x, vr.get(), vp.get(), vAp.get(), hd, 0.0},
                              CgUpdFin{hd, dhist.get(), hcap}));
     BSP_TRY(read_head(h, hd, &st));
     if (st.done != DONE_RUNNING) break;
-    if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, vr.get(), vz.get()));
-    else k_copy<<<g, 256, 0, h->stream>>>(len, vr.get(), vz.get());
+    if (pc) BSP_TRY(precond_apply(pc, op_prec,vr.get(), vz.get()));
+    else bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, vr.get(), vz.get());
     BSP_TRY(launch_reduce<1>(h, 6, len, CgRzBody{vr.get(), vz.get()}, CgRzFin{hd, o->max_iters}));
-    k_cg_p<<<g, 256, 0, h->stream>>>(len, vz.get(), hd, vp.get());
+    bsp::count_launch(), k_cg_p<<<g, 256, 0, h->stream>>>(len, vz.get(), hd, vp.get());
     BSP_CUDA_TRY(cudaPeekAtLastError());
     BSP_TRY(read_head(h, hd, &st));
   }
@@ -487,7 +494,7 @@ int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double*
     info->res0 = st.res0;
     info->final_res = st.res;
     info->solve_ms = solve_ms;
-    BSP_TRY(true_residual(h, A, b, x, vAp.get(), &info->true_rel_res));
+    if (want_true) BSP_TRY(true_residual(h, A, b, x, vAp.get(), &info->true_rel_res));
   }
   if (o->print_iters) {
     printf("pCG iters %d\n", st.j);  // solvers.hpp:99-103
@@ -498,7 +505,9 @@ int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double*
 
 // ------------------------------------------------------------------ pGMRES
 int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b, double* x,
-                 const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info) {
+                 const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info,
+                 int op_prec = BSP_PREC_F64, bool want_true = true) {
+  const int op_dtype = op_dtype_of(op_prec);
   const int64_t len = (int64_t)A->n_rows * A->bs;
   const int restart = o->restart;
   const int k_req = o->k;
@@ -593,11 +602,11 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
   BSP_TRY(ensure_basis(restart > 0 ? m + 1 : 2));
   BSP_CUDA_TRY(cudaMemsetAsync(vx0.get(), 0, len * sizeof(double), h->stream));  // x_0 = 0
   // r_0 = M^-1 b; res_mag[0] = ||r_0||; q_0 = r_0 / res_mag[0]
-  if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, b, vr0.get()));
-  else k_copy<<<g, 256, 0, h->stream>>>(len, b, vr0.get());
+  if (pc) BSP_TRY(precond_apply(pc, op_prec,b, vr0.get()));
+  else bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, b, vr0.get());
   BSP_TRY(launch_reduce<1>(h, 7, len, DotBody{vr0.get(), vr0.get()}, NormFin{&hd->res0}));
-  k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
-  k_gm_init<<<1, 1, 0, h->stream>>>(gp, o->tol);
+  bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
+  bsp::count_launch(), k_gm_init<<<1, 1, 0, h->stream>>>(gp, o->tol);
   BSP_CUDA_TRY(cudaPeekAtLastError());
   KHead st;
   BSP_TRY(read_head(h, hd, &st));
@@ -607,8 +616,8 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     const int j = st.j;
     BSP_TRY(ensure_basis(j + 2));
     // v = M^-1 A q_j
-    BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, qptr[j], 0.0, nullptr, vv.get(), h->stream));
-    if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, vv.get(), vv.get()));
+    BSP_TRY(bsmv_launch(A, 1, 0, op_dtype, 1.0,qptr[j], 0.0, nullptr, vv.get(), h->stream));
+    if (pc) BSP_TRY(precond_apply(pc, op_prec,vv.get(), vv.get()));
     // MGS: j+2 fused passes
     for (int i = 0; i <= j; ++i) {
       MgsBody body{vv.get(), i > 0 ? qptr[i - 1] : nullptr, qptr[i],
@@ -617,26 +626,26 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     }
     BSP_TRY(launch_reduce<1>(h, 10, len, MgsLastBody{vv.get(), qptr[j], gp.H + (size_t)j * m + j, 0.0},
                              NormFin{gp.H + (size_t)(j + 1) * m + j}));
-    k_div<<<g, 256, 0, h->stream>>>(len, vv.get(), gp.H + (size_t)(j + 1) * m + j, hd, qptr[j + 1]);
-    k_gm_ls<<<1, 1, 0, h->stream>>>(gp, o->max_iters);
+    bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vv.get(), gp.H + (size_t)(j + 1) * m + j, hd, qptr[j + 1]);
+    bsp::count_launch(), k_gm_ls<<<1, 1, 0, h->stream>>>(gp, o->max_iters);
     BSP_CUDA_TRY(cudaPeekAtLastError());
     BSP_TRY(read_head(h, hd, &st));
     if (st.done != DONE_RUNNING) break;
     if (restart > 0 && st.j == restart) {
       // x_0 = x_0 + Q y
-      k_gm_y<<<1, 1, 0, h->stream>>>(gp);
-      k_gm_combine<<<g, 256, 0, h->stream>>>(len, vx0.get(), dq.get(), gp.y, hd);
+      bsp::count_launch(), k_gm_y<<<1, 1, 0, h->stream>>>(gp);
+      bsp::count_launch(), k_gm_combine<<<g, 256, 0, h->stream>>>(len, vx0.get(), dq.get(), gp.y, hd);
       ++n_restarts;
       if (k_req == 0) {
         // r_0 = M^-1 (b - A x_0), pure restart
-        BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, -1.0, vx0.get(), 1.0, b, vr0.get(), h->stream));
-        if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, vr0.get(), vr0.get()));
+        BSP_TRY(bsmv_launch(A, 1, 0, op_dtype, -1.0, vx0.get(), 1.0, b, vr0.get(), h->stream));
+        if (pc) BSP_TRY(precond_apply(pc, op_prec,vr0.get(), vr0.get()));
         BSP_TRY(launch_reduce<1>(h, 7, len, DotBody{vr0.get(), vr0.get()}, NormFin{&hd->res0}));
-        k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
-        k_gm_pure_restart<<<1, 1, 0, h->stream>>>(gp);
+        bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
+        bsp::count_launch(), k_gm_pure_restart<<<1, 1, 0, h->stream>>>(gp);
       } else {
-        k_gm_deflate<<<1, 1, 0, h->stream>>>(gp, k_req, n_spare);
-        k_gm_qn_update<<<g, 256, 0, h->stream>>>(len, dq.get(), dspare.get(), gp.P, m + 1, hd, st.j + 1);
+        bsp::count_launch(), k_gm_deflate<<<1, 1, 0, h->stream>>>(gp, k_req, n_spare);
+        bsp::count_launch(), k_gm_qn_update<<<g, 256, 0, h->stream>>>(len, dq.get(), dspare.get(), gp.P, m + 1, hd, st.j + 1);
       }
       BSP_CUDA_TRY(cudaPeekAtLastError());
       BSP_TRY(read_head(h, hd, &st));
@@ -651,9 +660,9 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     }
   }
   // x = x_0 + Q y
-  k_gm_y<<<1, 1, 0, h->stream>>>(gp);
+  bsp::count_launch(), k_gm_y<<<1, 1, 0, h->stream>>>(gp);
   BSP_CUDA_TRY(cudaMemcpyAsync(x, vx0.get(), len * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  k_gm_combine<<<g, 256, 0, h->stream>>>(len, x, dq.get(), gp.y, hd);
+  bsp::count_launch(), k_gm_combine<<<g, 256, 0, h->stream>>>(len, x, dq.get(), gp.y, hd);
   BSP_CUDA_TRY(cudaPeekAtLastError());
   const double solve_ms = tm.stop_ms();
   if (pc) BSP_TRY(precond_check_status(pc));
@@ -668,13 +677,105 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     info->res0 = st.res0;
     info->final_res = st.res;
     info->solve_ms = solve_ms;
-    BSP_TRY(true_residual(h, A, b, x, vv.get(), &info->true_rel_res));
+    if (want_true) BSP_TRY(true_residual(h, A, b, x, vv.get(), &info->true_rel_res));
   }
   if (o->print_iters) {
     printf("pGMRES iters %d\n", st.tot);  // solvers.hpp:266-270
     if (st.tot > o->max_iters) printf("maximum pGMRES iterations reached\n");
   }
   return status_of(st.done);
+}
+
+int precond_ensure_precision(bsp_precond_s* pc, int precision);
+
+__global__ void k_add(int64_t n, const double* __restrict__ d, double* __restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += d[i];
+}
+
+// FP64 iterative refinement around the Krylov solver.  Used for the true-
+// residual stopping rule and for the mixed-precision inner operator:
+//   x = 0, r = b;  repeat: solve A d = r (inner tolerance), x += d,
+//   r = b - A x in FP64, stop when ||r|| / ||b|| <= tol.
+// The inner solve runs the reference's method with the requested operator
+// precision; its residual history entries are appended to hist.
+int refine_solve(bool gmres, bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b,
+                 double* x, const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info) {
+  const int64_t len = (int64_t)A->n_rows * A->bs;
+  const int prec = o->precision;
+  if (prec != BSP_PREC_F64) {
+    BSP_TRY(bsp_matrix_make_lowp(A, BSP_F32));
+    if (pc) BSP_TRY(precond_ensure_precision(pc, prec));
+  }
+  DevBuf<double> r, d, work;
+  BSP_TRY(r.alloc(len));
+  BSP_TRY(d.alloc(len));
+  BSP_TRY(work.alloc(len));
+  const int g = grid_for(h, len, 256);
+  EventTimer tm(h->stream);
+  double* sc = h->ws.scalars.get();
+  BSP_CUDA_TRY(cudaMemsetAsync(x, 0, len * sizeof(double), h->stream));
+  bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, b, r.get());
+  BSP_TRY(launch_reduce<1>(h, 11, len, DotBody{b, b}, StoreFin{sc + 8}));
+  double bb = 0.0;
+  BSP_CUDA_TRY(cudaMemcpyAsync(&bb, sc + 8, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const double bnorm = sqrt(bb);
+  double rel = 1.0;
+  int total_iters = 0, n_hist = 0, n_restarts = 0, outer = 0, status = BSP_MAXIT;
+  const int max_outer = o->max_outer > 0 ? o->max_outer : 50;
+  if (!(bnorm > 0.0)) {
+    status = std::isfinite(bnorm) ? BSP_OK : BSP_NAN;
+    rel = 0.0;
+  }
+  while (status == BSP_MAXIT && outer < max_outer) {
+    bsp_solve_opts in = *o;
+    in.print_iters = 0;
+    if (prec == BSP_PREC_F64)
+      in.tol = outer == 0 ? o->tol : std::min(0.5, 0.5 * o->tol / rel);
+    else
+      in.tol = std::max(o->inner_tol > 0 ? o->inner_tol : 1e-6, 0.5 * o->tol / rel);
+    in.max_iters = std::max(1, o->max_iters - total_iters);
+    bsp_solve_info ii{};
+    const int cap = hist ? std::max(0, hist_cap - n_hist) : 0;
+    const int s = gmres ? pgmres_solve(h, A, pc, r.get(), d.get(), &in, hist ? hist + n_hist : nullptr,
+                                       cap, &ii, prec, false)
+                        : pcg_solve(h, A, pc, r.get(), d.get(), &in, hist ? hist + n_hist : nullptr, cap,
+                                    &ii, prec, false);
+    total_iters += ii.iters;
+    n_hist += std::min(ii.n_hist, cap);
+    n_restarts += ii.n_restarts;
+    ++outer;
+    if (s != BSP_OK && s != BSP_MAXIT) {
+      status = s;
+      break;
+    }
+    bsp::count_launch(), k_add<<<g, 256, 0, h->stream>>>(len, d.get(), x);
+    // r = b - A x in FP64; rel = ||r|| / ||b||
+    BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, -1.0, x, 1.0, b, r.get(), h->stream));
+    BSP_TRY(launch_reduce<1>(h, 12, len, DotBody{r.get(), r.get()}, StoreFin{sc + 9}));
+    double rr = 0.0;
+    BSP_CUDA_TRY(cudaMemcpyAsync(&rr, sc + 9, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    rel = sqrt(rr) / bnorm;
+    if (!std::isfinite(rel)) status = BSP_NAN;
+    else if (rel <= o->tol) status = BSP_OK;
+    else if (total_iters >= o->max_iters) break;
+  }
+  const double ms = tm.stop_ms();
+  if (info) {
+    info->status = status;
+    info->iters = total_iters;
+    info->inner_iters = total_iters;
+    info->n_outer = outer;
+    info->n_hist = n_hist;
+    info->n_restarts = n_restarts;
+    info->final_res = rel;
+    info->true_rel_res = rel;
+    info->solve_ms = ms;
+  }
+  if (o->print_iters) printf("%s iters %d (refinement steps %d)\n", gmres ? "pGMRES" : "pCG", total_iters, outer);
+  return status;
 }
 
 }  // namespace bsp
@@ -689,6 +790,8 @@ static int solve_common(bool gmres, bsp_handle_t h, bsp_matrix_t A, bsp_precond_
   if (A->n_rows != A->n_cols) return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
   if (info) *info = bsp_solve_info{};
+  if (opts->precision != BSP_PREC_F64 || opts->stop_rule == BSP_STOP_TRUE_RESIDUAL)
+    return refine_solve(gmres, h, A, pc, b, x, opts, hist, hist_cap, info);
   return gmres ? pgmres_solve(h, A, pc, b, x, opts, hist, hist_cap, info)
                : pcg_solve(h, A, pc, b, x, opts, hist, hist_cap, info);
 }

@@ -89,7 +89,7 @@ extern "C" int bsp_dot_noalloc(void* stream, int64_t n, const double* x, const d
   // the ticket must start at zero; the partials are written before being read
   BSP_CUDA_TRY(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), s));
   const int blocks = (int)std::max<int64_t>(1, ceil_div(n, kNoAllocChunk));
-  k_reduce<1, DotBody, StoreFin><<<blocks, kRedThreads, 0, s>>>(n, DotBody{x, y}, StoreFin{out_dev},
+  bsp::count_launch(), k_reduce<1, DotBody, StoreFin><<<blocks, kRedThreads, 0, s>>>(n, DotBody{x, y}, StoreFin{out_dev},
                                                                  a.partials, a.ticket);
   BSP_CUDA_TRY(cudaPeekAtLastError());
   return BSP_OK;

@@ -549,7 +549,7 @@ static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* 
   BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BSP_CUDA_TRY(cudaMemsetAsync(pc->ticket.get(), 0, sizeof(unsigned), h->stream));
   const int grid = persistent_grid(h, k_factor, kFactorWarps * 32, smem);
-  k_factor<<<grid, kFactorWarps * 32, smem, h->stream>>>(fp);
+  bsp::count_launch(), k_factor<<<grid, kFactorWarps * 32, smem, h->stream>>>(fp);
   BSP_CUDA_TRY(cudaPeekAtLastError());
   DevStatus st;
   BSP_TRY(read_status(h, &st));
@@ -566,7 +566,7 @@ template <int BS, typename VT, typename AT, bool TRANS, int POST>
 static int launch_sweep_t(bsp_handle_s* h, const SweepP<VT, AT>& p) {
   static int grid = 0;
   if (!grid) grid = persistent_grid(h, k_sweep<BS, VT, AT, TRANS, POST>, kSweepThreads, 0);
-  k_sweep<BS, VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p);
+  bsp::count_launch(), k_sweep<BS, VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p);
   return BSP_OK;
 }
 
@@ -597,7 +597,7 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
   if (!done) {
     static int grid = 0;
     if (!grid) grid = persistent_grid(h, k_sweep_generic<VT, AT, TRANS, POST>, kSweepThreads, 0);
-    k_sweep_generic<VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p, bs);
+    bsp::count_launch(), k_sweep_generic<VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p, bs);
   }
   BSP_CUDA_TRY(cudaPeekAtLastError());
   return BSP_OK;
@@ -638,7 +638,7 @@ static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
   BSP_TRY(upload(pc->d_perm, perm));
   const int b2 = pc->bs * pc->bs;
   BSP_TRY(pc->f_vals.alloc(pc->f_nnzb * b2));
-  k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
+  bsp::count_launch(), k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
       pc->f_nnzb, b2, pc->d_perm.get(), A->vals.get(), pc->f_vals.get());
   BSP_CUDA_TRY(cudaPeekAtLastError());
   // level orders on the sorted structure
@@ -719,17 +719,17 @@ static int make_lowp_copies(bsp_precond_s* pc) {
   const int64_t nf = pc->f_nnzb * b2;
   if (pc->precision == BSP_PREC_F32) {
     BSP_TRY(pc->dinv32.alloc(nd));
-    k_convert<float><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv32.get());
+    bsp::count_launch(), k_convert<float><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv32.get());
     if (nf > 0) {
       BSP_TRY(pc->f_vals32.alloc(nf));
-      k_convert<float><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals32.get());
+      bsp::count_launch(), k_convert<float><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals32.get());
     }
   } else {
     BSP_TRY(pc->dinv16.alloc(nd));
-    k_convert<__nv_bfloat16><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv16.get());
+    bsp::count_launch(), k_convert<__nv_bfloat16><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv16.get());
     if (nf > 0) {
       BSP_TRY(pc->f_vals16.alloc(nf));
-      k_convert<__nv_bfloat16><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals16.get());
+      bsp::count_launch(), k_convert<__nv_bfloat16><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals16.get());
     }
   }
   BSP_CUDA_TRY(cudaPeekAtLastError());
@@ -875,29 +875,63 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
   }
 }
 
-int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z) {
+// z = M^{-1} r.  precision selects the stored factors (FP64 / FP32 / BF16);
+// vec64 selects FP64 vectors (the Krylov path, always FP64 accumulation) or
+// FP32 vectors (low-precision vectors, FP32 accumulation).
+int precond_apply_typed(bsp_precond_s* pc, int precision, bool vec64, const void* r, void* z) {
   if (precision == BSP_PREC_F64) {
     return apply_typed<double, double>(pc, (const double*)r, (double*)z, pc->f_vals.get(),
                                        pc->dinv.get(), pc->A->vals.get(), pc->sor_a.get(),
                                        pc->sor_b.get());
   }
   const size_t nv = (size_t)pc->n * pc->bs;
-  if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL) {
-    if (pc->sor_a32.n < nv) {
-      BSP_TRY(pc->sor_a32.alloc(nv));
-      BSP_TRY(pc->sor_b32.alloc(nv));
+  const bool sor = pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL;
+  if (precision == BSP_PREC_F32 && !pc->dinv32.get()) return BSP_INVALID;
+  if (precision == BSP_PREC_BF16 && !pc->dinv16.get()) return BSP_INVALID;
+  if (vec64) {
+    if (sor && pc->sor_a.n < nv) {
+      BSP_TRY(pc->sor_a.alloc(nv));
+      BSP_TRY(pc->sor_b.alloc(nv));
     }
+    if (precision == BSP_PREC_F32)
+      return apply_typed<float, double>(pc, (const double*)r, (double*)z, pc->f_vals32.get(),
+                                        pc->dinv32.get(), pc->A->vals32.get(), pc->sor_a.get(),
+                                        pc->sor_b.get());
+    return apply_typed<__nv_bfloat16, double>(pc, (const double*)r, (double*)z, pc->f_vals16.get(),
+                                              pc->dinv16.get(), pc->A->vals16.get(),
+                                              pc->sor_a.get(), pc->sor_b.get());
   }
-  if (precision == BSP_PREC_F32) {
-    if (!pc->dinv32.get()) return BSP_INVALID;
+  if (sor && pc->sor_a32.n < nv) {
+    BSP_TRY(pc->sor_a32.alloc(nv));
+    BSP_TRY(pc->sor_b32.alloc(nv));
+  }
+  if (precision == BSP_PREC_F32)
     return apply_typed<float, float>(pc, (const float*)r, (float*)z, pc->f_vals32.get(),
                                      pc->dinv32.get(), pc->A->vals32.get(), pc->sor_a32.get(),
                                      pc->sor_b32.get());
-  }
-  if (!pc->dinv16.get()) return BSP_INVALID;
   return apply_typed<__nv_bfloat16, float>(pc, (const float*)r, (float*)z, pc->f_vals16.get(),
                                            pc->dinv16.get(), pc->A->vals16.get(),
                                            pc->sor_a32.get(), pc->sor_b32.get());
+}
+
+int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z) {
+  return precond_apply_typed(pc, precision, true, r, z);
+}
+
+// Make the low-precision copies of the factors (and of A for SOR/Diag) that a
+// mixed-precision solve needs, if the preconditioner was built without them.
+int precond_ensure_precision(bsp_precond_s* pc, int precision) {
+  if (precision == BSP_PREC_F64) return BSP_OK;
+  if (precision == BSP_PREC_F32 && pc->dinv32.get()) return BSP_OK;
+  if (precision == BSP_PREC_BF16 && pc->dinv16.get()) return BSP_OK;
+  if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL || pc->kind == BSP_PC_DIAG_LU ||
+      pc->kind == BSP_PC_DIAG_CHOL)
+    BSP_TRY(bsp_matrix_make_lowp(pc->A, precision == BSP_PREC_F32 ? BSP_F32 : BSP_BF16));
+  const int saved = pc->precision;
+  pc->precision = precision;
+  const int s = make_lowp_copies(pc);
+  pc->precision = saved;
+  return s;
 }
 
 int precond_check_status(bsp_precond_s* pc) {

@@ -83,7 +83,7 @@ inline int launch_reduce(bsp_handle_s* h, int slot, int64_t n, Body body, Fin fi
   double* partials = h->ws.partials.get() + (size_t)slot * kRedBlocks * 4;
   unsigned* ticket = h->ws.tickets.get() + slot;
   static_assert(NV <= 4, "at most 4 simultaneous sums per launch");
-  k_reduce<NV, Body, Fin><<<kRedBlocks, kRedThreads, 0, h->stream>>>(n, body, fin, partials, ticket);
+  bsp::count_launch(), k_reduce<NV, Body, Fin><<<kRedBlocks, kRedThreads, 0, h->stream>>>(n, body, fin, partials, ticket);
   BSP_CUDA_TRY(cudaPeekAtLastError());
   return BSP_OK;
 }

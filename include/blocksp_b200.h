@@ -54,7 +54,11 @@ enum bsp_status {
   BSP_OUT_OF_MEMORY = 10
 };
 
-enum bsp_dtype { BSP_F64 = 0, BSP_F32 = 1, BSP_BF16 = 2 };
+/* Stored copy of the matrix a bsmv reads, and its vector type:
+ * BSP_F64 FP64 blocks and vectors; BSP_F32 FP32 blocks and vectors; BSP_BF16 BF16
+ * blocks with FP32 vectors; BSP_F32_STORE / BSP_BF16_STORE FP32 / BF16 blocks with
+ * FP64 vectors and FP64 accumulation (the mixed-precision inner operator). */
+enum bsp_dtype { BSP_F64 = 0, BSP_F32 = 1, BSP_BF16 = 2, BSP_F32_STORE = 3, BSP_BF16_STORE = 4 };
 
 /* Preconditioner kinds (blocksp_preconditioners.hpp:66-538). */
 enum bsp_precond_kind {
@@ -136,6 +140,9 @@ const char* bsp_status_string(int status);
 const char* bsp_last_error(bsp_handle_t h);
 int bsp_device_count(int* count);
 int bsp_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process (all
+ * handles and threads); a diagnostic for benchmarks and tests. */
+uint64_t bsp_launch_count(void);
 
 /* ---------------- matrix ----------------
  * Replaces the packing of BlockSp<T,N> = Sp::CSR<TinyMatrix<T,N,N>>
@@ -166,8 +173,8 @@ int bsp_matrix_make_lowp(bsp_matrix_t A, int dtype);
  * transpose != 0: op(A) = A^T (blocksp_multiply.hpp:196-204, 280-284).
  * The reference's void bsmv(b, A, x) (multiply.hpp:386-390, accumulating)
  * is alpha = 1, beta = 1, z = y; bsmv(A, x) returning a new array is beta = 0.
- * dtype selects the stored copy of A (BSP_F64 or, after bsp_matrix_make_lowp,
- * BSP_F32/BSP_BF16, which take and return FP32 vectors). */
+ * dtype selects the stored copy of A and the vector type (enum bsp_dtype); the
+ * low-precision copies must exist (bsp_matrix_make_lowp). */
 int bsp_bsmv_dev(bsp_handle_t h, bsp_matrix_t A, int nrhs, int transpose, int dtype,
                  double alpha, const void* x, double beta, const void* z, void* y);
 /* Host-buffer form (FP64): copies x (and y when beta != 0) in, y out. */

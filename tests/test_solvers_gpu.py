@@ -174,3 +174,29 @@ def test_zero_rhs_returns_zero(handle):
     assert not np.any(x)
     x = bsp.pGMRES(A, np.zeros_like(s.b), 1e-10, bsp.ILU0(A), 100)
     assert not np.any(x)
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])  # PREC_F64, PREC_F32, PREC_BF16 factors
+def test_true_residual_refinement_pgmres(handle, precision):
+    """FP64 iterative refinement reaches the FP64 true residual 1e-10 with any
+    inner operator precision; the solution error against the oracle's tight
+    FP64 solve is stated and bounded by the conditioning (<= 1e-6 here)."""
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (6, 6, 6), 8, 0.3, 31)
+    x, info, hist = bsp.pGMRES(A, s.b, 1e-10, bsp.ILU0(A), 5000, 30, 10, return_info=True,
+                               stop_rule=1, precision=precision)
+    assert info["status"] == 0
+    assert info["true_rel_res"] <= 1e-10
+    assert O.true_rel_residual(Ao, s.b, x) <= 1.5e-10
+    ref = O.pgmres(Ao, s.b, 1e-13, O.ILU0(Ao), 5000, 30, 10)
+    assert rel(x, ref.x) <= 1e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_true_residual_refinement_pcg(handle, precision):
+    import blocksp_b200 as bsp
+    s, A, Ao = setup_system(handle, (16, 16), 4, 0.0, 32)
+    x, info, hist = bsp.pCG(A, s.b, 1e-10, bsp.IChol0(A), 2000, return_info=True, stop_rule=1,
+                            precision=precision)
+    assert info["status"] == 0 and info["true_rel_res"] <= 1e-10
+    assert O.true_rel_residual(Ao, s.b, x) <= 1.5e-10
