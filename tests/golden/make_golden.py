@@ -1,0 +1,138 @@
+"""Generate the golden fixtures in tests/golden/ by running the reference itself.
+
+TEST INFRASTRUCTURE.  Runs oracle/_ref/ref_solve_hist (the reference BlockSp
+v1.0 headers compiled by oracle/Makefile, residual prints enabled) on small
+seeded systems from blocksp_b200.systems and stores, per case, the reference's
+outputs: the result vector, the residual history it prints, and the printed
+iteration count.  The systems are regenerated from their parameters by the
+tests (the generator is deterministic), so only outputs are stored.
+
+Also stores the LDG fixture (the reference's test_mats/LDG_2D_vecLap*.mtx,
+converted to arrays) and the reference's infinity-norm errors on it, so the GPU
+can be checked against the reference's only known answer where the reference
+sources are not present.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from blocksp_b200 import systems  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+EXE = ROOT / "oracle" / "_ref" / "ref_solve_hist"
+REF_MATS = Path("/root/reference/test_mats")
+
+# name: (dims, bs, seed, skew, B, D, solver, extra args)
+CASES = {
+    "bsmv_2d_bs4": ((8, 8), 4, 1, 0.0, 2, 2, "bsmv", []),
+    "bsmv_3d_bs8": ((4, 4, 4), 8, 2, 0.3, 4, 2, "bsmv", []),
+    "bsmv_3d_bs16": ((3, 3, 3), 16, 3, 0.3, 8, 2, "bsmv", []),
+    "bsmv_multi_bs4_d2": ((6, 6), 4, 4, 0.0, 4, 2, "bsmv_multi", []),
+    "ilu0_apply_3d_bs8": ((4, 4, 4), 8, 5, 0.3, 4, 2, "ilu0_apply", []),
+    "ichol0_apply_2d_bs4": ((8, 8), 4, 6, 0.0, 2, 2, "ichol0_apply", []),
+    "sor_apply_2d_bs4": ((8, 8), 4, 7, 0.3, 2, 2, "sor_apply", ["--w", "1.6", "--nu", "3", "--sortype", "0"]),
+    "diag_apply_3d_bs8": ((4, 4, 4), 8, 8, 0.3, 4, 2, "diag_apply", []),
+    "ichol0_pcg_2d_bs4": ((16, 16), 4, 9, 0.0, 2, 2, "ichol0_pcg", ["--tol", "1e-10", "--maxit", "2000"]),
+    "sor_pcg_2d_bs4": ((12, 12), 4, 10, 0.0, 2, 2, "sor_pcg", ["--tol", "1e-10", "--maxit", "2000"]),
+    "diag_pcg_2d_bs4": ((12, 12), 4, 11, 0.0, 2, 2, "diag_pcg", ["--tol", "1e-10", "--maxit", "2000"]),
+    "ilu0_pgmres_3d_bs8": ((6, 6, 6), 8, 12, 0.3, 4, 2, "ilu0_pgmres", ["--tol", "1e-10"]),
+    "ilu0_pgmres_dr_3d_bs8": ((6, 6, 6), 8, 13, 0.3, 4, 2, "ilu0_pgmres",
+                              ["--tol", "1e-10", "--restart", "30", "--k", "10"]),
+    "ilu0_pgmres_dr10_3d_bs8": ((6, 6, 6), 8, 14, 0.3, 4, 2, "ilu0_pgmres",
+                                ["--tol", "1e-10", "--restart", "10", "--k", "4"]),
+    "sor_pgmres_dr_2d_bs4": ((10, 10), 4, 15, 0.3, 2, 2, "sor_pgmres",
+                             ["--tol", "1e-10", "--restart", "12", "--k", "5"]),
+    "ilu0_pgmres_3d_bs16": ((4, 4, 4), 16, 16, 0.3, 8, 2, "ilu0_pgmres", ["--tol", "1e-10"]),
+}
+
+
+def system_for(dims, bs, seed, skew, nrhs=1):
+    return systems.grid_system(dims, bs, seed=seed, skew=skew, nrhs=nrhs)
+
+
+def run_case(name, spec, tmp: Path) -> dict:
+    dims, bs, seed, skew, B, D, solver, extra = spec
+    nrhs = D if solver == "bsmv_multi" else 1
+    s = system_for(dims, bs, seed, skew, nrhs)
+    f = tmp / f"{name}.bsps"
+    systems.write_bsr(f, s)
+    xo = tmp / f"{name}.x"
+    cmd = [str(EXE), str(f), "--B", str(B), "--D", str(D), "--solver", solver, "--x", str(xo),
+           "--print-iters", *extra]
+    r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+    hist, iters = [], -1
+    for line in r.stdout.splitlines():
+        p = line.split()
+        if not p:
+            continue
+        if p[0] == "RES0":
+            hist.append(float(p[1]))
+        elif p[0] == "RES":
+            hist.append(float(p[2]))
+        elif line.startswith("pCG iters") or line.startswith("pGMRES iters"):
+            iters = int(p[2])
+    x = systems.read_vec(xo)
+    meta = {"dims": list(dims), "bs": bs, "seed": seed, "skew": skew, "B": B, "D": D,
+            "solver": solver, "args": extra}
+    np.savez_compressed(OUT / f"{name}.npz", x=x, hist=np.array(hist), iters=np.array(iters),
+                        meta=np.array(json.dumps(meta)))
+    return {"name": name, "iters": iters, "hist_len": len(hist)}
+
+
+def ldg_fixture() -> None:
+    """The reference's LDG fixture as arrays plus its known-answer errors."""
+    if not REF_MATS.exists():
+        print("reference test_mats not present; LDG fixture not regenerated")
+        return
+
+    # these files start directly with the size line (the reference reads them
+    # with start_line = 1, i.e. from the first line: blocksp_tests.hpp:326-336)
+    def read_vec(path):
+        lines = path.read_text().split("\n")
+        n = int(lines[0].split()[0])
+        return np.array([float(v) for v in lines[1:1 + n]])
+
+    lines = (REF_MATS / "LDG_2D_vecLap.mtx").read_text().split("\n")
+    m, n, nnz = map(int, lines[0].split())
+    rows = np.empty(nnz, np.int32)
+    cols = np.empty(nnz, np.int32)
+    vals = np.empty(nnz)
+    for k in range(nnz):
+        i, j, v = lines[1 + k].split()
+        rows[k], cols[k], vals[k] = int(i) - 1, int(j) - 1, float(v)
+    b = read_vec(REF_MATS / "LDG_2D_vecLap_b.mtx")
+    sol = read_vec(REF_MATS / "LDG_2D_vecLap_sol.mtx")
+    errs = {}
+    for B in (1, 2, 4):
+        r = subprocess.run([str(EXE), "--ldg", str(REF_MATS), "--B", str(B)], capture_output=True,
+                           text=True, check=True)
+        for line in r.stdout.splitlines():
+            if line.startswith("ERRINF"):
+                _, name, v = line.split()
+                errs[f"B{B}_{name}"] = float(v)
+    np.savez_compressed(OUT / "ldg_2d_veclap.npz", n=np.array(m), rows=rows, cols=cols, vals=vals, b=b,
+                        sol=sol, ref_errinf=np.array(json.dumps(errs)))
+    print("LDG errors", errs)
+
+
+def main():
+    if not EXE.exists():
+        sys.exit("build the reference checker first: make -C oracle")
+    with tempfile.TemporaryDirectory() as d:
+        for name, spec in CASES.items():
+            print(run_case(name, spec, Path(d)))
+    ldg_fixture()
+
+
+if __name__ == "__main__":
+    main()
