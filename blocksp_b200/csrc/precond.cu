@@ -72,6 +72,14 @@ template <typename VT, typename AT> struct SweepP {
   int epoch;
   unsigned* ticket;
   DevStatus* st;
+  // Chains: task t covers rows task_row[t], task_row[t] + task_dir, ... (task_len[t]
+  // rows), each depending on the one before it; the group keeps the previous
+  // row's result in shared memory instead of waiting for its flag.  Null
+  // task_row: one row per task, taken from `order`.
+  const int* task_row;
+  const int* task_len;
+  int task_dir;
+  int n_tasks;
 };
 
 template <typename VT, typename AT>
@@ -92,7 +100,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
   using CV = typename Chunk<VT>::vec;
   constexpr int V = M::V, G = M::G, P = M::P, CPR = M::CPR, RPP = M::RPP, CPB = M::CPB;
   constexpr int GPC = kSweepThreads / G;
+  constexpr int NPF = 4;  // entries whose blocks are loaded before any wait
   __shared__ AT sm_s[GPC][BS];
+  __shared__ AT sm_x[GPC][BS];  // the group's previous row of its chain
   const int gl = threadIdx.x % G;
   const int gid = threadIdx.x / G;
   const int lane = threadIdx.x & 31;
@@ -101,13 +111,25 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
   const int c0 = (gl % CPR) * V;
   const CV* vb = reinterpret_cast<const CV*>(p.vals);
   AT* s = sm_s[gid];
+  AT* xs = sm_x[gid];
+  const int n_tasks = p.task_row ? p.n_tasks : p.n;
 
   while (true) {
     int t = 0;
     if (gl == 0) t = (int)atomicAdd(p.ticket, 1u);
     t = __shfl_sync(gmask, t, gbase);
-    if (t >= p.n) break;
-    const int i = p.order ? __ldg(p.order + t) : t;
+    if (t >= n_tasks) break;
+    int i0, len;
+    if (p.task_row) {
+      i0 = __ldg(p.task_row + t);
+      len = __ldg(p.task_len + t);
+    } else {
+      i0 = p.order ? __ldg(p.order + t) : t;
+      len = 1;
+    }
+   for (int step = 0; step < len; ++step) {
+    const int i = i0 + step * p.task_dir;
+    const int prev = step > 0 ? i - p.task_dir : -1;
     int beg, end;
     row_range(p, i, beg, end);
     AT acc[P];
@@ -116,31 +138,48 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
     for (int q = 0; q < P; ++q) acc[q] = AT(0);
 #pragma unroll
     for (int v = 0; v < V; ++v) tac[v] = AT(0);
-    for (int e = beg; e < end; ++e) {
+    // matrix blocks do not depend on the sweep: issue their loads first
+    CV pf[NPF][P];
+#pragma unroll
+    for (int u = 0; u < NPF; ++u) {
+      if (beg + u < end) {
+        const int64_t b = p.blk ? __ldg(p.blk + beg + u) : (int64_t)(beg + u);
+#pragma unroll
+        for (int q = 0; q < P; ++q) pf[u][q] = ld_stream(vb + b * CPB + q * G + gl);
+      }
+    }
+    auto consume = [&](int e, const CV (&a)[P]) {
       const int j = __ldg(p.idx + e);
       const AT* src;
+      bool from_prev = false;
       if (p.range == RANGE_SPLIT) {
-        if (j == i) continue;
+        if (j == i) return;
         const bool dep = (p.dep_dir < 0) ? (j < i) : (j > i);
         if (dep) {
-          wait_flag(p.flags + j, p.epoch, p.st, i);
+          from_prev = (j == prev);
+          if (!from_prev) wait_flag(p.flags + j, p.epoch, p.st, i);
           src = p.x;
         } else {
-          if (!p.xold) continue;
+          if (!p.xold) return;
           src = p.xold;
         }
       } else {
-        wait_flag(p.flags + j, p.epoch, p.st, i);
+        from_prev = (j == prev);
+        if (!from_prev) wait_flag(p.flags + j, p.epoch, p.st, i);
         src = p.x;
       }
-      const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
       if constexpr (!TRANS) {
         AT xv[V];
-        ld_vec_cg<V>(src + (int64_t)j * BS + c0, xv);
+        if (from_prev) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) xv[v] = xs[c0 + v];
+        } else {
+          ld_vec_cg<V>(src + (int64_t)j * BS + c0, xv);
+        }
 #pragma unroll
         for (int q = 0; q < P; ++q) {
           AT av[V];
-          unpack(ld_stream(vb + b * CPB + q * G + gl), av);
+          unpack(a[q], av);
 #pragma unroll
           for (int v = 0; v < V; ++v) acc[q] = fma(av[v], xv[v], acc[q]);
         }
@@ -148,13 +187,23 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
 #pragma unroll
         for (int q = 0; q < P; ++q) {
           const int r = q * RPP + gl / CPR;
-          const AT xr = __ldcg(src + (int64_t)j * BS + r);
+          const AT xr = from_prev ? xs[r] : __ldcg(src + (int64_t)j * BS + r);
           AT av[V];
-          unpack(ld_stream(vb + b * CPB + q * G + gl), av);
+          unpack(a[q], av);
 #pragma unroll
           for (int v = 0; v < V; ++v) tac[v] = fma(av[v], xr, tac[v]);
         }
       }
+    };
+#pragma unroll
+    for (int u = 0; u < NPF; ++u)
+      if (beg + u < end) consume(beg + u, pf[u]);
+    for (int e = beg + NPF; e < end; ++e) {
+      const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
+      CV a[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) a[q] = ld_stream(vb + b * CPB + q * G + gl);
+      consume(e, a);
     }
     // s = rhs_i - sum  (in shared memory, BS values per group)
     if constexpr (!TRANS) {
@@ -180,7 +229,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
     __syncwarp(gmask);
     // post-operation and write-back of row i
     if constexpr (POST == POST_NONE) {
-      for (int r = gl; r < BS; r += G) p.x[(int64_t)i * BS + r] = s[r];
+      for (int r = gl; r < BS; r += G) {
+        p.x[(int64_t)i * BS + r] = s[r];
+        xs[r] = s[r];
+      }
     } else if constexpr (POST == POST_D || POST == POST_SOR) {
       const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)i * CPB;
       AT sv[V];
@@ -207,6 +259,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
             val = xo + (-p.w * xo + p.w * val);
           }
           p.x[(int64_t)i * BS + r] = val;
+          xs[r] = val;
         }
       }
     } else {  // POST_DT: x = D^T s
@@ -229,13 +282,21 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         for (int off = CPR; off < G; off <<= 1) o[v] += __shfl_xor_sync(gmask, o[v], off);
       if (gl < CPR) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) p.x[(int64_t)i * BS + c0 + v] = o[v];
+        for (int v = 0; v < V; ++v) {
+          p.x[(int64_t)i * BS + c0 + v] = o[v];
+          xs[c0 + v] = o[v];
+        }
       }
     }
-    __threadfence();
+    // publish row i: the lanes' stores are ordered before lane 0's release by
+    // the warp barrier, and the fence makes them visible at GPU scope first
     __syncwarp(gmask);
-    if (gl == 0) st_release(p.flags + i, p.epoch);
+    if (gl == 0) {
+      __threadfence();
+      st_release(p.flags + i, p.epoch);
+    }
     __syncwarp(gmask);
+   }
   }
 }
 
@@ -457,6 +518,9 @@ struct bsp_precond_s {
   // level orders
   DevBuf<int> order_lo, order_up;
   int n_lev_lo = 0, n_lev_up = 0;
+  // chains of consecutive dependent rows, in chain-level order (sweep tasks)
+  DevBuf<int> task_lo_row, task_lo_len, task_up_row, task_up_len;
+  int n_task_lo = 0, n_task_up = 0;
   // sync-free state
   DevBuf<int> flags;
   DevBuf<unsigned> ticket;
@@ -499,10 +563,71 @@ static int level_order(int n, bool ascending, Deps deps, std::vector<int>& order
   return maxl + 1;
 }
 
+// Sweep tasks: maximal chains of rows visited consecutively in sweep order
+// (ascending: r, r+1, ...; descending: r, r-1, ...) in which every row depends
+// on the row visited just before it.  Chains are contiguous row ranges, so the
+// chain graph is acyclic; tasks are sorted by chain level (1 + the highest
+// level of any other chain a row of the chain depends on), so a task only
+// waits on rows of tasks with smaller tickets.
+template <class Deps>
+static int build_tasks(int n, bool ascending, Deps deps, std::vector<int>& row, std::vector<int>& len) {
+  std::vector<int> chain(n), first, clen;
+  const int dir = ascending ? 1 : -1;
+  for (int idx = 0; idx < n; ++idx) {
+    const int r = ascending ? idx : n - 1 - idx;
+    const int prev = r - dir;
+    bool cont = false;
+    if (idx > 0) deps(r, [&](int j) { cont |= (j == prev); });
+    if (cont) {
+      chain[r] = chain[prev];
+      clen[chain[r]]++;
+    } else {
+      chain[r] = (int)first.size();
+      first.push_back(r);
+      clen.push_back(1);
+    }
+  }
+  const int nc = (int)first.size();
+  std::vector<int> lvl(nc, 0);
+  for (int c = 0; c < nc; ++c)  // chains are created in sweep order: a topological order
+    for (int s = 0; s < clen[c]; ++s) {
+      const int r = first[c] + s * dir;
+      deps(r, [&](int j) {
+        if (chain[j] != c) lvl[c] = std::max(lvl[c], lvl[chain[j]] + 1);
+      });
+    }
+  std::vector<int> idx(nc);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return lvl[a] < lvl[b]; });
+  row.resize(nc);
+  len.resize(nc);
+  for (int t = 0; t < nc; ++t) {
+    row[t] = first[idx[t]];
+    len[t] = clen[idx[t]];
+  }
+  return nc;
+}
+
 template <typename T> static int upload(DevBuf<T>& d, const std::vector<T>& v) {
   BSP_TRY(d.alloc(v.empty() ? 1 : v.size()));
   if (!v.empty())
     BSP_CUDA_TRY(cudaMemcpy(d.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return BSP_OK;
+}
+
+template <class Deps>
+static int make_tasks(bsp_precond_s* pc, bool lower, int n, Deps deps) {
+  std::vector<int> row, len;
+  const int nt = build_tasks(n, lower, deps, row, len);
+  if (lower) {
+    pc->n_task_lo = nt;
+    BSP_TRY(upload(pc->task_lo_row, row));
+    BSP_TRY(upload(pc->task_lo_len, len));
+  } else {
+    pc->n_task_up = nt;
+    BSP_TRY(upload(pc->task_up_row, row));
+    BSP_TRY(upload(pc->task_up_len, len));
+  }
   return BSP_OK;
 }
 
@@ -597,6 +722,7 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
   if (!done) {
     static int grid = 0;
     if (!grid) grid = persistent_grid(h, k_sweep_generic<VT, AT, TRANS, POST>, kSweepThreads, 0);
+    p.task_row = nullptr;  // the generic kernel takes one row per ticket
     bsp::count_launch(), k_sweep_generic<VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p, bs);
   }
   BSP_CUDA_TRY(cudaPeekAtLastError());
@@ -641,17 +767,21 @@ static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
   bsp::count_launch(), k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
       pc->f_nnzb, b2, pc->d_perm.get(), A->vals.get(), pc->f_vals.get());
   BSP_CUDA_TRY(cudaPeekAtLastError());
-  // level orders on the sorted structure
+  // level orders and chain tasks on the sorted structure
   std::vector<int> order;
-  pc->n_lev_lo = level_order(n, true, [&](int i, auto&& f) {
+  auto lower_deps = [&](int i, auto&& f) {
     for (int e = ptr[i]; e < diag[i]; ++e) f(col[e]);
-  }, order);
+  };
+  pc->n_lev_lo = level_order(n, true, lower_deps, order);
   BSP_TRY(upload(pc->order_lo, order));
+  BSP_TRY(make_tasks(pc, true, n, lower_deps));
   if (!lower_only) {
-    pc->n_lev_up = level_order(n, false, [&](int i, auto&& f) {
+    auto upper_deps = [&](int i, auto&& f) {
       for (int e = diag[i] + 1; e < ptr[i + 1]; ++e) f(col[e]);
-    }, order);
+    };
+    pc->n_lev_up = level_order(n, false, upper_deps, order);
     BSP_TRY(upload(pc->order_up, order));
+    BSP_TRY(make_tasks(pc, false, n, upper_deps));
   } else {
     // L^T backward: row i depends on rows j > i with L_ji present
     std::vector<int> tp(n + 1, 0);
@@ -668,10 +798,12 @@ static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
         tblk[fill[i]] = e;
         fill[i]++;
       }
-    pc->n_lev_up = level_order(n, false, [&](int i, auto&& f) {
+    auto trans_deps = [&](int i, auto&& f) {
       for (int t = tp[i]; t < tp[i + 1]; ++t) f(trow[t]);
-    }, order);
+    };
+    pc->n_lev_up = level_order(n, false, trans_deps, order);
     BSP_TRY(upload(pc->order_up, order));
+    BSP_TRY(make_tasks(pc, false, n, trans_deps));
     BSP_TRY(upload(pc->t_ptr, tp));
     BSP_TRY(upload(pc->t_row, trow));
     BSP_TRY(upload(pc->t_blk, tblk));
@@ -696,16 +828,20 @@ static int build_diag_inverse(bsp_precond_s* pc) {
     std::vector<int> order;
     const auto& rp = A->h_row_ptr;
     const auto& ci = A->h_col_idx;
-    pc->n_lev_lo = level_order(n, true, [&](int i, auto&& f) {
+    auto lower_deps = [&](int i, auto&& f) {
       for (int t = rp[i]; t < rp[i + 1]; ++t)
         if (ci[t] < i) f(ci[t]);
-    }, order);
-    BSP_TRY(upload(pc->order_lo, order));
-    pc->n_lev_up = level_order(n, false, [&](int i, auto&& f) {
+    };
+    auto upper_deps = [&](int i, auto&& f) {
       for (int t = rp[i]; t < rp[i + 1]; ++t)
         if (ci[t] > i) f(ci[t]);
-    }, order);
+    };
+    pc->n_lev_lo = level_order(n, true, lower_deps, order);
+    BSP_TRY(upload(pc->order_lo, order));
+    BSP_TRY(make_tasks(pc, true, n, lower_deps));
+    pc->n_lev_up = level_order(n, false, upper_deps, order);
     BSP_TRY(upload(pc->order_up, order));
+    BSP_TRY(make_tasks(pc, false, n, upper_deps));
   }
   // makeADInv: invert every diagonal block (rows independent)
   return run_factor(pc, FACT_DIAG, nullptr, A->row_ptr.get(), A->col_idx.get(), pc->a_diag.get(),
@@ -775,6 +911,14 @@ int precond_build(bsp_precond_s* pc) {
 // ---------------------------------------------------------------- apply
 // z = M^{-1} r (z may alias r).  AT = double (FP64) or float (mixed precision).
 template <typename VT, typename AT>
+static void set_tasks(SweepP<VT, AT>& p, const bsp_precond_s* pc, bool lower) {
+  p.task_row = lower ? pc->task_lo_row.get() : pc->task_up_row.get();
+  p.task_len = lower ? pc->task_lo_len.get() : pc->task_up_len.get();
+  p.n_tasks = lower ? pc->n_task_lo : pc->n_task_up;
+  p.task_dir = lower ? 1 : -1;
+}
+
+template <typename VT, typename AT>
 static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, const VT* dinv,
                        const VT* avals, AT* sa, AT* sb) {
   bsp_handle_s* h = pc->h;
@@ -819,6 +963,7 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
         if (last && z == r && xold == nullptr) out = bufs[s & 1];  // nu == 1 in place: keep rhs intact
         p.dep_dir = dirs[s];
         p.order = dirs[s] < 0 ? pc->order_lo.get() : pc->order_up.get();
+        set_tasks(p, pc, dirs[s] < 0);
         p.xold = xold;
         p.x = out;
         BSP_TRY((launch_sweep<VT, AT, false, POST_SOR>(h, bs, p, tk)));
@@ -838,12 +983,14 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       // forward: unit L
       p.range = RANGE_LOWER;
       p.order = pc->order_lo.get();
+      set_tasks(p, pc, true);
       p.rhs = r;
       p.x = z;
       BSP_TRY((launch_sweep<VT, AT, false, POST_NONE>(h, bs, p, tk)));
       // backward: U with inverted diagonal
       p.range = RANGE_UPPER;
       p.order = pc->order_up.get();
+      set_tasks(p, pc, false);
       p.rhs = z;
       p.x = z;
       return launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk);
@@ -857,6 +1004,7 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       p.dinv = dinv;
       p.range = RANGE_LOWER;
       p.order = pc->order_lo.get();
+      set_tasks(p, pc, true);
       p.rhs = r;
       p.x = z;
       BSP_TRY((launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk)));
@@ -866,6 +1014,7 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       p.blk = pc->t_blk.get();
       p.range = RANGE_ALL;
       p.order = pc->order_up.get();
+      set_tasks(p, pc, false);
       p.rhs = z;
       p.x = z;
       return launch_sweep<VT, AT, true, POST_DT>(h, bs, p, tk);
