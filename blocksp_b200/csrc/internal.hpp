@@ -55,6 +55,20 @@ struct Workspace {
   DevBuf<DevStatus> status;  // device error word
 };
 
+// Structure-only analysis behind a preconditioner (sorted factor pattern,
+// permutation, dependency levels, chain tasks).  It depends on the matrix
+// pattern alone, so it is computed once per matrix and kind and reused by
+// every later preconditioner built on the same matrix.
+struct SymbolicCache {
+  bool valid = false;
+  int64_t f_nnzb = 0;
+  int n_lev_lo = 0, n_lev_up = 0, n_task_lo = 0, n_task_up = 0;
+  std::vector<int64_t> h_perm;
+  DevBuf<int> f_ptr, f_col, f_diag, order_lo, order_up, task_lo_row, task_lo_len, task_up_row,
+      task_up_len, t_ptr, t_row, a_diag;
+  DevBuf<int64_t> d_perm, t_blk;
+};
+
 }  // namespace bsp
 
 struct bsp_handle_s {
@@ -91,4 +105,6 @@ struct bsp_matrix_s {
   bsp::DevBuf<int> tr_ptr, tr_row;
   bsp::DevBuf<int64_t> tr_blk;
   bool has_transpose = false;
+  // symbolic analyses for ILU0 (full pattern), IChol0 (lower pattern), SOR/Diag
+  bsp::SymbolicCache sym_ilu, sym_ichol, sym_sor;
 };

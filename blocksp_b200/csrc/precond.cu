@@ -100,7 +100,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
   using CV = typename Chunk<VT>::vec;
   constexpr int V = M::V, G = M::G, P = M::P, CPR = M::CPR, RPP = M::RPP, CPB = M::CPB;
   constexpr int GPC = kSweepThreads / G;
-  constexpr int NPF = 4;  // entries whose blocks are loaded before any wait
+  // entries whose blocks are loaded ahead (for the next row of the chain)
+  constexpr int NPF = (P == 1) ? 4 : (P == 2 ? 2 : 1);
+  constexpr bool kUseD = POST != POST_NONE;
   __shared__ AT sm_s[GPC][BS];
   __shared__ AT sm_x[GPC][BS];  // the group's previous row of its chain
   const int gl = threadIdx.x % G;
@@ -127,27 +129,45 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       i0 = p.order ? __ldg(p.order + t) : t;
       len = 1;
     }
+    // Matrix blocks and inverted diagonals do not depend on the sweep, so the
+    // loads for row step+1 of the chain are issued while row step computes.
+    CV nf[NPF][P], nd[P];
+    int nbeg, nend;
+    auto prefetch = [&](int r, int& b0, int& b1) {
+      row_range(p, r, b0, b1);
+#pragma unroll
+      for (int u = 0; u < NPF; ++u) {
+        if (b0 + u < b1) {
+          const int64_t b = p.blk ? __ldg(p.blk + b0 + u) : (int64_t)(b0 + u);
+#pragma unroll
+          for (int q = 0; q < P; ++q) nf[u][q] = ld_stream(vb + b * CPB + q * G + gl);
+        }
+      }
+      if constexpr (kUseD) {
+        const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)r * CPB;
+#pragma unroll
+        for (int q = 0; q < P; ++q) nd[q] = ld_stream(db + q * G + gl);
+      }
+    };
+    prefetch(i0, nbeg, nend);
    for (int step = 0; step < len; ++step) {
     const int i = i0 + step * p.task_dir;
     const int prev = step > 0 ? i - p.task_dir : -1;
-    int beg, end;
-    row_range(p, i, beg, end);
+    const int beg = nbeg, end = nend;
+    CV pf[NPF][P], pd[P];
+#pragma unroll
+    for (int u = 0; u < NPF; ++u)
+#pragma unroll
+      for (int q = 0; q < P; ++q) pf[u][q] = nf[u][q];
+#pragma unroll
+    for (int q = 0; q < P; ++q) pd[q] = nd[q];
+    if (step + 1 < len) prefetch(i + p.task_dir, nbeg, nend);
     AT acc[P];
     AT tac[V];
 #pragma unroll
     for (int q = 0; q < P; ++q) acc[q] = AT(0);
 #pragma unroll
     for (int v = 0; v < V; ++v) tac[v] = AT(0);
-    // matrix blocks do not depend on the sweep: issue their loads first
-    CV pf[NPF][P];
-#pragma unroll
-    for (int u = 0; u < NPF; ++u) {
-      if (beg + u < end) {
-        const int64_t b = p.blk ? __ldg(p.blk + beg + u) : (int64_t)(beg + u);
-#pragma unroll
-        for (int q = 0; q < P; ++q) pf[u][q] = ld_stream(vb + b * CPB + q * G + gl);
-      }
-    }
     auto consume = [&](int e, const CV (&a)[P]) {
       const int j = __ldg(p.idx + e);
       const AT* src;
@@ -234,7 +254,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         xs[r] = s[r];
       }
     } else if constexpr (POST == POST_D || POST == POST_SOR) {
-      const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)i * CPB;
       AT sv[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) sv[v] = s[c0 + v];
@@ -242,7 +261,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
 #pragma unroll
       for (int q = 0; q < P; ++q) {
         AT av[V];
-        unpack(ld_stream(db + q * G + gl), av);
+        unpack(pd[q], av);
         o[q] = AT(0);
 #pragma unroll
         for (int v = 0; v < V; ++v) o[q] = fma(av[v], sv[v], o[q]);
@@ -263,7 +282,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         }
       }
     } else {  // POST_DT: x = D^T s
-      const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)i * CPB;
       AT o[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) o[v] = AT(0);
@@ -272,7 +290,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         const int r = q * RPP + gl / CPR;
         const AT sr = s[r];
         AT av[V];
-        unpack(ld_stream(db + q * G + gl), av);
+        unpack(pd[q], av);
 #pragma unroll
         for (int v = 0; v < V; ++v) o[v] = fma(av[v], sr, o[v]);
       }
@@ -615,6 +633,40 @@ template <typename T> static int upload(DevBuf<T>& d, const std::vector<T>& v) {
   return BSP_OK;
 }
 
+template <typename T> static int copy_dev(DevBuf<T>& dst, const DevBuf<T>& src, cudaStream_t s) {
+  BSP_TRY(dst.alloc(src.n ? src.n : 1));
+  if (src.n) BSP_CUDA_TRY(cudaMemcpyAsync(dst.get(), src.get(), src.n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  return BSP_OK;
+}
+
+// Preconditioner <-> the matrix's cached symbolic analysis (device-to-device copies).
+static int sym_transfer(bsp_precond_s* pc, SymbolicCache& C, bool save) {
+  cudaStream_t s = pc->h->stream;
+#define BSP_SYM_FIELD(f) BSP_TRY(save ? copy_dev(C.f, pc->f, s) : copy_dev(pc->f, C.f, s));
+  BSP_SYM_FIELD(f_ptr) BSP_SYM_FIELD(f_col) BSP_SYM_FIELD(f_diag) BSP_SYM_FIELD(d_perm)
+  BSP_SYM_FIELD(order_lo) BSP_SYM_FIELD(order_up) BSP_SYM_FIELD(task_lo_row) BSP_SYM_FIELD(task_lo_len)
+  BSP_SYM_FIELD(task_up_row) BSP_SYM_FIELD(task_up_len) BSP_SYM_FIELD(t_ptr) BSP_SYM_FIELD(t_row)
+  BSP_SYM_FIELD(t_blk) BSP_SYM_FIELD(a_diag)
+#undef BSP_SYM_FIELD
+  if (save) {
+    C.h_perm = pc->h_perm;
+    C.f_nnzb = pc->f_nnzb;
+    C.n_lev_lo = pc->n_lev_lo;
+    C.n_lev_up = pc->n_lev_up;
+    C.n_task_lo = pc->n_task_lo;
+    C.n_task_up = pc->n_task_up;
+    C.valid = true;
+  } else {
+    pc->h_perm = C.h_perm;
+    pc->f_nnzb = C.f_nnzb;
+    pc->n_lev_lo = C.n_lev_lo;
+    pc->n_lev_up = C.n_lev_up;
+    pc->n_task_lo = C.n_task_lo;
+    pc->n_task_up = C.n_task_up;
+  }
+  return BSP_OK;
+}
+
 template <class Deps>
 static int make_tasks(bsp_precond_s* pc, bool lower, int n, Deps deps) {
   std::vector<int> row, len;
@@ -703,9 +755,11 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
   BSP_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), h->stream));
   constexpr int V = Chunk<VT>::V;
   bool done = false;
+  // blocks of more than 4 chunk passes per lane (bs 32 in FP64) would not fit
+  // the double-buffered registers: they use the generic kernel
 #define BSP_SWEEP_CASE(B)                                          \
   case B:                                                          \
-    if constexpr (B % V == 0) {                                    \
+    if constexpr (B % V == 0 && (B * B / V) / ((B * B / V) < 32 ? (B * B / V) : 32) <= 4) { \
       launch_sweep_t<B, VT, AT, TRANS, POST>(h, p);                \
       done = true;                                                 \
     }                                                              \
@@ -730,7 +784,7 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
 }
 
 // ---------------------------------------------------------------- build
-static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
+static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
   const bsp_matrix_s* A = pc->A;
   const int n = A->n_rows;
   std::vector<int> ptr(n + 1, 0), col, diag(n, -1);
@@ -762,11 +816,6 @@ static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
   BSP_TRY(upload(pc->f_col, col));
   BSP_TRY(upload(pc->f_diag, diag));
   BSP_TRY(upload(pc->d_perm, perm));
-  const int b2 = pc->bs * pc->bs;
-  BSP_TRY(pc->f_vals.alloc(pc->f_nnzb * b2));
-  bsp::count_launch(), k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
-      pc->f_nnzb, b2, pc->d_perm.get(), A->vals.get(), pc->f_vals.get());
-  BSP_CUDA_TRY(cudaPeekAtLastError());
   // level orders and chain tasks on the sorted structure
   std::vector<int> order;
   auto lower_deps = [&](int i, auto&& f) {
@@ -811,7 +860,25 @@ static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
   return BSP_OK;
 }
 
-static int build_diag_inverse(bsp_precond_s* pc) {
+// Factor storage for ILU0 / IChol0: the symbolic part from the matrix's cache
+// (computed on first use), then A's values gathered into it on the device.
+static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
+  SymbolicCache& C = lower_only ? pc->A->sym_ichol : pc->A->sym_ilu;
+  if (C.valid) {
+    BSP_TRY(sym_transfer(pc, C, false));
+  } else {
+    BSP_TRY(analyse_factor_structure(pc, lower_only));
+    BSP_TRY(sym_transfer(pc, C, true));
+  }
+  const int b2 = pc->bs * pc->bs;
+  BSP_TRY(pc->f_vals.alloc(pc->f_nnzb * b2));
+  bsp::count_launch(), k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
+      pc->f_nnzb, b2, pc->d_perm.get(), pc->A->vals.get(), pc->f_vals.get());
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+static int analyse_diag_structure(bsp_precond_s* pc) {
   const bsp_matrix_s* A = pc->A;
   const int n = A->n_rows;
   std::vector<int> diag(n, -1);
@@ -843,9 +910,21 @@ static int build_diag_inverse(bsp_precond_s* pc) {
     BSP_TRY(upload(pc->order_up, order));
     BSP_TRY(make_tasks(pc, false, n, upper_deps));
   }
+  return BSP_OK;
+}
+
+static int build_diag_inverse(bsp_precond_s* pc) {
+  SymbolicCache& C = pc->A->sym_sor;
+  const bool sor = pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL;
+  if (C.valid && (!sor || C.n_task_lo > 0)) {
+    BSP_TRY(sym_transfer(pc, C, false));
+  } else {
+    BSP_TRY(analyse_diag_structure(pc));
+    BSP_TRY(sym_transfer(pc, C, true));
+  }
   // makeADInv: invert every diagonal block (rows independent)
-  return run_factor(pc, FACT_DIAG, nullptr, A->row_ptr.get(), A->col_idx.get(), pc->a_diag.get(),
-                    A->vals.get(), n);
+  return run_factor(pc, FACT_DIAG, nullptr, pc->A->row_ptr.get(), pc->A->col_idx.get(), pc->a_diag.get(),
+                    pc->A->vals.get(), pc->n);
 }
 
 static int make_lowp_copies(bsp_precond_s* pc) {
