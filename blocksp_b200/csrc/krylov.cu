@@ -71,13 +71,51 @@ __global__ void k_cg_p(int64_t n, const double* __restrict__ z, const KHead* __r
     p[i] = z[i] + beta * p[i];
 }
 
+// ---- 4-element chunks: the reduction bodies below take a chunk index c and
+// handle elements 4c .. 4c+3 (fewer at the tail), issuing every load of the
+// chunk before the arithmetic so that a read-modify-write of one vector does
+// not serialise the loads of the next elements behind it.
+constexpr int kC = 4;
+inline int64_t chunks_of(int64_t n) { return (n + kC - 1) / kC; }
+
+struct V4 {
+  double v[kC];
+};
+__device__ __forceinline__ V4 ld4(const double* p, int64_t e, int64_t n) {
+  V4 r;
+  if (e + kC <= n) {
+    const double2 a = *reinterpret_cast<const double2*>(p + e);
+    const double2 b = *reinterpret_cast<const double2*>(p + e + 2);
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kC; ++k) r.v[k] = (e + k < n) ? p[e + k] : 0.0;
+  }
+  return r;
+}
+__device__ __forceinline__ void st4(double* p, int64_t e, int64_t n, const V4& r) {
+  if (e + kC <= n) {
+    *reinterpret_cast<double2*>(p + e) = make_double2(r.v[0], r.v[1]);
+    *reinterpret_cast<double2*>(p + e + 2) = make_double2(r.v[2], r.v[3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kC; ++k)
+      if (e + k < n) p[e + k] = r.v[k];
+  }
+}
+
 // ---- reduction bodies / finalisers (pCG) ----
 struct CgInitBody {  // sums p.p and r.z  (z == p initially)
   const double *p, *r;
+  int64_t n;
   __device__ void setup() {}
-  __device__ void operator()(int64_t i, double (&a)[2]) const {
-    a[0] = fma(p[i], p[i], a[0]);
-    a[1] = fma(r[i], p[i], a[1]);
+  __device__ void operator()(int64_t c, double (&a)[2]) const {
+    const V4 pv = ld4(p, c * kC, n), rv = ld4(r, c * kC, n);
+#pragma unroll
+    for (int k = 0; k < kC; ++k) {
+      a[0] = fma(pv.v[k], pv.v[k], a[0]);
+      a[1] = fma(rv.v[k], pv.v[k], a[1]);
+    }
   }
 };
 struct CgInitFin {
@@ -99,8 +137,13 @@ struct CgInitFin {
 };
 struct CgPApBody {
   const double *p, *Ap;
+  int64_t n;
   __device__ void setup() {}
-  __device__ void operator()(int64_t i, double (&a)[1]) const { a[0] = fma(p[i], Ap[i], a[0]); }
+  __device__ void operator()(int64_t c, double (&a)[1]) const {
+    const V4 pv = ld4(p, c * kC, n), av = ld4(Ap, c * kC, n);
+#pragma unroll
+    for (int k = 0; k < kC; ++k) a[0] = fma(pv.v[k], av.v[k], a[0]);
+  }
 };
 struct CgPApFin {
   KHead* head;
@@ -114,12 +157,20 @@ struct CgUpdBody {  // x += alpha p; r -= alpha Ap; sum r.r
   const double *p, *Ap;
   const KHead* head;
   double alpha;
+  int64_t n;
   __device__ void setup() { alpha = head->alpha; }
-  __device__ void operator()(int64_t i, double (&a)[1]) {
-    x[i] += alpha * p[i];
-    const double ri = r[i] - alpha * Ap[i];
-    r[i] = ri;
-    a[0] = fma(ri, ri, a[0]);
+  __device__ void operator()(int64_t c, double (&a)[1]) {
+    const int64_t e = c * kC;
+    V4 xv = ld4(x, e, n), rv = ld4(r, e, n);
+    const V4 pv = ld4(p, e, n), av = ld4(Ap, e, n);
+#pragma unroll
+    for (int k = 0; k < kC; ++k) {
+      xv.v[k] += alpha * pv.v[k];
+      rv.v[k] = rv.v[k] - alpha * av.v[k];
+      a[0] = fma(rv.v[k], rv.v[k], a[0]);
+    }
+    st4(x, e, n, xv);
+    st4(r, e, n, rv);
   }
 };
 struct CgUpdFin {
@@ -137,8 +188,13 @@ struct CgUpdFin {
 };
 struct CgRzBody {
   const double *r, *z;
+  int64_t n;
   __device__ void setup() {}
-  __device__ void operator()(int64_t i, double (&a)[1]) const { a[0] = fma(r[i], z[i], a[0]); }
+  __device__ void operator()(int64_t c, double (&a)[1]) const {
+    const V4 rv = ld4(r, c * kC, n), zv = ld4(z, c * kC, n);
+#pragma unroll
+    for (int k = 0; k < kC; ++k) a[0] = fma(rv.v[k], zv.v[k], a[0]);
+  }
 };
 struct CgRzFin {
   KHead* head;
@@ -162,14 +218,20 @@ struct MgsBody {
   const double *qprev, *qi;
   const double* hprev_ptr;
   double hprev;
+  int64_t n;
   __device__ void setup() { hprev = qprev ? *hprev_ptr : 0.0; }
-  __device__ void operator()(int64_t e, double (&a)[1]) {
-    double ve = v[e];
+  __device__ void operator()(int64_t c, double (&a)[1]) {
+    const int64_t e = c * kC;
+    V4 vv = ld4(v, e, n);
+    const V4 qv = ld4(qi, e, n);
     if (qprev) {
-      ve = fma(-hprev, qprev[e], ve);
-      v[e] = ve;
+      const V4 pv = ld4(qprev, e, n);
+#pragma unroll
+      for (int k = 0; k < kC; ++k) vv.v[k] = fma(-hprev, pv.v[k], vv.v[k]);
+      st4(v, e, n, vv);
     }
-    a[0] = fma(qi[e], ve, a[0]);
+#pragma unroll
+    for (int k = 0; k < kC; ++k) a[0] = fma(qv.v[k], vv.v[k], a[0]);
   }
 };
 // last pass: v -= H(j, j) q_j; H(j+1, j) = ||v||
@@ -178,11 +240,18 @@ struct MgsLastBody {
   const double* qj;
   const double* h_ptr;
   double h;
+  int64_t n;
   __device__ void setup() { h = *h_ptr; }
-  __device__ void operator()(int64_t e, double (&a)[1]) {
-    const double ve = fma(-h, qj[e], v[e]);
-    v[e] = ve;
-    a[0] = fma(ve, ve, a[0]);
+  __device__ void operator()(int64_t c, double (&a)[1]) {
+    const int64_t e = c * kC;
+    V4 vv = ld4(v, e, n);
+    const V4 qv = ld4(qj, e, n);
+#pragma unroll
+    for (int k = 0; k < kC; ++k) {
+      vv.v[k] = fma(-h, qv.v[k], vv.v[k]);
+      a[0] = fma(vv.v[k], vv.v[k], a[0]);
+    }
+    st4(v, e, n, vv);
   }
 };
 
@@ -464,19 +533,19 @@ int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double*
   if (pc) BSP_TRY(precond_apply(pc, op_prec,b, vp.get()));              // p = M^-1 b
   else bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, b, vp.get());
   bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, vp.get(), vz.get());                  // z = p
-  BSP_TRY(launch_reduce<2>(h, 3, len, CgInitBody{vp.get(), vr.get()}, CgInitFin{hd, o->tol, dhist.get()}));
+  BSP_TRY(launch_reduce<2>(h, 3, chunks_of(len), CgInitBody{vp.get(), vr.get(), len}, CgInitFin{hd, o->tol, dhist.get()}));
   KHead st;
   BSP_TRY(read_head(h, hd, &st));
   while (st.done == DONE_RUNNING) {
     BSP_TRY(bsmv_launch(A, 1, 0, op_dtype, 1.0,vp.get(), 0.0, nullptr, vAp.get(), h->stream));
-    BSP_TRY(launch_reduce<1>(h, 4, len, CgPApBody{vp.get(), vAp.get()}, CgPApFin{hd}));
-    BSP_TRY(launch_reduce<1>(h, 5, len, CgUpdBody{x, vr.get(), vp.get(), vAp.get(), hd, 0.0},
+    BSP_TRY(launch_reduce<1>(h, 4, chunks_of(len), CgPApBody{vp.get(), vAp.get(), len}, CgPApFin{hd}));
+    BSP_TRY(launch_reduce<1>(h, 5, chunks_of(len), CgUpdBody{x, vr.get(), vp.get(), vAp.get(), hd, 0.0, len},
                              CgUpdFin{hd, dhist.get(), hcap}));
     BSP_TRY(read_head(h, hd, &st));
     if (st.done != DONE_RUNNING) break;
     if (pc) BSP_TRY(precond_apply(pc, op_prec,vr.get(), vz.get()));
     else bsp::count_launch(), k_copy<<<g, 256, 0, h->stream>>>(len, vr.get(), vz.get());
-    BSP_TRY(launch_reduce<1>(h, 6, len, CgRzBody{vr.get(), vz.get()}, CgRzFin{hd, o->max_iters}));
+    BSP_TRY(launch_reduce<1>(h, 6, chunks_of(len), CgRzBody{vr.get(), vz.get(), len}, CgRzFin{hd, o->max_iters}));
     bsp::count_launch(), k_cg_p<<<g, 256, 0, h->stream>>>(len, vz.get(), hd, vp.get());
     BSP_CUDA_TRY(cudaPeekAtLastError());
     BSP_TRY(read_head(h, hd, &st));
@@ -621,10 +690,10 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     // MGS: j+2 fused passes
     for (int i = 0; i <= j; ++i) {
       MgsBody body{vv.get(), i > 0 ? qptr[i - 1] : nullptr, qptr[i],
-                   i > 0 ? gp.H + (size_t)(i - 1) * m + j : nullptr, 0.0};
-      BSP_TRY(launch_reduce<1>(h, 8 + (i & 1), len, body, StoreFin{gp.H + (size_t)i * m + j}));
+                   i > 0 ? gp.H + (size_t)(i - 1) * m + j : nullptr, 0.0, len};
+      BSP_TRY(launch_reduce<1>(h, 8 + (i & 1), chunks_of(len), body, StoreFin{gp.H + (size_t)i * m + j}));
     }
-    BSP_TRY(launch_reduce<1>(h, 10, len, MgsLastBody{vv.get(), qptr[j], gp.H + (size_t)j * m + j, 0.0},
+    BSP_TRY(launch_reduce<1>(h, 10, chunks_of(len), MgsLastBody{vv.get(), qptr[j], gp.H + (size_t)j * m + j, 0.0, len},
                              NormFin{gp.H + (size_t)(j + 1) * m + j}));
     bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vv.get(), gp.H + (size_t)(j + 1) * m + j, hd, qptr[j + 1]);
     bsp::count_launch(), k_gm_ls<<<1, 1, 0, h->stream>>>(gp, o->max_iters);

@@ -49,6 +49,37 @@ __device__ __forceinline__ void wait_flag(const int* f, int epoch, DevStatus* st
   }
 }
 
+// ----------------------------------------------------------------- sentinel
+// A sweep's output vector is filled with a signalling-NaN bit pattern before
+// the launch.  Arithmetic never produces it (NaN results are quiet), so a row
+// is final exactly when its words differ from the pattern.  Aligned 8- and
+// 4-byte accesses are single-copy atomic, so a reader never sees half a value.
+constexpr unsigned long long kSentinel64 = 0x7FF4B5B5B5B5B5B5ull;
+constexpr unsigned kSentinel32 = 0x7FA5B5B5u;
+__device__ __forceinline__ bool is_sentinel(double v) {
+  return (unsigned long long)__double_as_longlong(v) == kSentinel64;
+}
+__device__ __forceinline__ bool is_sentinel(float v) { return __float_as_uint(v) == kSentinel32; }
+// Re-reads inside a polling loop: relaxed loads at GPU scope, never merged.
+__device__ __forceinline__ double ld_poll(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_poll(const float* p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__global__ void k_fill_sentinel64(int64_t n, unsigned long long* __restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = kSentinel64;
+}
+__global__ void k_fill_sentinel32(int64_t n, unsigned* __restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = kSentinel32;
+}
+
 // ----------------------------------------------------------------- sweeps
 enum { RANGE_LOWER = 0, RANGE_UPPER = 1, RANGE_SPLIT = 2, RANGE_ALL = 3, RANGE_NONE = 4 };
 enum { POST_NONE = 0, POST_D = 1, POST_DT = 2, POST_SOR = 3 };
@@ -168,34 +199,64 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
     for (int q = 0; q < P; ++q) acc[q] = AT(0);
 #pragma unroll
     for (int v = 0; v < V; ++v) tac[v] = AT(0);
-    auto consume = [&](int e, const CV (&a)[P]) {
-      const int j = __ldg(p.idx + e);
-      const AT* src;
-      bool from_prev = false;
+    // Entry classes: 0 skip, 1 the chain's previous row (shared memory),
+    // 2 a row of this sweep (polled until it is no longer the sentinel),
+    // 3 the previous iterate (SOR, final values).
+    constexpr int XV = TRANS ? P : V;  // x values a lane reads per entry
+    auto classify = [&](int e, int& j) -> int {
+      j = __ldg(p.idx + e);
       if (p.range == RANGE_SPLIT) {
-        if (j == i) return;
+        if (j == i) return 0;
         const bool dep = (p.dep_dir < 0) ? (j < i) : (j > i);
-        if (dep) {
-          from_prev = (j == prev);
-          if (!from_prev) wait_flag(p.flags + j, p.epoch, p.st, i);
-          src = p.x;
-        } else {
-          if (!p.xold) return;
-          src = p.xold;
-        }
-      } else {
-        from_prev = (j == prev);
-        if (!from_prev) wait_flag(p.flags + j, p.epoch, p.st, i);
-        src = p.x;
+        if (!dep) return p.xold ? 3 : 0;
       }
+      return j == prev ? 1 : 2;
+    };
+    auto load_x = [&](int kind, int j, AT (&xv)[XV]) {
+      const AT* src = kind == 3 ? p.xold : p.x;
       if constexpr (!TRANS) {
-        AT xv[V];
-        if (from_prev) {
+        if (kind == 1) {
 #pragma unroll
           for (int v = 0; v < V; ++v) xv[v] = xs[c0 + v];
         } else {
           ld_vec_cg<V>(src + (int64_t)j * BS + c0, xv);
         }
+      } else {
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const int r = q * RPP + gl / CPR;
+          xv[q] = kind == 1 ? xs[r] : __ldcg(src + (int64_t)j * BS + r);
+        }
+      }
+    };
+    auto poll_x = [&](int j, AT (&xv)[XV]) {
+      bool pending = false;
+#pragma unroll
+      for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
+      unsigned spins = 0;
+      while (pending) {
+        __nanosleep(32);
+        if constexpr (!TRANS) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) xv[v] = ld_poll(p.x + (int64_t)j * BS + c0 + v);
+        } else {
+#pragma unroll
+          for (int q = 0; q < P; ++q) xv[q] = ld_poll(p.x + (int64_t)j * BS + q * RPP + gl / CPR);
+        }
+        pending = false;
+#pragma unroll
+        for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
+        if (pending && (++spins & 255u) == 0u) {
+          if (*reinterpret_cast<volatile int*>(&p.st->code) != 0) break;  // already failed
+          if (spins > kSpinLimit) {
+            set_status(p.st, BSP_TIMEOUT, i);
+            break;
+          }
+        }
+      }
+    };
+    auto fma_entry = [&](const CV (&a)[P], const AT (&xv)[XV]) {
+      if constexpr (!TRANS) {
 #pragma unroll
         for (int q = 0; q < P; ++q) {
           AT av[V];
@@ -206,24 +267,41 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       } else {
 #pragma unroll
         for (int q = 0; q < P; ++q) {
-          const int r = q * RPP + gl / CPR;
-          const AT xr = from_prev ? xs[r] : __ldcg(src + (int64_t)j * BS + r);
           AT av[V];
           unpack(a[q], av);
 #pragma unroll
-          for (int v = 0; v < V; ++v) tac[v] = fma(av[v], xr, tac[v]);
+          for (int v = 0; v < V; ++v) tac[v] = fma(av[v], xv[q], tac[v]);
         }
       }
     };
+    // first NPF entries: issue every dependency load, then poll the ones
+    // that are not final yet, so their round trips overlap
+    {
+      AT xv[NPF][XV];
+      int kind[NPF], jj[NPF];
 #pragma unroll
-    for (int u = 0; u < NPF; ++u)
-      if (beg + u < end) consume(beg + u, pf[u]);
+      for (int u = 0; u < NPF; ++u) {
+        kind[u] = (beg + u < end) ? classify(beg + u, jj[u]) : 0;
+        if (kind[u]) load_x(kind[u], jj[u], xv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < NPF; ++u) {
+        if (kind[u] == 2) poll_x(jj[u], xv[u]);
+        if (kind[u]) fma_entry(pf[u], xv[u]);
+      }
+    }
     for (int e = beg + NPF; e < end; ++e) {
+      int j;
+      const int kind = classify(e, j);
+      if (!kind) continue;
       const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
       CV a[P];
 #pragma unroll
       for (int q = 0; q < P; ++q) a[q] = ld_stream(vb + b * CPB + q * G + gl);
-      consume(e, a);
+      AT xv[XV];
+      load_x(kind, j, xv);
+      if (kind == 2) poll_x(j, xv);
+      fma_entry(a, xv);
     }
     // s = rhs_i - sum  (in shared memory, BS values per group)
     if constexpr (!TRANS) {
@@ -306,13 +384,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         }
       }
     }
-    // publish row i: the lanes' stores are ordered before lane 0's release by
-    // the warp barrier, and the fence makes them visible at GPU scope first
-    __syncwarp(gmask);
-    if (gl == 0) {
-      __threadfence();
-      st_release(p.flags + i, p.epoch);
-    }
+    // Row i is published by its values themselves: readers poll the 8-byte
+    // words until they are no longer the sentinel, so no flag or fence is
+    // needed.  The barrier keeps shared memory consistent for the next row.
     __syncwarp(gmask);
    }
   }
@@ -337,18 +411,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_generic(const SweepP<VT
     for (int e = beg; e < end; ++e) {
       const int j = __ldg(p.idx + e);
       const AT* src;
+      bool poll = true;
       if (p.range == RANGE_SPLIT) {
         if (j == i) continue;
         const bool dep = (p.dep_dir < 0) ? (j < i) : (j > i);
         if (dep) {
-          wait_flag(p.flags + j, p.epoch, p.st, i);
           src = p.x;
         } else {
           if (!p.xold) continue;
           src = p.xold;
+          poll = false;
         }
       } else {
-        wait_flag(p.flags + j, p.epoch, p.st, i);
         src = p.x;
       }
       const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
@@ -356,7 +430,22 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_generic(const SweepP<VT
         const VT* a = p.vals + b * b2;
         for (int c = 0; c < bs; ++c) {
           const AT m = TRANS ? AT(a[c * bs + lane]) : AT(a[lane * bs + c]);
-          acc = fma(m, __ldcg(src + (int64_t)j * bs + c), acc);
+          AT xc = __ldcg(src + (int64_t)j * bs + c);
+          if (poll) {
+            unsigned spins = 0;
+            while (is_sentinel(xc)) {  // row j of this sweep not final yet
+              __nanosleep(32);
+              xc = ld_poll(src + (int64_t)j * bs + c);
+              if ((++spins & 255u) == 0u) {
+                if (*reinterpret_cast<volatile int*>(&p.st->code) != 0) break;
+                if (spins > kSpinLimit) {
+                  set_status(p.st, BSP_TIMEOUT, i);
+                  break;
+                }
+              }
+            }
+          }
+          acc = fma(m, xc, acc);
         }
       }
     }
@@ -378,9 +467,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_generic(const SweepP<VT
       }
       p.x[(int64_t)i * bs + lane] = val;
     }
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) st_release(p.flags + i, p.epoch);
     __syncwarp();
   }
 }
@@ -542,9 +628,10 @@ struct bsp_precond_s {
   // sync-free state
   DevBuf<int> flags;
   DevBuf<unsigned> ticket;
-  // SOR ping-pong iterates
-  DevBuf<double> sor_a, sor_b;
-  DevBuf<float> sor_a32, sor_b32;
+  // apply scratch: sweep outputs (pre-filled with the sentinel), SOR ping-pong
+  // iterates and the copy of an in-place right-hand side
+  DevBuf<double> s64[3];
+  DevBuf<float> s32[3];
 };
 
 namespace bsp {
@@ -965,10 +1052,6 @@ int precond_build(bsp_precond_s* pc) {
     case BSP_PC_SOR_LU:
     case BSP_PC_SOR_CHOL:
       BSP_TRY(build_diag_inverse(pc));
-      if (pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL) {
-        BSP_TRY(pc->sor_a.alloc((size_t)n * pc->bs));
-        BSP_TRY(pc->sor_b.alloc((size_t)n * pc->bs));
-      }
       break;
     case BSP_PC_ILU0:
       BSP_TRY(build_factor_structure(pc, false));
@@ -997,12 +1080,27 @@ static void set_tasks(SweepP<VT, AT>& p, const bsp_precond_s* pc, bool lower) {
   p.task_dir = lower ? 1 : -1;
 }
 
+template <typename AT> static int fill_sentinel(bsp_handle_s* h, AT* x, int64_t count) {
+  if constexpr (sizeof(AT) == 8)
+    bsp::count_launch(), k_fill_sentinel64<<<grid_for(h, count, 256), 256, 0, h->stream>>>(
+        count, reinterpret_cast<unsigned long long*>(x));
+  else
+    bsp::count_launch(), k_fill_sentinel32<<<grid_for(h, count, 256), 256, 0, h->stream>>>(
+        count, reinterpret_cast<unsigned*>(x));
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+// z = M^{-1} r (z may alias r).  Every sweep with dependencies writes into a
+// buffer pre-filled with the sentinel and reads its right-hand side from a
+// different buffer; sa, sb, sc are scratch vectors of n*bs values.
 template <typename VT, typename AT>
 static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, const VT* dinv,
-                       const VT* avals, AT* sa, AT* sb) {
+                       const VT* avals, AT* sa, AT* sb, AT* sc) {
   bsp_handle_s* h = pc->h;
   const bsp_matrix_s* A = pc->A;
   const int n = pc->n, bs = pc->bs;
+  const int64_t nv = (int64_t)n * bs;
   unsigned* tk = pc->ticket.get();
   SweepP<VT, AT> p{};
   p.n = n;
@@ -1028,8 +1126,13 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       p.range = RANGE_SPLIT;
       p.vals = avals;
       p.dinv = dinv;
-      p.rhs = r;
       p.w = (AT)pc->w;
+      const AT* rhs = r;
+      if (z == r) {  // in place: keep a copy of the right-hand side
+        BSP_CUDA_TRY(cudaMemcpyAsync(sc, r, nv * sizeof(AT), cudaMemcpyDeviceToDevice, h->stream));
+        rhs = sc;
+      }
+      p.rhs = rhs;
       std::vector<int> dirs;
       if (pc->type < 0) dirs.assign(pc->nu, +1);
       else if (pc->type == 0) { dirs.assign(pc->nu, -1); dirs.insert(dirs.end(), pc->nu, +1); }
@@ -1039,7 +1142,7 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       for (size_t s = 0; s < dirs.size(); ++s) {
         const bool last = s + 1 == dirs.size();
         AT* out = last ? z : bufs[s & 1];
-        if (last && z == r && xold == nullptr) out = bufs[s & 1];  // nu == 1 in place: keep rhs intact
+        BSP_TRY(fill_sentinel(h, out, nv));
         p.dep_dir = dirs[s];
         p.order = dirs[s] < 0 ? pc->order_lo.get() : pc->order_up.get();
         set_tasks(p, pc, dirs[s] < 0);
@@ -1048,8 +1151,6 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
         BSP_TRY((launch_sweep<VT, AT, false, POST_SOR>(h, bs, p, tk)));
         xold = out;
       }
-      if (xold != z)
-        BSP_CUDA_TRY(cudaMemcpyAsync(z, xold, (size_t)n * bs * sizeof(AT), cudaMemcpyDeviceToDevice, h->stream));
       return BSP_OK;
     }
     case BSP_PC_ILU0:
@@ -1064,14 +1165,16 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       p.order = pc->order_lo.get();
       set_tasks(p, pc, true);
       p.rhs = r;
-      p.x = z;
+      p.x = sa;
+      BSP_TRY(fill_sentinel(h, sa, nv));
       BSP_TRY((launch_sweep<VT, AT, false, POST_NONE>(h, bs, p, tk)));
       // backward: U with inverted diagonal
       p.range = RANGE_UPPER;
       p.order = pc->order_up.get();
       set_tasks(p, pc, false);
-      p.rhs = z;
+      p.rhs = sa;
       p.x = z;
+      BSP_TRY(fill_sentinel(h, z, nv));
       return launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk);
     }
     case BSP_PC_ICHOL0:
@@ -1085,7 +1188,8 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       p.order = pc->order_lo.get();
       set_tasks(p, pc, true);
       p.rhs = r;
-      p.x = z;
+      p.x = sa;
+      BSP_TRY(fill_sentinel(h, sa, nv));
       BSP_TRY((launch_sweep<VT, AT, false, POST_D>(h, bs, p, tk)));
       // backward: L^T through the transposed structure, diagonal L_ii^{-T}
       p.ptr = pc->t_ptr.get();
@@ -1094,8 +1198,9 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
       p.range = RANGE_ALL;
       p.order = pc->order_up.get();
       set_tasks(p, pc, false);
-      p.rhs = z;
+      p.rhs = sa;
       p.x = z;
+      BSP_TRY(fill_sentinel(h, z, nv));
       return launch_sweep<VT, AT, true, POST_DT>(h, bs, p, tk);
     }
     default:
@@ -1107,39 +1212,30 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
 // vec64 selects FP64 vectors (the Krylov path, always FP64 accumulation) or
 // FP32 vectors (low-precision vectors, FP32 accumulation).
 int precond_apply_typed(bsp_precond_s* pc, int precision, bool vec64, const void* r, void* z) {
-  if (precision == BSP_PREC_F64) {
-    return apply_typed<double, double>(pc, (const double*)r, (double*)z, pc->f_vals.get(),
-                                       pc->dinv.get(), pc->A->vals.get(), pc->sor_a.get(),
-                                       pc->sor_b.get());
-  }
-  const size_t nv = (size_t)pc->n * pc->bs;
-  const bool sor = pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL;
+  const size_t nv = (size_t)std::max(pc->n, 1) * pc->bs;
   if (precision == BSP_PREC_F32 && !pc->dinv32.get()) return BSP_INVALID;
   if (precision == BSP_PREC_BF16 && !pc->dinv16.get()) return BSP_INVALID;
-  if (vec64) {
-    if (sor && pc->sor_a.n < nv) {
-      BSP_TRY(pc->sor_a.alloc(nv));
-      BSP_TRY(pc->sor_b.alloc(nv));
-    }
+  if (precision == BSP_PREC_F64 || vec64) {
+    for (auto& s : pc->s64)
+      if (s.n < nv) BSP_TRY(s.alloc(nv));
+    double *a = pc->s64[0].get(), *b = pc->s64[1].get(), *c = pc->s64[2].get();
+    if (precision == BSP_PREC_F64)
+      return apply_typed<double, double>(pc, (const double*)r, (double*)z, pc->f_vals.get(),
+                                         pc->dinv.get(), pc->A->vals.get(), a, b, c);
     if (precision == BSP_PREC_F32)
       return apply_typed<float, double>(pc, (const double*)r, (double*)z, pc->f_vals32.get(),
-                                        pc->dinv32.get(), pc->A->vals32.get(), pc->sor_a.get(),
-                                        pc->sor_b.get());
+                                        pc->dinv32.get(), pc->A->vals32.get(), a, b, c);
     return apply_typed<__nv_bfloat16, double>(pc, (const double*)r, (double*)z, pc->f_vals16.get(),
-                                              pc->dinv16.get(), pc->A->vals16.get(),
-                                              pc->sor_a.get(), pc->sor_b.get());
+                                              pc->dinv16.get(), pc->A->vals16.get(), a, b, c);
   }
-  if (sor && pc->sor_a32.n < nv) {
-    BSP_TRY(pc->sor_a32.alloc(nv));
-    BSP_TRY(pc->sor_b32.alloc(nv));
-  }
+  for (auto& s : pc->s32)
+    if (s.n < nv) BSP_TRY(s.alloc(nv));
+  float *a = pc->s32[0].get(), *b = pc->s32[1].get(), *c = pc->s32[2].get();
   if (precision == BSP_PREC_F32)
     return apply_typed<float, float>(pc, (const float*)r, (float*)z, pc->f_vals32.get(),
-                                     pc->dinv32.get(), pc->A->vals32.get(), pc->sor_a32.get(),
-                                     pc->sor_b32.get());
+                                     pc->dinv32.get(), pc->A->vals32.get(), a, b, c);
   return apply_typed<__nv_bfloat16, float>(pc, (const float*)r, (float*)z, pc->f_vals16.get(),
-                                           pc->dinv16.get(), pc->A->vals16.get(),
-                                           pc->sor_a32.get(), pc->sor_b32.get());
+                                           pc->dinv16.get(), pc->A->vals16.get(), a, b, c);
 }
 
 int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z) {
