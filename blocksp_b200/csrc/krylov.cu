@@ -13,8 +13,8 @@
 //     column per iteration (the reference re-solves it with gels each time;
 //     both give the minimiser of the same problem),
 //   * the deflated restart (harmonic Ritz values, Schur form, selection,
-//     invariant subspace, P_{k+1}, c_r, H_new) runs on one GPU thread in
-//     small_dense.h, and Qn <- Qn P_{k+1} is a tall-skinny in-place kernel.
+//     invariant subspace, P_{k+1}, c_r, H_new) runs on one GPU warp in
+//     small_dense.h (working set in shared memory), and Qn <- Qn P_{k+1} is a tall-skinny in-place kernel.
 #include <algorithm>
 #include <vector>
 #include "reduce.cuh"
@@ -326,91 +326,141 @@ __global__ void k_gm_combine(int64_t len, double* __restrict__ x, double* const*
   }
 }
 
-// Deflated restart (deflated_restart.hpp:38-269) on one thread.
+// Shared-memory footprint (doubles, then ints) of the deflated restart's
+// working set for restart length m; the kernel stages it in shared memory
+// when it fits and otherwise works in the global scratch.
+inline size_t deflate_smem_bytes(int m) {
+  const size_t d = (size_t)m * m * 2 + ((size_t)m * m + 4 * (size_t)m + 32) + (size_t)(m + 1) * (m + 2) +
+                   3 * (size_t)(m + 1) + (size_t)(m + 2);
+  return d * sizeof(double) + 2 * (size_t)m * sizeof(int);
+}
+constexpr size_t kDeflateSmemMax = 200 * 1024;
+
+// Deflated restart (deflated_restart.hpp:38-269) on one warp.
 // Input: H ((n+1) x n, n = head->j), rhs, y (current LS solution), k.
 // Output: P_{k+1} in g.P ((n+1) x (keff+1), ld = m+1), H_new, c_r, new LS state.
-__global__ void k_gm_deflate(GPtrs g, int k_req, int max_keep) {
+__global__ void __launch_bounds__(32) k_gm_deflate(GPtrs g, int k_req, int max_keep, int use_smem) {
+  extern __shared__ __align__(16) double dsm[];
+  const sd::WarpTeam tm;
+  const int r0 = tm.rank(), ns = tm.size();
   KHead* h = g.head;
   const int n = h->j, m1 = n + 1, ld = g.m;
   int k = k_req > n ? n : k_req;
+  // working arrays: shared memory when they fit, else the global scratch
+  GPtrs L = g;
+  if (use_smem) {
+    double* b = dsm;
+    const int m = g.m;
+    L.Hn = b; b += (size_t)m * m;
+    L.Z = b; b += (size_t)m * m;
+    L.work = b; b += (size_t)m * m + 4 * (size_t)m + 32;
+    L.P = b; b += (size_t)(m + 1) * (m + 2);
+    L.w = b; b += m + 1;
+    L.wr = b; b += m + 1;
+    L.wi = b; b += m + 1;
+    L.resv = b; b += m + 2;
+    L.perm = reinterpret_cast<int*>(b);
+    L.sel = L.perm + m;
+  }
   // residual vector res_vec = rhs - H y (solvers.hpp:202-203, 226-227)
-  for (int i = 0; i < m1; ++i) {
+  for (int i = r0; i < m1; i += ns) {
     double s = 0.0;
     for (int t = 0; t < n; ++t) s += g.H[i * ld + t] * g.y[t];
-    g.resv[i] = g.rhs[i] - s;
+    L.resv[i] = g.rhs[i] - s;
   }
   const double zero_thresh = 10.0 * n * n * kEps;
   // (1) H_tilde = H_n + |h_mn|^2 H_n^{-T} e_n e_n^T
   const int ldn = g.m;
-  for (int i = 0; i < n; ++i)
-    for (int t = 0; t < n; ++t) g.Hn[i * ldn + t] = g.H[i * ld + t];
+  for (int e = r0; e < n * n; e += ns) {
+    const int i = e / n, t = e % n;
+    L.Hn[i * ldn + t] = g.H[i * ld + t];
+  }
   const double hmn = g.H[n * ld + n - 1];
-  for (int i = 0; i < n; ++i) g.w[i] = 0.0;
-  g.w[n - 1] = 1.0;
-  sd::solve_transposed(g.Hn, ldn, n, g.w, g.work, g.perm);
-  for (int i = 0; i < n; ++i) g.Hn[i * ldn + n - 1] += hmn * hmn * g.w[i];
+  for (int i = r0; i < n; i += ns) L.w[i] = (i == n - 1) ? 1.0 : 0.0;
+  tm.sync();
+  sd::solve_transposed(tm, L.Hn, ldn, n, L.w, L.work, L.perm);
+  for (int i = r0; i < n; i += ns) L.Hn[i * ldn + n - 1] += hmn * hmn * L.w[i];
+  tm.sync();
   // (2) real Schur form, selection of the k smallest harmonic Ritz values
-  sd::hessenberg(g.Hn, ldn, n, g.Z, ldn, g.work);
-  const bool conv = sd::francis_qr(g.Hn, ldn, n, g.Z, ldn);
-  sd::schur_eigs(g.Hn, ldn, n, g.wr, g.wi);
-  sd::select_smallest(g.wr, g.wi, n, k, zero_thresh, g.perm, g.sel);
+  sd::hessenberg(tm, L.Hn, ldn, n, L.Z, ldn, L.work);
+  const bool conv = sd::francis_qr(tm, L.Hn, ldn, n, L.Z, ldn);
+  if (r0 == 0) {
+    sd::schur_eigs(L.Hn, ldn, n, L.wr, L.wi);
+    sd::select_smallest(L.wr, L.wi, n, k, zero_thresh, L.perm, L.sel);
+  }
+  tm.sync();
   // (3) orthonormal basis P_k of the selected invariant subspace
   const int ldp = g.m + 1;
-  const int keff = sd::invariant_basis(g.Hn, ldn, n, g.Z, ldn, g.wr, g.wi, g.sel, g.P, ldp, g.work);
+  const int keff = sd::invariant_basis(tm, L.Hn, ldn, n, L.Z, ldn, L.wr, L.wi, L.sel, L.P, ldp, L.work);
   k = keff;
   if (!conv || k < 1 || k + 1 > max_keep) {
-    h->done = DONE_BREAKDOWN;  // the Qn update below is skipped (keff = -1)
-    h->keff = -1;
+    if (r0 == 0) {
+      h->done = DONE_BREAKDOWN;  // the Qn update below is skipped (keff = -1)
+      h->keff = -1;
+    }
     return;
   }
   // (4) P_{k+1}: [P_k; 0] and res_vec orthogonalised (classical GS as in :211-232)
-  for (int t = 0; t < k; ++t) g.P[n * ldp + t] = 0.0;
-  for (int i = 0; i < m1; ++i) g.P[i * ldp + k] = g.resv[i];
+  for (int t = r0; t < k; t += ns) L.P[n * ldp + t] = 0.0;
+  for (int i = r0; i < m1; i += ns) L.P[i * ldp + k] = L.resv[i];
+  tm.sync();
   for (int c = 0; c < k; ++c) {
     double d = 0.0;
-    for (int i = 0; i < m1; ++i) d += g.P[i * ldp + c] * g.P[i * ldp + k];
-    for (int i = 0; i < m1; ++i) g.P[i * ldp + k] -= d * g.P[i * ldp + c];
+    for (int i = r0; i < m1; i += ns) d += L.P[i * ldp + c] * L.P[i * ldp + k];
+    d = tm.sum(d);
+    for (int i = r0; i < m1; i += ns) L.P[i * ldp + k] -= d * L.P[i * ldp + c];
+    tm.sync();
   }
   {
     double nrm = 0.0;
-    for (int i = 0; i < m1; ++i) nrm += g.P[i * ldp + k] * g.P[i * ldp + k];
-    nrm = sqrt(nrm);
-    for (int i = 0; i < m1; ++i) g.P[i * ldp + k] /= nrm;
+    for (int i = r0; i < m1; i += ns) nrm += L.P[i * ldp + k] * L.P[i * ldp + k];
+    nrm = sqrt(tm.sum(nrm));
+    for (int i = r0; i < m1; i += ns) L.P[i * ldp + k] /= nrm;
+    tm.sync();
   }
   // (5) c_r = P_{k+1}^T res_vec
-  for (int c = 0; c <= k; ++c) {
+  for (int c = r0; c <= k; c += ns) {
     double s = 0.0;
-    for (int i = 0; i < m1; ++i) s += g.P[i * ldp + c] * g.resv[i];
+    for (int i = 0; i < m1; ++i) s += L.P[i * ldp + c] * L.resv[i];
     g.rhs[c] = s;
   }
-  for (int i = k + 1; i <= g.m; ++i) g.rhs[i] = 0.0;
-  // (6) H_new = P_{k+1}^T H P_k  ((k+1) x k)
-  for (int i = 0; i < m1; ++i)  // W = H P_k -> Hnew as scratch ((n+1) x k, ld = m)
-    for (int c = 0; c < k; ++c) {
-      double s = 0.0;
-      for (int t = 0; t < n; ++t) s += g.H[i * ld + t] * g.P[t * ldp + c];
-      g.Hnew[i * ld + c] = s;
+  for (int i = k + 1 + r0; i <= g.m; i += ns) g.rhs[i] = 0.0;
+  // (6) H_new = P_{k+1}^T H P_k  ((k+1) x k); W = H P_k in g.Hnew ((n+1) x k, ld = m)
+  for (int e = r0; e < m1 * k; e += ns) {
+    const int i = e / k, c = e % k;
+    double s = 0.0;
+    for (int t = 0; t < n; ++t) s += g.H[i * ld + t] * L.P[t * ldp + c];
+    g.Hnew[i * ld + c] = s;
+  }
+  tm.sync();
+  for (int e = r0; e < (k + 1) * k; e += ns) {
+    const int r = e / k, c = e % k;
+    double s = 0.0;
+    for (int i = 0; i < m1; ++i) s += L.P[i * ldp + r] * g.Hnew[i * ld + c];
+    L.work[r * ld + c] = s;
+  }
+  tm.sync();
+  for (int e = r0; e < (g.m + 1) * g.m; e += ns) {
+    const int r = e / g.m, c = e % g.m;
+    g.H[e] = (r <= k && c < k) ? L.work[r * ld + c] : 0.0;
+  }
+  // P_{k+1} to the global scratch for the Qn update
+  if (use_smem)
+    for (int e = r0; e < m1 * (k + 1); e += ns) {
+      const int i = e / (k + 1), c = e % (k + 1);
+      g.P[i * ldp + c] = L.P[i * ldp + c];
     }
-  for (int r = 0; r <= k; ++r)
-    for (int c = 0; c < k; ++c) {
-      double s = 0.0;
-      for (int i = 0; i < m1; ++i) s += g.P[i * ldp + r] * g.Hnew[i * ld + c];
-      g.work[r * ld + c] = s;
-    }
-  for (int i = 0; i <= g.m; ++i)
-    for (int c = 0; c < g.m; ++c) g.H[i * ld + c] = 0.0;
-  for (int r = 0; r <= k; ++r)
-    for (int c = 0; c < k; ++c) g.H[r * ld + c] = g.work[r * ld + c];
+  tm.sync();
   // (8) restart the least-squares state from H_new and c_r
-  int nrot = 0;
-  for (int i = 0; i <= g.m; ++i) g.g[i] = g.rhs[i];
-  double res = 0.0;
-  for (int c = 0; c < k; ++c) res = sd::ls_add_column(g.H, ld, c, k, g.R, g.rots, nrot, g.g);
-  *g.nrot = nrot;
-  (void)res;
-  h->keff = k;
-  h->j = k;
-  h->restarted = 1;
+  if (r0 == 0) {
+    int nrot = 0;
+    for (int i = 0; i <= g.m; ++i) g.g[i] = g.rhs[i];
+    for (int c = 0; c < k; ++c) sd::ls_add_column(g.H, ld, c, k, g.R, g.rots, nrot, g.g);
+    *g.nrot = nrot;
+    h->keff = k;
+    h->j = k;
+    h->restarted = 1;
+  }
 }
 
 // Qout[0..k] <- Qn[0..m1-1] P_{k+1} (deflated_restart.hpp:250-258), written to
@@ -666,6 +716,11 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
   gp.sel = dint.get() + 1 + m;
   KHead* hd = dhead.get();
   const int g = grid_for(h, len, 256);
+  size_t defl_smem = 0;
+  if (restart > 0 && deflate_smem_bytes(m) <= kDeflateSmemMax) {
+    defl_smem = deflate_smem_bytes(m);
+    BSP_CUDA_TRY(cudaFuncSetAttribute(k_gm_deflate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)defl_smem));
+  }
 
   EventTimer tm(h->stream);
   BSP_TRY(ensure_basis(restart > 0 ? m + 1 : 2));
@@ -713,7 +768,7 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
         bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vr0.get(), &hd->res0, hd, qptr[0]);
         bsp::count_launch(), k_gm_pure_restart<<<1, 1, 0, h->stream>>>(gp);
       } else {
-        bsp::count_launch(), k_gm_deflate<<<1, 1, 0, h->stream>>>(gp, k_req, n_spare);
+        bsp::count_launch(), k_gm_deflate<<<1, 32, defl_smem, h->stream>>>(gp, k_req, n_spare, defl_smem > 0);
         bsp::count_launch(), k_gm_qn_update<<<g, 256, 0, h->stream>>>(len, dq.get(), dspare.get(), gp.P, m + 1, hd, st.j + 1);
       }
       BSP_CUDA_TRY(cudaPeekAtLastError());

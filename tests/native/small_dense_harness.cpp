@@ -10,8 +10,8 @@ extern "C" {
 int sd_schur(const double* A, int n, double* T, double* Z, double* wr, double* wi) {
   std::vector<double> v(n + 1);
   for (int i = 0; i < n * n; ++i) T[i] = A[i];
-  hessenberg(T, n, n, Z, n, v.data());
-  const bool ok = francis_qr(T, n, n, Z, n);
+  hessenberg(SoloTeam{}, T, n, n, Z, n, v.data());
+  const bool ok = francis_qr(SoloTeam{}, T, n, n, Z, n);
   schur_eigs(T, n, n, wr, wi);
   return ok ? 1 : 0;
 }
@@ -21,11 +21,11 @@ int sd_invariant(const double* A, int n, int k, double zero_thresh, double* P, i
   std::vector<double> T(n * n), Z(n * n), wr(n), wi(n), work(n * n + 8 * n + 32), v(n + 1);
   std::vector<int> perm(n), sel(n);
   for (int i = 0; i < n * n; ++i) T[i] = A[i];
-  hessenberg(T.data(), n, n, Z.data(), n, v.data());
-  const bool ok = francis_qr(T.data(), n, n, Z.data(), n);
+  hessenberg(SoloTeam{}, T.data(), n, n, Z.data(), n, v.data());
+  const bool ok = francis_qr(SoloTeam{}, T.data(), n, n, Z.data(), n);
   schur_eigs(T.data(), n, n, wr.data(), wi.data());
   select_smallest(wr.data(), wi.data(), n, k, zero_thresh, perm.data(), sel.data());
-  *keff = invariant_basis(T.data(), n, n, Z.data(), n, wr.data(), wi.data(), sel.data(), P, n,
+  *keff = invariant_basis(SoloTeam{}, T.data(), n, n, Z.data(), n, wr.data(), wi.data(), sel.data(), P, n,
                           work.data());
   return ok ? 1 : 0;
 }
@@ -48,6 +48,6 @@ double sd_lstsq(const double* H, int m, int ncols, int last_row_dense, const dou
 int sd_solve_transposed(const double* A, int n, double* w) {
   std::vector<double> work(n * n);
   std::vector<int> piv(n);
-  return solve_transposed(A, n, n, w, work.data(), piv.data()) ? 1 : 0;
+  return solve_transposed(SoloTeam{}, A, n, n, w, work.data(), piv.data()) ? 1 : 0;
 }
 }
