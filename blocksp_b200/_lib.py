@@ -48,6 +48,17 @@ class SolveInfo(C.Structure):
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iters", C.c_int), ("mode", C.c_int),
+                ("check_every", C.c_int), ("hist_cap", C.c_int), ("retune", C.c_int)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("n_pairs", C.c_int), ("n_converged", C.c_int),
+                ("iters_max", C.c_int), ("iters_total", C.c_longlong), ("graph_iters", C.c_int),
+                ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
+
+
 _P = C.c_void_p
 _I = C.c_int
 _I64 = C.c_int64
@@ -88,6 +99,12 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_pcg": (_I, [_P, _P, _P, _P, _P, C.POINTER(SolveOpts), _P, _I, C.POINTER(SolveInfo)]),
     "bsp_pgmres": (_I, [_P, _P, _P, _P, _P, C.POINTER(SolveOpts), _P, _I, C.POINTER(SolveInfo)]),
     "bsp_true_residual_dev": (_I, [_P, _P, _P, _P, _PD]),
+    "bsp_batch_create": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    "bsp_batch_destroy": (_I, [_P]),
+    "bsp_batch_tuning": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "bsp_batch_pcg_dev": (_I, [_P, _P, _I, _P, _P, C.POINTER(BatchOpts), C.POINTER(BatchInfo)]),
+    "bsp_batch_pcg": (_I, [_P, _P, _I, _P, _P, C.POINTER(BatchOpts), C.POINTER(BatchInfo)]),
+    "bsp_batch_results": (_I, [_P, _I, _P, _P, _P, _P, _I]),
 }
 
 _lib = None

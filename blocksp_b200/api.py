@@ -377,3 +377,110 @@ class ez:
     @staticmethod
     def ichol0_pCG(A, b, printIters=False):
         return IChol0_pCG(A, 1e-8, 5000, printIters).solve(A, b)
+
+
+# ---------------------------------------------------------------- batched solver
+
+class Batch:
+    """Many independent SPD block systems solved together by block-IChol0 pCG.
+
+    Equivalent to running ``IChol0_pCG<T,bs,1>(A_s, tol, maxIters).solve(A_s, b)``
+    (blocksp_solvers.hpp:481-492) for every system s and every right-hand side,
+    each (system, RHS) pair with its own alpha, beta and stopping test; the whole
+    batch runs as one CUDA-graph launch.  ``systems`` are objects with
+    ``row_ptr``, ``col_idx``, ``vals`` (n_blocks x bs x bs) and ``bs``.
+    Vectors are the systems' solArray<T,bs,nrhs> blocks concatenated in order.
+    """
+
+    def __init__(self, systems, handle: Handle | None = None):
+        self.handle = handle or default_handle()
+        lib = self.handle.lib
+        self.n_rows = np.array([len(s.row_ptr) - 1 for s in systems], dtype=np.int32)
+        self.bs = np.array([s.bs for s in systems], dtype=np.int32)
+        self.nnzb = np.array([len(s.col_idx) for s in systems], dtype=np.int64)
+        rp = np.ascontiguousarray(np.concatenate([np.asarray(s.row_ptr, dtype=np.int32) for s in systems]))
+        ci = np.ascontiguousarray(np.concatenate([np.asarray(s.col_idx, dtype=np.int32) for s in systems]))
+        vals = np.ascontiguousarray(np.concatenate([np.asarray(s.vals, dtype=np.float64).ravel()
+                                                    for s in systems]))
+        b = C.c_void_p()
+        check(lib.bsp_batch_create(self.handle.h, len(systems), _ptr(self.n_rows), _ptr(self.bs),
+                                   _ptr(self.nnzb), _ptr(rp), _ptr(ci), _ptr(vals), C.byref(b)),
+              "bsp_batch_create", self.handle.h)
+        self.b = b
+        self._last = (1, 0)
+        self.handle.adopt(self)
+
+    @property
+    def n_sys(self) -> int:
+        return int(self.n_rows.shape[0])
+
+    def vector_size(self, nrhs: int) -> int:
+        return int(np.sum(self.n_rows.astype(np.int64) * self.bs) * nrhs)
+
+    def offsets(self, nrhs: int) -> np.ndarray:
+        """Start of each system's block in a batch vector with nrhs right-hand sides."""
+        sizes = self.n_rows.astype(np.int64) * self.bs * nrhs
+        return np.concatenate([[0], np.cumsum(sizes)])
+
+    def pcg(self, b, nrhs: int, tol: float = 1e-10, max_iters: int = 2000, mode: int = 0,
+            check_every: int = 8, hist_cap: int = 0, retune: bool = False):
+        """Solve; returns (x, info dict).  b is a device tensor or a host array."""
+        lib = self.handle.lib
+        opts = _lib.BatchOpts(float(tol), int(max_iters), int(mode), int(check_every), int(hist_cap),
+                              int(bool(retune)))
+        info = _lib.BatchInfo()
+        if hasattr(b, "data_ptr"):
+            import torch
+            x = torch.empty_like(b)
+            st = lib.bsp_batch_pcg_dev(self.handle.h, self.b, int(nrhs), _ptr(b), _ptr(x), C.byref(opts),
+                                       C.byref(info))
+        else:
+            bb = np.ascontiguousarray(b, dtype=np.float64)
+            x = np.zeros_like(bb)
+            st = lib.bsp_batch_pcg(self.handle.h, self.b, int(nrhs), _ptr(bb), _ptr(x), C.byref(opts),
+                                   C.byref(info))
+        if st not in (_lib.BSP_OK, 4, 5):  # MAXIT / NAN still return x
+            check(st, "bsp_batch_pcg", self.handle.h)
+        self._last = (int(nrhs), int(hist_cap))
+        return x, {f: getattr(info, f) for f, _ in _lib.BatchInfo._fields_}
+
+    def results(self) -> dict:
+        """Per-pair results of the last solve, arrays indexed [system, rhs]."""
+        nrhs, hcap = self._last
+        n = self.n_sys * nrhs
+        iters = np.zeros(n, dtype=np.int32)
+        state = np.zeros(n, dtype=np.int32)
+        res = np.zeros(n)
+        hist = np.zeros((n, hcap)) if hcap > 0 else None
+        check(self.handle.lib.bsp_batch_results(self.b, nrhs, _ptr(iters), _ptr(state), _ptr(res),
+                                                _ptr(hist) if hist is not None else None, hcap),
+              "bsp_batch_results")
+        out = {"iters": iters.reshape(self.n_sys, nrhs), "state": state.reshape(self.n_sys, nrhs),
+               "final_res": res.reshape(self.n_sys, nrhs)}
+        if hist is not None:
+            out["hist"] = hist.reshape(self.n_sys, nrhs, hcap)
+        return out
+
+    def tuning(self) -> list[dict]:
+        """Groups (one per block size) with the launch shapes the autotuner chose."""
+        k = 4
+        ng = C.c_int()
+        arr = {n: np.zeros(k, dtype=np.int32) for n in ("bs", "systems", "tile_threads", "tile_ctas_per_sm",
+                                                        "sweep_ctas_per_sm")}
+        rows = np.zeros(k, dtype=np.int64)
+        check(self.handle.lib.bsp_batch_tuning(self.b, C.byref(ng), _ptr(arr["bs"]), _ptr(arr["systems"]),
+                                               _ptr(rows), _ptr(arr["tile_threads"]),
+                                               _ptr(arr["tile_ctas_per_sm"]), _ptr(arr["sweep_ctas_per_sm"])),
+              "bsp_batch_tuning")
+        return [{**{n: int(v[i]) for n, v in arr.items()}, "rows": int(rows[i])} for i in range(ng.value)]
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            self.handle.lib.bsp_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

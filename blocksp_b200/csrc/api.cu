@@ -11,6 +11,7 @@ void record_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launch_add(int64_t n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha,
                 const void* x, double beta, const void* z, void* y, cudaStream_t s);
@@ -263,6 +264,14 @@ int bsp_matrix_device_ptrs(bsp_matrix_t A, const int** row_ptr, const int** col_
 }
 
 }  // extern "C"
+
+int matrix_create_struct(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb, const int* row_ptr,
+                         const int* col_idx, bsp_matrix_t* out) {
+  std::unique_ptr<bsp_matrix_s> A;
+  BSP_TRY(matrix_create_common(h, n_rows, n_cols, bs, nnzb, row_ptr, col_idx, out, A));
+  *out = A.release();
+  return BSP_OK;
+}
 
 namespace bsp {
 __global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {

@@ -145,6 +145,8 @@ __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + 
 
 // Process-wide count of kernel launches made by this library (bsp_launch_count).
 void count_launch();
+// Adds n (possibly negative) to the count: kernels replayed inside a CUDA graph.
+void count_launch_add(int64_t n);
 
 }  // namespace bsp
 

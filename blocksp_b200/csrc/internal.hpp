@@ -69,6 +69,28 @@ struct SymbolicCache {
   DevBuf<int64_t> d_perm, t_blk;
 };
 
+// Device time between construction and stop_ms() on one stream.
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+  }
+  double stop_ms() {
+    float ms = 0;
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EventTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 }  // namespace bsp
 
 struct bsp_handle_s {
@@ -108,3 +130,7 @@ struct bsp_matrix_s {
   // symbolic analyses for ILU0 (full pattern), IChol0 (lower pattern), SOR/Diag
   bsp::SymbolicCache sym_ilu, sym_ichol, sym_sor;
 };
+
+// Uploads a validated structure and allocates (uninitialised) FP64 values.
+int matrix_create_struct(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb, const int* row_ptr,
+                         const int* col_idx, bsp_matrix_t* out);

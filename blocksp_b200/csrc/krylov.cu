@@ -533,26 +533,6 @@ int true_residual(bsp_handle_s* h, bsp_matrix_s* A, const double* b, const doubl
   return BSP_OK;
 }
 
-struct EventTimer {
-  cudaEvent_t a = nullptr, b = nullptr;
-  cudaStream_t s;
-  explicit EventTimer(cudaStream_t st) : s(st) {
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    cudaEventRecord(a, s);
-  }
-  double stop_ms() {
-    float ms = 0;
-    cudaEventRecord(b, s);
-    cudaEventSynchronize(b);
-    cudaEventElapsedTime(&ms, a, b);
-    return ms;
-  }
-  ~EventTimer() {
-    if (a) cudaEventDestroy(a);
-    if (b) cudaEventDestroy(b);
-  }
-};
 
 // ------------------------------------------------------------------ pCG
 // Stored copy the inner operator reads: FP64 for the reference method, FP32

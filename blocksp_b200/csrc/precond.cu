@@ -15,13 +15,16 @@
 // computed but not what it computes, so the preconditioner is the same
 // operator as the reference's (no recolouring, no reordering).
 //
-// Sync-free execution: a launch is persistent; each group of lanes claims the
-// next row of the level order with an atomic ticket, waits (bounded spin) on
-// the ready flags of the rows it depends on, computes, publishes its row and
-// raises its own flag.  A row only waits on rows with smaller tickets, which
-// were claimed by groups that are already running, so the launch always
-// progresses without any co-residency requirement.  Flags hold the epoch of
-// the sweep that last wrote them, so they never need clearing.
+// Sync-free execution: a sweep launch is persistent; each group of lanes
+// claims the next task (a chain of consecutive dependent rows, in chain-level
+// order) with an atomic ticket.  The output vector is pre-filled with a
+// signalling-NaN sentinel and a row is published by its values: a consumer
+// polls the words it needs (bounded spin) until they differ from the
+// sentinel, so no flag or fence is involved.  A task only waits on rows of
+// tasks with smaller tickets, which were claimed by groups that are already
+// running, so the launch always progresses without any co-residency
+// requirement.  The factorisation uses per-row ready flags that hold the
+// epoch of the launch that last wrote them, so they never need clearing.
 //
 // The factorisation is row-oriented (IKJ): row k applies the eliminations of
 // rows i < k in increasing i, exactly the sequence of updates the reference's
@@ -29,7 +32,9 @@
 #include <algorithm>
 #include <numeric>
 #include "blockops.cuh"
+#include "precond.hpp"
 #include "reduce.cuh"
+#include "sentinel.cuh"
 
 namespace bsp {
 
@@ -49,28 +54,6 @@ __device__ __forceinline__ void wait_flag(const int* f, int epoch, DevStatus* st
   }
 }
 
-// ----------------------------------------------------------------- sentinel
-// A sweep's output vector is filled with a signalling-NaN bit pattern before
-// the launch.  Arithmetic never produces it (NaN results are quiet), so a row
-// is final exactly when its words differ from the pattern.  Aligned 8- and
-// 4-byte accesses are single-copy atomic, so a reader never sees half a value.
-constexpr unsigned long long kSentinel64 = 0x7FF4B5B5B5B5B5B5ull;
-constexpr unsigned kSentinel32 = 0x7FA5B5B5u;
-__device__ __forceinline__ bool is_sentinel(double v) {
-  return (unsigned long long)__double_as_longlong(v) == kSentinel64;
-}
-__device__ __forceinline__ bool is_sentinel(float v) { return __float_as_uint(v) == kSentinel32; }
-// Re-reads inside a polling loop: relaxed loads at GPU scope, never merged.
-__device__ __forceinline__ double ld_poll(const double* p) {
-  double v;
-  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ float ld_poll(const float* p) {
-  float v;
-  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
-  return v;
-}
 __global__ void k_fill_sentinel64(int64_t n, unsigned long long* __restrict__ x) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] = kSentinel64;
@@ -595,44 +578,7 @@ int grid_for(const bsp_handle_s* h, int64_t n, int threads);
 // ================================================================= host side
 using namespace bsp;
 
-struct bsp_precond_s {
-  bsp_handle_t h = nullptr;
-  int device = 0;
-  bsp_matrix_t A = nullptr;
-  int kind = 0, n = 0, bs = 0, precision = 0;
-  double w = 1.6;
-  int nu = 3, type = 0;
-  // factor storage (ILU0: every block of A; IChol0: A.lowTri()), columns sorted
-  DevBuf<int> f_ptr, f_col, f_diag;
-  DevBuf<double> f_vals;
-  DevBuf<float> f_vals32;
-  DevBuf<__nv_bfloat16> f_vals16;
-  std::vector<int64_t> h_perm;  // factor entry -> block index in A
-  DevBuf<int64_t> d_perm;
-  int64_t f_nnzb = 0;
-  // IChol0 backward sweep: transposed strictly-lower structure of L
-  DevBuf<int> t_ptr, t_row;
-  DevBuf<int64_t> t_blk;
-  // SOR / Diag on A's own structure
-  DevBuf<int> a_diag;
-  // inverted diagonal blocks (U_ii^-1, L_ii^-1 or A_ii^-1)
-  DevBuf<double> dinv;
-  DevBuf<float> dinv32;
-  DevBuf<__nv_bfloat16> dinv16;
-  // level orders
-  DevBuf<int> order_lo, order_up;
-  int n_lev_lo = 0, n_lev_up = 0;
-  // chains of consecutive dependent rows, in chain-level order (sweep tasks)
-  DevBuf<int> task_lo_row, task_lo_len, task_up_row, task_up_len;
-  int n_task_lo = 0, n_task_up = 0;
-  // sync-free state
-  DevBuf<int> flags;
-  DevBuf<unsigned> ticket;
-  // apply scratch: sweep outputs (pre-filled with the sentinel), SOR ping-pong
-  // iterates and the copy of an in-place right-hand side
-  DevBuf<double> s64[3];
-  DevBuf<float> s32[3];
-};
+
 
 namespace bsp {
 

@@ -1,0 +1,50 @@
+// precond.hpp — host-side state of a block preconditioner (shared by the
+// single-system, batched and learned solvers).
+#pragma once
+#include "internal.hpp"
+
+struct bsp_precond_s {
+  bsp_handle_t h = nullptr;
+  int device = 0;
+  bsp_matrix_t A = nullptr;
+  int kind = 0, n = 0, bs = 0, precision = 0;
+  double w = 1.6;
+  int nu = 3, type = 0;
+  // factor storage (ILU0: every block of A; IChol0: A.lowTri()), columns sorted
+  bsp::DevBuf<int> f_ptr, f_col, f_diag;
+  bsp::DevBuf<double> f_vals;
+  bsp::DevBuf<float> f_vals32;
+  bsp::DevBuf<__nv_bfloat16> f_vals16;
+  std::vector<int64_t> h_perm;  // factor entry -> block index in A
+  bsp::DevBuf<int64_t> d_perm;
+  int64_t f_nnzb = 0;
+  // IChol0 backward sweep: transposed strictly-lower structure of L
+  bsp::DevBuf<int> t_ptr, t_row;
+  bsp::DevBuf<int64_t> t_blk;
+  // SOR / Diag on A's own structure
+  bsp::DevBuf<int> a_diag;
+  // inverted diagonal blocks (U_ii^-1, L_ii^-1 or A_ii^-1)
+  bsp::DevBuf<double> dinv;
+  bsp::DevBuf<float> dinv32;
+  bsp::DevBuf<__nv_bfloat16> dinv16;
+  // level orders
+  bsp::DevBuf<int> order_lo, order_up;
+  int n_lev_lo = 0, n_lev_up = 0;
+  // chains of consecutive dependent rows, in chain-level order (sweep tasks)
+  bsp::DevBuf<int> task_lo_row, task_lo_len, task_up_row, task_up_len;
+  int n_task_lo = 0, n_task_up = 0;
+  // sync-free state
+  bsp::DevBuf<int> flags;
+  bsp::DevBuf<unsigned> ticket;
+  // apply scratch: sweep outputs (pre-filled with the sentinel), SOR ping-pong
+  // iterates and the copy of an in-place right-hand side
+  bsp::DevBuf<double> s64[3];
+  bsp::DevBuf<float> s32[3];
+};
+
+namespace bsp {
+int grid_for(const bsp_handle_s* h, int64_t n, int threads);
+int precond_build(bsp_precond_s* pc);
+int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z);
+int precond_check_status(bsp_precond_s* pc);
+}  // namespace bsp

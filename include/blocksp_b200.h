@@ -235,6 +235,62 @@ int bsp_pgmres(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b
 int bsp_true_residual_dev(bsp_handle_t h, bsp_matrix_t A, const double* b, const double* x,
                           double* rel_res_host);
 
+/* ---- batched solver -------------------------------------------------------
+ * Many independent SPD systems (block sizes 4, 8 or 16, uneven sizes), each
+ * with nrhs right-hand sides, solved by block-IChol0 pCG.  Replaces the loop
+ *     for each system s, for each RHS d:
+ *         x[s][d] = IChol0_pCG<T,bs,1>(A_s, tol, maxIters).solve(A_s, b[s][d])
+ * (blocksp_solvers.hpp:481-492 with pCG :51-105 and IChol0
+ * blocksp_preconditioners.hpp:364-536); no single reference call computes it,
+ * because the reference pCG couples the D dims of a solArray<T,B,D> through
+ * one alpha/beta.  Every (system, RHS) pair keeps its own alpha, beta,
+ * stopping test and iteration count.
+ *
+ * Packed inputs: systems in order; row_ptr holds each system's n_rows[s]+1
+ * entries (starting at 0), col_idx and vals each system's nnzb[s] blocks
+ * (local column indices; bs[s] x bs[s] row-major FP64 blocks).
+ * Vectors (b, x): systems in order, each n_rows[s] x nrhs x bs[s] doubles in
+ * the solArray<T,bs,nrhs> (element, RHS, component) order. */
+typedef struct bsp_batch_s* bsp_batch_t;
+
+typedef struct {
+  double tol;       /* relative tolerance of every pair (reference pCG rule) */
+  int max_iters;    /* per pair, as pCG's maxIters */
+  int mode;         /* 0: one graph launch with a device-side loop; 1: the
+                       iteration graph replayed by the host */
+  int check_every;  /* mode 1: iterations between status reads */
+  int hist_cap;     /* residual-history entries kept per pair (0: none) */
+  int retune;       /* 1: re-run the launch-shape autotuner */
+} bsp_batch_opts;
+
+typedef struct {
+  int status;           /* BSP_OK when every pair converged */
+  int n_pairs;          /* systems x nrhs */
+  int n_converged;
+  int iters_max;        /* most pCG iterations of any pair */
+  long long iters_total;
+  int graph_iters;      /* iterations the batched loop executed */
+  double setup_ms;      /* autotune + graph capture (0 when reused) */
+  double solve_ms;      /* device time of the solve */
+} bsp_batch_info;
+
+int bsp_batch_create(bsp_handle_t h, int n_sys, const int* n_rows, const int* bs, const int64_t* nnzb,
+                     const int* row_ptr, const int* col_idx, const double* vals, bsp_batch_t* out);
+int bsp_batch_destroy(bsp_batch_t B);
+/* Per group of equal block size: its block size, systems, rows and the launch
+ * shapes the autotuner chose (0 before the first solve).  Arrays hold up to 4. */
+int bsp_batch_tuning(bsp_batch_t B, int* n_groups, int* group_bs, int* group_systems, int64_t* group_rows,
+                     int* tile_threads, int* tile_ctas_per_sm, int* sweep_ctas_per_sm);
+int bsp_batch_pcg_dev(bsp_handle_t h, bsp_batch_t B, int nrhs, const double* b, double* x,
+                      const bsp_batch_opts* opts, bsp_batch_info* info);
+int bsp_batch_pcg(bsp_handle_t h, bsp_batch_t B, int nrhs, const double* b_host, double* x_host,
+                  const bsp_batch_opts* opts, bsp_batch_info* info);
+/* Per-pair results of the last solve, indexed [system * nrhs + rhs]: pCG
+ * iterations, state (1 converged, 2 max iterations, 4 NaN), last residual and
+ * (hist_cap > 0) the residual history, hist_cap entries per pair. */
+int bsp_batch_results(bsp_batch_t B, int nrhs, int* iters, int* state, double* final_res, double* hist,
+                      int hist_cap);
+
 #ifdef __cplusplus
 }
 #endif

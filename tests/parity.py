@@ -37,11 +37,14 @@ def arg(meta, key, default):
     return type(default)(a[a.index(key) + 1]) if key in a else default
 
 
-def cg_envelope(Ao, b, tol, pre, max_iters, ref_hist, trials=3, eps=1e-15):
-    """Per-step spread of the oracle's normalised pCG history when its matrix
-    product and preconditioner output are perturbed at rounding level."""
-    r = np.asarray(ref_hist) / ref_hist[0]
+def cg_spread(Ao, b, tol, pre, max_iters, ref, trials=3, eps=1e-15):
+    """The oracle's pCG rerun with its matrix product and preconditioner output
+    perturbed at rounding level (relative 1e-15): per-step spread of the
+    normalised history, the iteration counts and the solutions' relative
+    distance from the unperturbed run ``ref``."""
+    r = np.asarray(ref.hist) / ref.hist[0]
     env = np.zeros(len(r))
+    iters, xdev = [], []
     for t in range(trials):
         rng = np.random.default_rng(100 + t)
 
@@ -53,7 +56,18 @@ def cg_envelope(Ao, b, tol, pre, max_iters, ref_hist, trials=3, eps=1e-15):
         env[:n] = np.maximum(env[:n], np.abs(h[:n] - r[:n]))
         if n < len(r):
             env[n:] = np.maximum(env[n:], r[n:])
-    return env
+        iters.append(o.iters)
+        xdev.append(rel(o.x, ref.x))
+    return env, iters, xdev
+
+
+def cg_envelope(Ao, b, tol, pre, max_iters, ref_hist, trials=3, eps=1e-15):
+    """Per-step spread of the oracle's normalised pCG history when its matrix
+    product and preconditioner output are perturbed at rounding level."""
+    class _Ref:
+        hist = list(ref_hist)
+        x = np.zeros_like(b)
+    return cg_spread(Ao, b, tol, pre, max_iters, _Ref, trials, eps)[0]
 
 
 def check_history(hist, ref_hist, h_tol=1e-10, envelope=None):
