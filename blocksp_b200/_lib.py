@@ -105,6 +105,18 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_batch_pcg_dev": (_I, [_P, _P, _I, _P, _P, C.POINTER(BatchOpts), C.POINTER(BatchInfo)]),
     "bsp_batch_pcg": (_I, [_P, _P, _I, _P, _P, C.POINTER(BatchOpts), C.POINTER(BatchInfo)]),
     "bsp_batch_results": (_I, [_P, _I, _P, _P, _P, _P, _I]),
+    "bsp_learned_create": (_I, [_P, _I, _I, C.POINTER(_P)]),
+    "bsp_learned_destroy": (_I, [_P]),
+    "bsp_learned_param_count": (_I, [_P, C.POINTER(_I64)]),
+    "bsp_learned_set_params": (_I, [_P, _P, _I64]),
+    "bsp_learned_get_params": (_I, [_P, _P, _I64]),
+    "bsp_learned_get_grads": (_I, [_P, _P, _I64]),
+    "bsp_learned_forward": (_I, [_P, _P, _P, _P]),
+    "bsp_learned_ilu_factors": (_I, [_P, _P, _P]),
+    "bsp_learned_loss_grad": (_I, [_P, _P, _P, _P, _I, _P, _PD]),
+    "bsp_learned_adam_step": (_I, [_P, _P, _D, _D, _D, _D]),
+    "bsp_learned_probes": (_I, [_P, _P, _P, _P, _I, _P]),
+    "bsp_learned_precond": (_I, [_P, _P, _P, _I, C.POINTER(_P)]),
 }
 
 _lib = None

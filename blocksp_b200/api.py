@@ -173,6 +173,17 @@ class Precond:
         self.p = p
         self.handle.adopt(self)
 
+    @classmethod
+    def wrap(cls, A: Matrix, ptr, kind: int) -> "Precond":
+        """Adopts a preconditioner handle built by another entry point."""
+        obj = cls.__new__(cls)
+        obj.A = A
+        obj.handle = A.handle
+        obj.kind = kind
+        obj.p = ptr
+        obj.handle.adopt(obj)
+        return obj
+
     def __call__(self, r) -> None:
         check(self.handle.lib.bsp_precond_apply_dev(self.handle.h, self.p, _ptr(r)),
               "bsp_precond_apply_dev", self.handle.h)
@@ -193,7 +204,7 @@ class Precond:
     def export(self) -> np.ndarray:
         inf = self.info()
         bs = self.A.bs
-        nblk = inf["factor_nnzb"] if self.kind in (_lib.PC_ILU0, _lib.PC_ICHOL0) else self.A.n_rows
+        nblk = inf["factor_nnzb"] if self.kind in (_lib.PC_ILU0, _lib.PC_ICHOL0, _lib.PC_LEARNED_LU) else self.A.n_rows
         out = np.zeros((nblk, bs, bs))
         check(self.handle.lib.bsp_precond_export(self.p, _ptr(out), out.size), "bsp_precond_export")
         return out

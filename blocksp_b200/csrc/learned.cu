@@ -1,0 +1,1093 @@
+// learned.cu — learned block-LU preconditioner: a message-passing network over
+// the block graph of A, with hand-written forward and backward kernels, trained
+// on the GPU, whose output corrects the block-ILU0 factors.
+//
+// No reference counterpart: the reference's preconditioners end at IChol0
+// (blocksp_preconditioners.hpp:364-538).  The factors keep A's sparsity and
+// are stored in the ILU0 structures (PC_LEARNED_LU), so the same sync-free
+// triangular sweeps apply them (ILU0::invmul order, :294-349).
+//
+// Network (8x8 blocks, hidden H = 32, 3 layers; nodes = block rows, one
+// directed edge per off-diagonal block A_ij in CSR order):
+//   s_i = rms(A_ii); x_i = [A_ii / s_i, log s_i]; a_k = A_ij / sqrt(s_i s_j)
+//   h = relu(Wn x + bn); e = relu(We a + be)
+//   per layer: msg_k = relu(Wm [h_j; e_k] + bm); m_i = sum_{k in row i} msg_k;
+//              h_i += relu(Wu [h_i; m_i] + bu)
+//   dF_ij = 0.01 sqrt(s_i s_j) (Wo [h_i; h_j; e_k] + bo);  dF_ii = 0.01 s_i (Wd h_i + bd)
+// M = L U with (L, U) the ILU0 factors plus dF.  Training minimises
+//   loss = (1/K) sum_k ||(L U - A) q_k||^2 / ||A q_k||^2
+// over probe vectors q_k = the Arnoldi vectors of the ILU0-preconditioned
+// operator started from M0^-1 b (the Krylov basis pGMRES itself builds).
+//
+// Kernels: every layer is "one warp per row (node or edge), one lane per
+// output unit" with the weights transposed into shared memory; they are
+// gather/HBM-bound (a few hundred bytes and ~2-6 kflop per row), so they run
+// on the FP32 (or FP64) pipes.  Weight gradients are per-CTA partial sums of
+// outer products over a fixed partition of the rows, summed in CTA order:
+// training steps are deterministic.  Everything is templated on T: float for
+// training and inference, double for the gradient check against the oracle.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+#include "precond.hpp"
+#include "reduce.cuh"
+
+namespace bsp {
+namespace lf {
+
+constexpr int H = 32;
+constexpr int kLayers = 3;
+constexpr double kAlpha = 0.01;
+constexpr int kB2 = 64;              // 8x8 blocks
+constexpr int kWarps = 8;            // warps per CTA of the row kernels
+constexpr int kGradBlocks = 2 * kB200SMs;
+constexpr int kLossThreads = 256;
+
+struct Graph {
+  int n, E, nnzb;
+  const int* row_ptr;
+  const int* col_idx;
+  const int* diag_pos;  // n
+  const int* e_blk;     // E
+  const int* e_row;
+  const int* e_col;
+  const int* er_ptr;    // n+1: edges of row i
+  const int* ec_ptr;    // n+1: edges whose column is j ...
+  const int* ec_idx;    // ... listed here by increasing row
+  const int* lt_ptr;    // n+1: strictly-lower blocks (i, j), grouped by column j ...
+  const int* lt_row;    // ... their row i ...
+  const int* lt_blk;    // ... and block index
+};
+
+template <typename T> __device__ __forceinline__ T relu(T v) { return v > T(0) ? v : T(0); }
+
+// ------------------------------------------------------------------ row kernels
+// out(r, o) = sum_t W[o][t] in_r[t] + b[o], o < NOUT: one warp per row.
+template <typename T, int NIN, int NOUT, class In, class Out>
+__global__ void __launch_bounds__(kWarps * 32) k_dense(int rows, const T* __restrict__ W,
+                                                       const T* __restrict__ bias, In in, Out out) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Wt = reinterpret_cast<T*>(smraw);  // [NIN][NOUT]
+  T* bs = Wt + NIN * NOUT;
+  T* xin = bs + NOUT;                   // [kWarps][NIN]
+  for (int e = threadIdx.x; e < NIN * NOUT; e += blockDim.x) {
+    const int o = e / NIN, t = e % NIN;
+    Wt[t * NOUT + o] = W[e];
+  }
+  for (int o = threadIdx.x; o < NOUT; o += blockDim.x) bs[o] = bias[o];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* xv = xin + warp * NIN;
+  for (int r = blockIdx.x * kWarps + warp; r < rows; r += gridDim.x * kWarps) {
+    in.load(r, xv, lane);
+    __syncwarp();
+#pragma unroll
+    for (int oo = 0; oo < NOUT / 32; ++oo) {
+      const int o = lane + 32 * oo;
+      T acc = bs[o];
+#pragma unroll 8
+      for (int t = 0; t < NIN; ++t) acc = fma(Wt[t * NOUT + o], xv[t], acc);
+      out.store(r, o, acc);
+    }
+    __syncwarp();
+  }
+}
+
+// out(r, t) = sum_o W[o][t] g_r[o], t < NIN (the input gradient of a layer).
+template <typename T, int NIN, int NOUT, class G, class Out>
+__global__ void __launch_bounds__(kWarps * 32) k_dense_t(int rows, const T* __restrict__ W, G g, Out out) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Ws = reinterpret_cast<T*>(smraw);  // [NOUT][NIN] as stored
+  T* gin = Ws + NIN * NOUT;             // [kWarps][NOUT]
+  for (int e = threadIdx.x; e < NIN * NOUT; e += blockDim.x) Ws[e] = W[e];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* gv = gin + warp * NOUT;
+  for (int r = blockIdx.x * kWarps + warp; r < rows; r += gridDim.x * kWarps) {
+    g.load(r, gv, lane);
+    __syncwarp();
+#pragma unroll
+    for (int tt = 0; tt < (NIN + 31) / 32; ++tt) {
+      const int t = lane + 32 * tt;
+      if (t < NIN) {
+        T acc = T(0);
+#pragma unroll 8
+        for (int o = 0; o < NOUT; ++o) acc = fma(Ws[o * NIN + t], gv[o], acc);
+        out.store(r, t, acc);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Partial weight/bias gradients: CTA b sums g_r in_r^T and g_r over its fixed
+// chunk of rows; part[b][NOUT*NIN + NOUT].
+template <typename T, int NIN, int NOUT, class G, class In>
+__global__ void __launch_bounds__(256) k_wgrad(int rows, G g, In in, T* __restrict__ part) {
+  constexpr int NE = NOUT * NIN + NOUT;
+  constexpr int PER = (NE + 255) / 256;
+  constexpr int RB = 16;
+  __shared__ T sg[RB][NOUT];
+  __shared__ T sx[RB][NIN];
+  T acc[PER];
+#pragma unroll
+  for (int p = 0; p < PER; ++p) acc[p] = T(0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int chunk = (rows + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
+  for (int base = r0; base < r1; base += RB) {
+    for (int q = warp; q < RB; q += 8) {
+      const int r = base + q;
+      if (r < r1) {
+        g.load(r, sg[q], lane);
+        in.load(r, sx[q], lane);
+      } else {
+        for (int o = lane; o < NOUT; o += 32) sg[q][o] = T(0);
+        for (int t = lane; t < NIN; t += 32) sx[q][t] = T(0);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int e = threadIdx.x + p * 256;
+      if (e < NOUT * NIN) {
+        const int o = e / NIN, t = e % NIN;
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < RB; ++q) s = fma(sg[q][o], sx[q][t], s);
+        acc[p] += s;
+      } else if (e < NE) {
+        const int o = e - NOUT * NIN;
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < RB; ++q) s += sg[q][o];
+        acc[p] += s;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int e = threadIdx.x + p * 256;
+    if (e < NE) part[(int64_t)blockIdx.x * NE + e] = acc[p];
+  }
+}
+
+template <typename T>
+__global__ void k_wgrad_sum(int ne, int nb, const T* __restrict__ part, T* __restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  T s = T(0);
+  for (int b = 0; b < nb; ++b) s += part[(int64_t)b * ne + e];
+  out[e] = s;
+}
+
+// ------------------------------------------------------------------ features
+template <typename T>
+__global__ void k_node_features(Graph g, const double* __restrict__ vals, T* __restrict__ s, T* __restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < g.n; i += (gridDim.x * blockDim.x) >> 5) {
+    const double* D = vals + (int64_t)g.diag_pos[i] * kB2;
+    T ss = T(0);
+    for (int c = lane; c < kB2; c += 32) ss += T(D[c]) * T(D[c]);
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    const T si = sqrt(ss / T(kB2));
+    T* xi = x + (int64_t)i * (kB2 + 1);
+    for (int c = lane; c < kB2; c += 32) xi[c] = T(D[c]) / si;
+    if (lane == 0) {
+      xi[kB2] = log(si);
+      s[i] = si;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_edge_features(Graph g, const double* __restrict__ vals, const T* __restrict__ s,
+                                T* __restrict__ a) {
+  const int lane = threadIdx.x & 31;
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < g.E; k += (gridDim.x * blockDim.x) >> 5) {
+    const double* B = vals + (int64_t)g.e_blk[k] * kB2;
+    const T den = sqrt(s[g.e_row[k]] * s[g.e_col[k]]);
+    for (int c = lane; c < kB2; c += 32) a[(int64_t)k * kB2 + c] = T(B[c]) / den;
+  }
+}
+
+// ------------------------------------------------------------------ functors
+// Input rows (each loads NIN values into dst with the 32 lanes of a warp).
+template <typename T, int N> struct RowIn {       // dst = src[r]
+  const T* src;
+  __device__ void load(int r, T* dst, int lane) const {
+    for (int t = lane; t < N; t += 32) dst[t] = src[(int64_t)r * N + t];
+  }
+};
+template <typename T> struct MsgIn {               // [h[col(k)]; e[k]]
+  const T* h;
+  const T* e;
+  const int* col;
+  __device__ void load(int k, T* dst, int lane) const {
+    dst[lane] = h[(int64_t)col[k] * H + lane];
+    dst[H + lane] = e[(int64_t)k * H + lane];
+  }
+};
+template <typename T> struct UpdIn {               // [h[i]; m[i]], m summed here and stored
+  const T* h;
+  const T* msg;
+  const int* er_ptr;
+  T* m;
+  __device__ void load(int i, T* dst, int lane) const {
+    T acc = T(0);
+    for (int k = er_ptr[i]; k < er_ptr[i + 1]; ++k) acc += msg[(int64_t)k * H + lane];
+    m[(int64_t)i * H + lane] = acc;
+    dst[lane] = h[(int64_t)i * H + lane];
+    dst[H + lane] = acc;
+  }
+};
+template <typename T> struct UpdInStored {         // [h[i]; m[i]] with m already stored
+  const T* h;
+  const T* m;
+  __device__ void load(int i, T* dst, int lane) const {
+    dst[lane] = h[(int64_t)i * H + lane];
+    dst[H + lane] = m[(int64_t)i * H + lane];
+  }
+};
+template <typename T> struct DecIn {               // [h[row]; h[col]; e[k]]
+  const T* h;
+  const T* e;
+  const int* row;
+  const int* col;
+  __device__ void load(int k, T* dst, int lane) const {
+    dst[lane] = h[(int64_t)row[k] * H + lane];
+    dst[H + lane] = h[(int64_t)col[k] * H + lane];
+    dst[2 * H + lane] = e[(int64_t)k * H + lane];
+  }
+};
+
+// Outputs
+template <typename T> struct ReluOut {
+  T* dst;
+  __device__ void store(int r, int o, T v) const { dst[(int64_t)r * H + o] = relu(v); }
+};
+template <typename T> struct ResidOut {            // u = relu(v); h_next = h + u
+  const T* h;
+  T* u;
+  T* hn;
+  __device__ void store(int r, int o, T v) const {
+    const T uv = relu(v);
+    u[(int64_t)r * H + o] = uv;
+    hn[(int64_t)r * H + o] = h[(int64_t)r * H + o] + uv;
+  }
+};
+template <typename T> struct DecEdgeOut {          // dF[blk] = alpha sqrt(s_i s_j) v
+  const T* s;
+  const int* row;
+  const int* col;
+  const int* blk;
+  double* dF;
+  __device__ void store(int k, int o, T v) const {
+    const T sc = T(kAlpha) * sqrt(s[row[k]] * s[col[k]]);
+    dF[(int64_t)blk[k] * kB2 + o] = double(sc * v);
+  }
+};
+template <typename T> struct DecDiagOut {
+  const T* s;
+  const int* diag;
+  double* dF;
+  __device__ void store(int i, int o, T v) const {
+    dF[(int64_t)diag[i] * kB2 + o] = double(T(kAlpha) * s[i] * v);
+  }
+};
+
+// Gradient rows
+template <typename T> struct GEdgeDec {            // alpha sqrt(s_i s_j) gdF[blk[k]]
+  const T* s;
+  const int* row;
+  const int* col;
+  const int* blk;
+  const T* gdF;
+  __device__ void load(int k, T* dst, int lane) const {
+    const T sc = T(kAlpha) * sqrt(s[row[k]] * s[col[k]]);
+    for (int o = lane; o < kB2; o += 32) dst[o] = sc * gdF[(int64_t)blk[k] * kB2 + o];
+  }
+};
+template <typename T> struct GDiagDec {
+  const T* s;
+  const int* diag;
+  const T* gdF;
+  __device__ void load(int i, T* dst, int lane) const {
+    const T sc = T(kAlpha) * s[i];
+    for (int o = lane; o < kB2; o += 32) dst[o] = sc * gdF[(int64_t)diag[i] * kB2 + o];
+  }
+};
+template <typename T> struct GMask {               // g[r] * (act[r] > 0)
+  const T* g;
+  const T* act;
+  __device__ void load(int r, T* dst, int lane) const {
+    const T a = act[(int64_t)r * H + lane];
+    dst[lane] = a > T(0) ? g[(int64_t)r * H + lane] : T(0);
+  }
+};
+template <typename T> struct GMaskRow {            // dm[row(k)] * (msg[k] > 0)
+  const T* dm;
+  const T* msg;
+  const int* row;
+  __device__ void load(int k, T* dst, int lane) const {
+    const T a = msg[(int64_t)k * H + lane];
+    dst[lane] = a > T(0) ? dm[(int64_t)row[k] * H + lane] : T(0);
+  }
+};
+
+// Input-gradient outputs
+template <typename T> struct SplitDecOut {         // t<H: gdr, t<2H: gdc, else de
+  T* gdr;
+  T* gdc;
+  T* de;
+  __device__ void store(int k, int t, T v) const {
+    if (t < H) gdr[(int64_t)k * H + t] = v;
+    else if (t < 2 * H) gdc[(int64_t)k * H + t - H] = v;
+    else de[(int64_t)k * H + t - 2 * H] = v;
+  }
+};
+template <typename T> struct DiagDhOut {           // dh[i] = v + sum gdr(row i) + sum gdc(col i)
+  Graph g;
+  const T* gdr;
+  const T* gdc;
+  T* dh;
+  __device__ void store(int i, int t, T v) const {
+    T acc = v;
+    for (int k = g.er_ptr[i]; k < g.er_ptr[i + 1]; ++k) acc += gdr[(int64_t)k * H + t];
+    for (int q = g.ec_ptr[i]; q < g.ec_ptr[i + 1]; ++q) acc += gdc[(int64_t)g.ec_idx[q] * H + t];
+    dh[(int64_t)i * H + t] = acc;
+  }
+};
+template <typename T> struct UpdBwdOut {           // t<H: dh2 = dh + v; else dm
+  const T* dh;
+  T* dh2;
+  T* dm;
+  __device__ void store(int i, int t, T v) const {
+    if (t < H) dh2[(int64_t)i * H + t] = dh[(int64_t)i * H + t] + v;
+    else dm[(int64_t)i * H + t - H] = v;
+  }
+};
+template <typename T> struct MsgBwdOut {           // t<H: gmh; else de += v
+  T* gmh;
+  T* de;
+  __device__ void store(int k, int t, T v) const {
+    if (t < H) gmh[(int64_t)k * H + t] = v;
+    else de[(int64_t)k * H + t - H] += v;
+  }
+};
+
+template <typename T>
+__global__ void k_gather_cols(Graph g, const T* __restrict__ gmh, T* __restrict__ dh) {
+  const int lane = threadIdx.x & 31;
+  for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < g.n; j += (gridDim.x * blockDim.x) >> 5) {
+    T acc = dh[(int64_t)j * H + lane];
+    for (int q = g.ec_ptr[j]; q < g.ec_ptr[j + 1]; ++q) acc += gmh[(int64_t)g.ec_idx[q] * H + lane];
+    dh[(int64_t)j * H + lane] = acc;
+  }
+}
+
+// ------------------------------------------------------------------ loss
+// Vectors are [K][n][bs]; F = F0 + dF per block, A in FP64.
+template <typename T>
+__global__ void k_loss_upper(Graph g, int bs, int K, const double* __restrict__ F0, const double* __restrict__ dF,
+                             const T* __restrict__ q, T* __restrict__ y) {
+  const int64_t N = (int64_t)g.n * bs;
+  const int b2 = bs * bs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N * K; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e / N);
+    const int64_t li = e % N;
+    const int i = (int)(li / bs), r = (int)(li % bs);
+    const T* qk = q + (int64_t)k * N;
+    T acc = T(0);
+    for (int b = g.row_ptr[i]; b < g.row_ptr[i + 1]; ++b) {
+      const int j = g.col_idx[b];
+      if (j < i) continue;
+      const int64_t o = (int64_t)b * b2 + r * bs;
+      for (int c = 0; c < bs; ++c) acc = fma(T(F0[o + c] + dF[o + c]), qk[(int64_t)j * bs + c], acc);
+    }
+    y[e] = acc;
+  }
+}
+
+// err = y + Lstrict y - A q; per-(probe, CTA) partials of ||Aq||^2 and ||err||^2.
+template <typename T>
+__global__ void __launch_bounds__(kLossThreads) k_loss_lower(Graph g, int bs, int K, const double* __restrict__ F0,
+                                                             const double* __restrict__ dF,
+                                                             const double* __restrict__ Av,
+                                                             const T* __restrict__ q, const T* __restrict__ y,
+                                                             T* __restrict__ err, T* __restrict__ part) {
+  const int64_t N = (int64_t)g.n * bs;
+  const int b2 = bs * bs;
+  const int k = blockIdx.y;
+  const T* qk = q + (int64_t)k * N;
+  const T* yk = y + (int64_t)k * N;
+  T s_aq = T(0), s_err = T(0);
+  for (int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; li < N; li += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(li / bs), r = (int)(li % bs);
+    T w = yk[li], aq = T(0);
+    for (int b = g.row_ptr[i]; b < g.row_ptr[i + 1]; ++b) {
+      const int j = g.col_idx[b];
+      const int64_t o = (int64_t)b * b2 + r * bs;
+      for (int c = 0; c < bs; ++c) {
+        aq = fma(T(Av[o + c]), qk[(int64_t)j * bs + c], aq);
+        if (j < i) w = fma(T(F0[o + c] + dF[o + c]), yk[(int64_t)j * bs + c], w);
+      }
+    }
+    const T ev = w - aq;
+    err[(int64_t)k * N + li] = ev;
+    s_aq = fma(aq, aq, s_aq);
+    s_err = fma(ev, ev, s_err);
+  }
+  __shared__ T sh[2][kLossThreads];
+  sh[0][threadIdx.x] = s_aq;
+  sh[1][threadIdx.x] = s_err;
+  __syncthreads();
+  for (int w = kLossThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[((int64_t)k * gridDim.x + blockIdx.x) * 2 + 0] = sh[0][0];
+    part[((int64_t)k * gridDim.x + blockIdx.x) * 2 + 1] = sh[1][0];
+  }
+}
+
+// c_k = 1 / (K ||A q_k||^2); loss = sum c_k ||err_k||^2 (one thread).
+template <typename T>
+__global__ void k_loss_final(int K, int nb, const T* __restrict__ part, T* __restrict__ ck, double* __restrict__ loss) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double L = 0.0;
+  for (int k = 0; k < K; ++k) {
+    T aq = T(0), er = T(0);
+    for (int b = 0; b < nb; ++b) {
+      aq += part[((int64_t)k * nb + b) * 2 + 0];
+      er += part[((int64_t)k * nb + b) * 2 + 1];
+    }
+    const T c = T(1) / (T(K) * aq);
+    ck[k] = c;
+    L += double(c * er);
+  }
+  *loss = L;
+}
+
+// gy = gw + Lstrict^T gw with gw = 2 c_k err (column gather over the lower blocks)
+template <typename T>
+__global__ void k_loss_gy(Graph g, int bs, int K, const double* __restrict__ F0, const double* __restrict__ dF,
+                          const T* __restrict__ ck, const T* __restrict__ err, T* __restrict__ gy) {
+  const int64_t N = (int64_t)g.n * bs;
+  const int b2 = bs * bs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N * K; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e / N);
+    const int64_t lj = e % N;
+    const int j = (int)(lj / bs), c = (int)(lj % bs);
+    const T* ek = err + (int64_t)k * N;
+    const T two_c = T(2) * ck[k];
+    T acc = two_c * ek[lj];
+    for (int t = g.lt_ptr[j]; t < g.lt_ptr[j + 1]; ++t) {
+      const int i = g.lt_row[t];
+      const int64_t o = (int64_t)g.lt_blk[t] * b2;
+      for (int r = 0; r < bs; ++r)
+        acc = fma(T(F0[o + r * bs + c] + dF[o + r * bs + c]), two_c * ek[(int64_t)i * bs + r], acc);
+    }
+    gy[e] = acc;
+  }
+}
+
+// gF[b] for every block: lower (j < i): sum_k gw_k[i] y_k[j]^T; else sum_k gy_k[i] q_k[j]^T
+template <typename T>
+__global__ void k_loss_gF(Graph g, int bs, int K, const T* __restrict__ ck, const T* __restrict__ err,
+                          const T* __restrict__ y, const T* __restrict__ gy, const T* __restrict__ q,
+                          T* __restrict__ gF) {
+  const int64_t N = (int64_t)g.n * bs;
+  const int b2 = bs * bs;
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < g.n; i += (gridDim.x * blockDim.x) >> 5) {
+    for (int b = g.row_ptr[i]; b < g.row_ptr[i + 1]; ++b) {
+      const int j = g.col_idx[b];
+      const bool lower = j < i;
+      for (int e = lane; e < b2; e += 32) {
+        const int r = e / bs, c = e % bs;
+        T acc = T(0);
+        for (int k = 0; k < K; ++k) {
+          const int64_t base = (int64_t)k * N;
+          const T left = lower ? T(2) * ck[k] * err[base + (int64_t)i * bs + r] : gy[base + (int64_t)i * bs + r];
+          const T right = lower ? y[base + (int64_t)j * bs + c] : q[base + (int64_t)j * bs + c];
+          acc = fma(left, right, acc);
+        }
+        gF[(int64_t)b * b2 + e] = acc;
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_adam(int64_t n, T* __restrict__ p, const T* __restrict__ g, T* __restrict__ m, T* __restrict__ v,
+                       T lr, T b1, T b2, T eps, T c1, T c2) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T gi = g[i];
+    const T mi = b1 * m[i] + (T(1) - b1) * gi;
+    const T vi = b2 * v[i] + (T(1) - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrt(vi / c2) + eps);
+  }
+}
+
+template <typename T> __global__ void k_cast(int64_t n, const double* __restrict__ a, T* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = T(a[i]);
+}
+
+// F0 in A's block order from the ILU0 factor order: F0[perm[e]] = f[e]
+__global__ void k_scatter_f0(int64_t nblk, int b2, const int64_t* __restrict__ perm, const double* __restrict__ f,
+                             double* __restrict__ F0) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nblk * b2; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t blk = e / b2, c = e % b2;
+    F0[perm[blk] * b2 + c] = f[e];
+  }
+}
+
+__global__ void k_normalize(int64_t n, const double* __restrict__ v, const double* __restrict__ nrm2,
+                            double* __restrict__ q) {
+  const double s = 1.0 / sqrt(*nrm2);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    q[i] = v[i] * s;
+}
+__global__ void k_sub_proj(int64_t n, const double* __restrict__ a, const double* __restrict__ x,
+                           double* __restrict__ y) {
+  const double s = -*a;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = fma(s, x[i], y[i]);
+}
+
+}  // namespace lf
+}  // namespace bsp
+
+// ================================================================= host side
+using namespace bsp;
+using namespace bsp::lf;
+
+namespace {
+
+struct ParamSlot {
+  int64_t off;  // W offset; the bias follows W
+  int nout, nin;
+};
+
+struct GraphBuf {
+  const bsp_matrix_s* A = nullptr;
+  DevBuf<int> diag_pos, e_blk, e_row, e_col, er_ptr, ec_ptr, ec_idx, lt_ptr, lt_row, lt_blk;
+  int n = 0, E = 0;
+  Graph view() const {
+    Graph g{};
+    g.n = n;
+    g.E = E;
+    g.nnzb = (int)A->nnzb;
+    g.row_ptr = A->row_ptr.get();
+    g.col_idx = A->col_idx.get();
+    g.diag_pos = diag_pos.get();
+    g.e_blk = e_blk.get();
+    g.e_row = e_row.get();
+    g.e_col = e_col.get();
+    g.er_ptr = er_ptr.get();
+    g.ec_ptr = ec_ptr.get();
+    g.ec_idx = ec_idx.get();
+    g.lt_ptr = lt_ptr.get();
+    g.lt_row = lt_row.get();
+    g.lt_blk = lt_blk.get();
+    return g;
+  }
+};
+
+template <typename V> int upload_vec(DevBuf<V>& d, const std::vector<V>& v) {
+  BSP_TRY(d.alloc(std::max<size_t>(v.size(), 1)));
+  if (!v.empty()) BSP_CUDA_TRY(cudaMemcpy(d.get(), v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return BSP_OK;
+}
+
+int build_graph(const bsp_matrix_s* A, GraphBuf& G) {
+  const int n = A->n_rows;
+  const auto& rp = A->h_row_ptr;
+  const auto& ci = A->h_col_idx;
+  std::vector<int> diag(n, -1), eb, er, ec, erp(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    for (int b = rp[i]; b < rp[i + 1]; ++b) {
+      if (ci[b] == i) {
+        diag[i] = b;
+      } else {
+        eb.push_back(b);
+        er.push_back(i);
+        ec.push_back(ci[b]);
+      }
+    }
+    erp[i + 1] = (int)eb.size();
+    if (diag[i] < 0) {
+      record_error("learned preconditioner: block row " + std::to_string(i) + " has no diagonal block");
+      return BSP_INVALID;
+    }
+  }
+  const int E = (int)eb.size();
+  // edges by column, rows increasing (stable counting sort)
+  std::vector<int> ecp(n + 1, 0), eci(E);
+  for (int k = 0; k < E; ++k) ecp[ec[k] + 1]++;
+  for (int j = 0; j < n; ++j) ecp[j + 1] += ecp[j];
+  {
+    std::vector<int> fill(ecp.begin(), ecp.end() - 1);
+    for (int k = 0; k < E; ++k) eci[fill[ec[k]]++] = k;
+  }
+  // strictly-lower blocks by column
+  std::vector<int> ltp(n + 1, 0), ltr, ltb;
+  for (int k = 0; k < E; ++k)
+    if (ec[k] < er[k]) ltp[ec[k] + 1]++;
+  for (int j = 0; j < n; ++j) ltp[j + 1] += ltp[j];
+  ltr.resize(ltp[n]);
+  ltb.resize(ltp[n]);
+  {
+    std::vector<int> fill(ltp.begin(), ltp.end() - 1);
+    for (int k = 0; k < E; ++k)
+      if (ec[k] < er[k]) {
+        const int t = fill[ec[k]]++;
+        ltr[t] = er[k];
+        ltb[t] = eb[k];
+      }
+  }
+  G.A = A;
+  G.n = n;
+  G.E = E;
+  BSP_TRY(upload_vec(G.diag_pos, diag));
+  BSP_TRY(upload_vec(G.e_blk, eb));
+  BSP_TRY(upload_vec(G.e_row, er));
+  BSP_TRY(upload_vec(G.e_col, ec));
+  BSP_TRY(upload_vec(G.er_ptr, erp));
+  BSP_TRY(upload_vec(G.ec_ptr, ecp));
+  BSP_TRY(upload_vec(G.ec_idx, eci));
+  BSP_TRY(upload_vec(G.lt_ptr, ltp));
+  BSP_TRY(upload_vec(G.lt_row, ltr));
+  BSP_TRY(upload_vec(G.lt_blk, ltb));
+  return BSP_OK;
+}
+
+struct ModelBase {
+  virtual ~ModelBase() = default;
+  virtual int forward(bsp_handle_s* h, const bsp_matrix_s* A, double* dF) = 0;
+  virtual int loss_grad(bsp_handle_s* h, const bsp_matrix_s* A, const double* F0, int K, const double* probes,
+                        double* loss) = 0;
+  virtual int adam(bsp_handle_s* h, double lr, double b1, double b2, double eps) = 0;
+  virtual int get(double* out, int64_t cnt, int which) = 0;
+  virtual int set(const double* in, int64_t cnt) = 0;
+};
+
+}  // namespace
+
+struct bsp_learned_s {
+  bsp_handle_t h = nullptr;
+  int device = 0;
+  int bs = 0, dtype = 0;
+  int64_t n_params = 0;
+  std::vector<ParamSlot> slots;
+  std::unique_ptr<ModelBase> impl;
+};
+
+namespace {
+
+std::vector<ParamSlot> layout(int64_t& total) {
+  std::vector<ParamSlot> s;
+  int64_t off = 0;
+  auto add = [&](int nout, int nin) {
+    s.push_back({off, nout, nin});
+    off += (int64_t)nout * nin + nout;
+  };
+  add(H, kB2 + 1);  // Wn, bn
+  add(H, kB2);      // We, be
+  for (int l = 0; l < kLayers; ++l) {
+    add(H, 2 * H);  // Wm_l, bm_l
+    add(H, 2 * H);  // Wu_l, bu_l
+  }
+  add(kB2, 3 * H);  // Wo, bo
+  add(kB2, H);      // Wd, bd
+  total = off;
+  return s;
+}
+
+template <typename T, int NIN, int NOUT, class In, class Out>
+int run_dense(bsp_handle_s* h, int rows, const T* W, const T* b, In in, Out out) {
+  if (rows <= 0) return BSP_OK;
+  const size_t smem = (size_t)(NIN * NOUT + NOUT + kWarps * NIN) * sizeof(T);
+  auto kern = k_dense<T, NIN, NOUT, In, Out>;
+  BSP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (int)std::min<int64_t>(ceil_div(rows, kWarps), (int64_t)h->num_sms * 8);
+  bsp::count_launch(), kern<<<grid, kWarps * 32, smem, h->stream>>>(rows, W, b, in, out);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+template <typename T, int NIN, int NOUT, class G, class Out>
+int run_dense_t(bsp_handle_s* h, int rows, const T* W, G g, Out out) {
+  if (rows <= 0) return BSP_OK;
+  const size_t smem = (size_t)(NIN * NOUT + kWarps * NOUT) * sizeof(T);
+  auto kern = k_dense_t<T, NIN, NOUT, G, Out>;
+  BSP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (int)std::min<int64_t>(ceil_div(rows, kWarps), (int64_t)h->num_sms * 8);
+  bsp::count_launch(), kern<<<grid, kWarps * 32, smem, h->stream>>>(rows, W, g, out);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+template <typename T, int NIN, int NOUT, class G, class In>
+int run_wgrad(bsp_handle_s* h, int rows, G g, In in, T* part, T* out) {
+  constexpr int NE = NOUT * NIN + NOUT;
+  bsp::count_launch(), k_wgrad<T, NIN, NOUT, G, In><<<kGradBlocks, 256, 0, h->stream>>>(rows, g, in, part);
+  bsp::count_launch(), k_wgrad_sum<T><<<(NE + 255) / 256, 256, 0, h->stream>>>(NE, kGradBlocks, part, out);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
+// grow-only allocation (training steps reuse the buffers)
+template <typename V> int ensure(DevBuf<V>& d, size_t n) {
+  if (d.n >= n && d.p) return BSP_OK;
+  return d.alloc(std::max<size_t>(n, 1));
+}
+
+template <typename T> struct Model : ModelBase {
+  bsp_learned_s* M;
+  DevBuf<T> p, g, m, v, part;
+  int64_t step = 0;
+  // per-matrix cache
+  GraphBuf G;
+  const bsp_matrix_s* cachedA = nullptr;
+  int64_t cached_nnzb = -1;
+  DevBuf<T> s, x, a, e, hs, msgs, ms, us;   // hs: (L+1) n H; msgs: L E H; ms, us: L n H
+  DevBuf<T> dh, dh2, dm, gdr, gdc, de, gmh, gdF;
+  DevBuf<T> q, y, err, gy, lpart, ck;
+  DevBuf<double> dF, dloss;
+
+  explicit Model(bsp_learned_s* mm) : M(mm) {}
+
+  const T* W(int slot) const { return p.get() + M->slots[slot].off; }
+  const T* B(int slot) const {
+    const ParamSlot& sl = M->slots[slot];
+    return p.get() + sl.off + (int64_t)sl.nout * sl.nin;
+  }
+  T* Gp(int slot) { return g.get() + M->slots[slot].off; }
+
+  int init() {
+    const int64_t np = M->n_params;
+    for (DevBuf<T>* b : {&p, &g, &m, &v}) {
+      BSP_TRY(b->alloc(np));
+      BSP_CUDA_TRY(cudaMemset(b->get(), 0, np * sizeof(T)));
+    }
+    BSP_TRY(part.alloc((size_t)kGradBlocks * (kB2 * 3 * H + kB2)));
+    return BSP_OK;
+  }
+
+  int prepare(const bsp_matrix_s* A) {
+    if (cachedA == A && G.A == A && G.n == A->n_rows && cached_nnzb == A->nnzb) return BSP_OK;
+    BSP_TRY(build_graph(A, G));
+    const int n = G.n, E = std::max(G.E, 1);
+    BSP_TRY(s.alloc(n));
+    BSP_TRY(x.alloc((size_t)n * (kB2 + 1)));
+    BSP_TRY(a.alloc((size_t)E * kB2));
+    BSP_TRY(e.alloc((size_t)E * H));
+    BSP_TRY(hs.alloc((size_t)(kLayers + 1) * n * H));
+    BSP_TRY(msgs.alloc((size_t)kLayers * E * H));
+    BSP_TRY(ms.alloc((size_t)kLayers * n * H));
+    BSP_TRY(us.alloc((size_t)kLayers * n * H));
+    BSP_TRY(dF.alloc((size_t)A->nnzb * kB2));
+    cachedA = A;
+    cached_nnzb = A->nnzb;
+    return BSP_OK;
+  }
+
+  // forward; writes dF (A order, FP64) into out (or the internal buffer)
+  int run_forward(bsp_handle_s* h, const bsp_matrix_s* A, double* out) {
+    BSP_TRY(prepare(A));
+    const Graph gr = G.view();
+    const int n = G.n, E = G.E, Es = std::max(E, 1);
+    const int rg = (int)std::min<int64_t>(ceil_div((int64_t)std::max(n, E) * 32, 256), (int64_t)h->num_sms * 16);
+    bsp::count_launch(), k_node_features<T><<<rg, 256, 0, h->stream>>>(gr, A->vals.get(), s.get(), x.get());
+    if (E > 0) bsp::count_launch(), k_edge_features<T><<<rg, 256, 0, h->stream>>>(gr, A->vals.get(), s.get(), a.get());
+    T* h0 = hs.get();
+    BSP_TRY((run_dense<T, kB2 + 1, H>(h, n, W(0), B(0), RowIn<T, kB2 + 1>{x.get()}, ReluOut<T>{h0})));
+    BSP_TRY((run_dense<T, kB2, H>(h, E, W(1), B(1), RowIn<T, kB2>{a.get()}, ReluOut<T>{e.get()})));
+    for (int l = 0; l < kLayers; ++l) {
+      T* hl = hs.get() + (size_t)l * n * H;
+      T* hn = hs.get() + (size_t)(l + 1) * n * H;
+      T* msg = msgs.get() + (size_t)l * Es * H;
+      T* ml = ms.get() + (size_t)l * n * H;
+      T* ul = us.get() + (size_t)l * n * H;
+      BSP_TRY((run_dense<T, 2 * H, H>(h, E, W(2 + 2 * l), B(2 + 2 * l), MsgIn<T>{hl, e.get(), G.e_col.get()},
+                                      ReluOut<T>{msg})));
+      BSP_TRY((run_dense<T, 2 * H, H>(h, n, W(3 + 2 * l), B(3 + 2 * l), UpdIn<T>{hl, msg, G.er_ptr.get(), ml},
+                                      ResidOut<T>{hl, ul, hn})));
+    }
+    const T* hL = hs.get() + (size_t)kLayers * n * H;
+    const int so = 2 + 2 * kLayers;
+    double* dst = out ? out : dF.get();
+    BSP_TRY((run_dense<T, 3 * H, kB2>(h, E, W(so), B(so), DecIn<T>{hL, e.get(), G.e_row.get(), G.e_col.get()},
+                                      DecEdgeOut<T>{s.get(), G.e_row.get(), G.e_col.get(), G.e_blk.get(), dst})));
+    BSP_TRY((run_dense<T, H, kB2>(h, n, W(so + 1), B(so + 1), RowIn<T, H>{hL},
+                                  DecDiagOut<T>{s.get(), G.diag_pos.get(), dst})));
+    return BSP_OK;
+  }
+
+  int forward(bsp_handle_s* h, const bsp_matrix_s* A, double* out) override { return run_forward(h, A, out); }
+
+  int loss_grad(bsp_handle_s* h, const bsp_matrix_s* A, const double* F0, int K, const double* probes,
+                double* loss_out) override {
+    BSP_TRY(run_forward(h, A, nullptr));
+    const Graph gr = G.view();
+    const int n = G.n, E = G.E, Es = std::max(E, 1), bs = 8;
+    const int64_t N = (int64_t)n * bs;
+    BSP_TRY(ensure(q, N * K));
+    BSP_TRY(ensure(y, N * K));
+    BSP_TRY(ensure(err, N * K));
+    BSP_TRY(ensure(gy, N * K));
+    BSP_TRY(ensure(ck, K));
+    BSP_TRY(ensure(gdF, (size_t)A->nnzb * kB2));
+    for (DevBuf<T>* b : {&dh, &dh2, &dm}) BSP_TRY(ensure(*b, (size_t)n * H));
+    for (DevBuf<T>* b : {&gdr, &gdc, &de, &gmh}) BSP_TRY(ensure(*b, (size_t)Es * H));
+    BSP_TRY(ensure(dloss, 1));
+    const int lgrid = kB200SMs * 2;
+    BSP_TRY(ensure(lpart, (size_t)K * lgrid * 2));
+    const int eg = grid_for(h, N * K, 256);
+    bsp::count_launch(), k_cast<T><<<eg, 256, 0, h->stream>>>(N * K, probes, q.get());
+    bsp::count_launch(), k_loss_upper<T><<<eg, 256, 0, h->stream>>>(gr, bs, K, F0, dF.get(), q.get(), y.get());
+    bsp::count_launch(), k_loss_lower<T><<<dim3(lgrid, K), kLossThreads, 0, h->stream>>>(
+        gr, bs, K, F0, dF.get(), A->vals.get(), q.get(), y.get(), err.get(), lpart.get());
+    bsp::count_launch(), k_loss_final<T><<<1, 32, 0, h->stream>>>(K, lgrid, lpart.get(), ck.get(), dloss.get());
+    bsp::count_launch(), k_loss_gy<T><<<eg, 256, 0, h->stream>>>(gr, bs, K, F0, dF.get(), ck.get(), err.get(), gy.get());
+    const int ng = (int)std::min<int64_t>(ceil_div((int64_t)n * 32, 256), (int64_t)h->num_sms * 16);
+    bsp::count_launch(), k_loss_gF<T><<<ng, 256, 0, h->stream>>>(gr, bs, K, ck.get(), err.get(), y.get(), gy.get(),
+                                                                q.get(), gdF.get());
+    BSP_CUDA_TRY(cudaPeekAtLastError());
+    // network backward: decoders
+    const T* hL = hs.get() + (size_t)kLayers * n * H;
+    const int so = 2 + 2 * kLayers;
+    GEdgeDec<T> ge{s.get(), G.e_row.get(), G.e_col.get(), G.e_blk.get(), gdF.get()};
+    GDiagDec<T> gd{s.get(), G.diag_pos.get(), gdF.get()};
+    if (E > 0) {
+      BSP_TRY((run_wgrad<T, 3 * H, kB2>(h, E, ge, DecIn<T>{hL, e.get(), G.e_row.get(), G.e_col.get()}, part.get(),
+                                        Gp(so))));
+      BSP_TRY((run_dense_t<T, 3 * H, kB2>(h, E, W(so), ge, SplitDecOut<T>{gdr.get(), gdc.get(), de.get()})));
+    } else {
+      BSP_CUDA_TRY(cudaMemsetAsync(Gp(so), 0, (size_t)(kB2 * 3 * H + kB2) * sizeof(T), h->stream));
+    }
+    BSP_TRY((run_wgrad<T, H, kB2>(h, n, gd, RowIn<T, H>{hL}, part.get(), Gp(so + 1))));
+    BSP_TRY((run_dense_t<T, H, kB2>(h, n, W(so + 1), gd, DiagDhOut<T>{gr, gdr.get(), gdc.get(), dh.get()})));
+    // message-passing layers, last first
+    T* dcur = dh.get();
+    T* dnext = dh2.get();
+    for (int l = kLayers - 1; l >= 0; --l) {
+      T* hl = hs.get() + (size_t)l * n * H;
+      T* msg = msgs.get() + (size_t)l * Es * H;
+      T* ml = ms.get() + (size_t)l * n * H;
+      T* ul = us.get() + (size_t)l * n * H;
+      GMask<T> gu{dcur, ul};
+      BSP_TRY((run_wgrad<T, 2 * H, H>(h, n, gu, UpdInStored<T>{hl, ml}, part.get(), Gp(3 + 2 * l))));
+      BSP_TRY((run_dense_t<T, 2 * H, H>(h, n, W(3 + 2 * l), gu, UpdBwdOut<T>{dcur, dnext, dm.get()})));
+      if (E > 0) {
+        GMaskRow<T> gm{dm.get(), msg, G.e_row.get()};
+        BSP_TRY((run_wgrad<T, 2 * H, H>(h, E, gm, MsgIn<T>{hl, e.get(), G.e_col.get()}, part.get(), Gp(2 + 2 * l))));
+        BSP_TRY((run_dense_t<T, 2 * H, H>(h, E, W(2 + 2 * l), gm, MsgBwdOut<T>{gmh.get(), de.get()})));
+        bsp::count_launch(), k_gather_cols<T><<<ng, 256, 0, h->stream>>>(gr, gmh.get(), dnext);
+      } else {
+        BSP_CUDA_TRY(cudaMemsetAsync(Gp(2 + 2 * l), 0, (size_t)(H * 2 * H + H) * sizeof(T), h->stream));
+      }
+      std::swap(dcur, dnext);
+    }
+    if (E > 0)
+      BSP_TRY((run_wgrad<T, kB2, H>(h, E, GMask<T>{de.get(), e.get()}, RowIn<T, kB2>{a.get()}, part.get(), Gp(1))));
+    else
+      BSP_CUDA_TRY(cudaMemsetAsync(Gp(1), 0, (size_t)(H * kB2 + H) * sizeof(T), h->stream));
+    BSP_TRY((run_wgrad<T, kB2 + 1, H>(h, n, GMask<T>{dcur, hs.get()}, RowIn<T, kB2 + 1>{x.get()}, part.get(), Gp(0))));
+    BSP_CUDA_TRY(cudaMemcpyAsync(loss_out, dloss.get(), sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BSP_OK;
+  }
+
+  int adam(bsp_handle_s* h, double lr, double b1, double b2, double eps) override {
+    ++step;
+    const double c1 = 1.0 - std::pow(b1, (double)step), c2 = 1.0 - std::pow(b2, (double)step);
+    bsp::count_launch(), k_adam<T><<<grid_for(h, M->n_params, 256), 256, 0, h->stream>>>(
+        M->n_params, p.get(), g.get(), m.get(), v.get(), (T)lr, (T)b1, (T)b2, (T)eps, (T)c1, (T)c2);
+    BSP_CUDA_TRY(cudaPeekAtLastError());
+    return BSP_OK;
+  }
+
+  int get(double* out, int64_t cnt, int which) override {
+    if (cnt < M->n_params) return BSP_INVALID;
+    std::vector<T> tmp(M->n_params);
+    BSP_CUDA_TRY(cudaMemcpy(tmp.data(), which ? g.get() : p.get(), M->n_params * sizeof(T), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < M->n_params; ++i) out[i] = (double)tmp[i];
+    return BSP_OK;
+  }
+  int set(const double* in, int64_t cnt) override {
+    if (cnt != M->n_params) return BSP_INVALID;
+    std::vector<T> tmp(in, in + cnt);
+    BSP_CUDA_TRY(cudaMemcpy(p.get(), tmp.data(), cnt * sizeof(T), cudaMemcpyHostToDevice));
+    BSP_CUDA_TRY(cudaMemset(m.get(), 0, cnt * sizeof(T)));
+    BSP_CUDA_TRY(cudaMemset(v.get(), 0, cnt * sizeof(T)));
+    step = 0;
+    return BSP_OK;
+  }
+};
+
+}  // namespace
+
+namespace bsp {
+int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha, const void* x, double beta,
+                const void* z, void* y, cudaStream_t s);
+int precond_build_learned(bsp_precond_s* pc, const double* dF);
+}  // namespace bsp
+
+// ================================================================= C ABI
+extern "C" {
+
+int bsp_learned_create(bsp_handle_t h, int bs, int dtype, bsp_learned_t* out) {
+  if (!h || !out) return BSP_INVALID;
+  *out = nullptr;
+  if (bs != 8 || (dtype != BSP_F32 && dtype != BSP_F64)) {
+    record_error("the learned preconditioner supports 8x8 blocks and FP32 or FP64 arithmetic");
+    return BSP_INVALID;
+  }
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  auto M = std::make_unique<bsp_learned_s>();
+  M->h = h;
+  M->device = h->device;
+  M->bs = bs;
+  M->dtype = dtype;
+  M->slots = layout(M->n_params);
+  if (dtype == BSP_F32) {
+    auto m = std::make_unique<Model<float>>(M.get());
+    BSP_TRY(m->init());
+    M->impl = std::move(m);
+  } else {
+    auto m = std::make_unique<Model<double>>(M.get());
+    BSP_TRY(m->init());
+    M->impl = std::move(m);
+  }
+  *out = M.release();
+  return BSP_OK;
+}
+
+int bsp_learned_destroy(bsp_learned_t M) {
+  if (!M) return BSP_OK;
+  cudaSetDevice(M->device);
+  delete M;
+  return BSP_OK;
+}
+
+int bsp_learned_param_count(bsp_learned_t M, int64_t* count) {
+  if (!M || !count) return BSP_INVALID;
+  *count = M->n_params;
+  return BSP_OK;
+}
+
+int bsp_learned_set_params(bsp_learned_t M, const double* params, int64_t count) {
+  if (!M || !params) return BSP_INVALID;
+  cudaSetDevice(M->device);
+  return M->impl->set(params, count);
+}
+
+int bsp_learned_get_params(bsp_learned_t M, double* params, int64_t count) {
+  if (!M || !params) return BSP_INVALID;
+  cudaSetDevice(M->device);
+  return M->impl->get(params, count, 0);
+}
+
+int bsp_learned_get_grads(bsp_learned_t M, double* grads, int64_t count) {
+  if (!M || !grads) return BSP_INVALID;
+  cudaSetDevice(M->device);
+  return M->impl->get(grads, count, 1);
+}
+
+int bsp_learned_forward(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, double* dF) {
+  if (!h || !M || !A || !dF || A->bs != M->bs || A->n_rows != A->n_cols) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  BSP_TRY(M->impl->forward(h, A, dF));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+int bsp_learned_ilu_factors(bsp_handle_t h, bsp_precond_t ilu, double* F0) {
+  if (!h || !ilu || !F0 || ilu->kind != BSP_PC_ILU0) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  const int b2 = ilu->bs * ilu->bs;
+  bsp::count_launch(), k_scatter_f0<<<grid_for(h, ilu->f_nnzb * b2, 256), 256, 0, h->stream>>>(
+      ilu->f_nnzb, b2, ilu->d_perm.get(), ilu->f_vals.get(), F0);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+int bsp_learned_loss_grad(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, const double* F0, int n_probes,
+                          const double* probes, double* loss) {
+  if (!h || !M || !A || !F0 || !probes || !loss || n_probes < 1 || n_probes > 65535 || A->bs != M->bs)
+    return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  return M->impl->loss_grad(h, A, F0, n_probes, probes, loss);
+}
+
+int bsp_learned_adam_step(bsp_handle_t h, bsp_learned_t M, double lr, double beta1, double beta2, double eps) {
+  if (!h || !M) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  return M->impl->adam(h, lr, beta1, beta2, eps);
+}
+
+int bsp_learned_probes(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, int K, double* probes) {
+  if (!h || !A || !b || !probes || K < 1) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  const int64_t N = (int64_t)A->n_rows * A->bs;
+  DevBuf<double> v, sc;
+  BSP_TRY(v.alloc(N));
+  BSP_TRY(sc.alloc(2));
+  const int g = grid_for(h, N, 256);
+  // q_0 = M^-1 b / ||.||; q_{j+1} = orthonormalised M^-1 A q_j (modified Gram-Schmidt)
+  BSP_CUDA_TRY(cudaMemcpyAsync(v.get(), b, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, v.get(), v.get()));
+  for (int j = 0; j < K; ++j) {
+    if (j > 0) {
+      BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, probes + (int64_t)(j - 1) * N, 0.0, nullptr, v.get(), h->stream));
+      if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, v.get(), v.get()));
+      for (int i = 0; i < j; ++i) {
+        BSP_TRY(bsp_dot_dev(h, N, probes + (int64_t)i * N, v.get(), sc.get()));
+        bsp::count_launch(), k_sub_proj<<<g, 256, 0, h->stream>>>(N, sc.get(), probes + (int64_t)i * N, v.get());
+      }
+    }
+    BSP_TRY(bsp_dot_dev(h, N, v.get(), v.get(), sc.get() + 1));
+    bsp::count_launch(), k_normalize<<<g, 256, 0, h->stream>>>(N, v.get(), sc.get() + 1, probes + (int64_t)j * N);
+  }
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int precision, bsp_precond_t* out) {
+  if (!h || !M || !A || !out || A->bs != M->bs || A->n_rows != A->n_cols) return BSP_INVALID;
+  *out = nullptr;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  DevBuf<double> dF;
+  BSP_TRY(dF.alloc((size_t)A->nnzb * A->bs * A->bs));
+  BSP_TRY(M->impl->forward(h, A, dF.get()));
+  auto pc = std::make_unique<bsp_precond_s>();
+  pc->h = h;
+  pc->device = h->device;
+  pc->A = A;
+  pc->kind = BSP_PC_LEARNED_LU;
+  pc->n = A->n_rows;
+  pc->bs = A->bs;
+  pc->precision = precision;
+  if (precision != BSP_PREC_F64)
+    BSP_TRY(bsp_matrix_make_lowp(A, precision == BSP_PREC_F32 ? BSP_F32 : BSP_BF16));
+  BSP_TRY(precond_build_learned(pc.get(), dF.get()));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = pc.release();
+  return BSP_OK;
+}
+
+}  // extern "C"

@@ -1016,6 +1016,32 @@ int precond_build(bsp_precond_s* pc) {
   return make_lowp_copies(pc);
 }
 
+__global__ void k_add_perm(int64_t nblk, int b2, const int64_t* __restrict__ perm, const double* __restrict__ dF,
+                           double* __restrict__ f) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nblk * b2; e += (int64_t)gridDim.x * blockDim.x)
+    f[e] += dF[perm[e / b2] * b2 + e % b2];
+}
+
+// Learned LU: the block-ILU0 factors plus a correction dF given in A's block
+// order; the diagonal inverses are recomputed from the corrected U_ii.
+int precond_build_learned(bsp_precond_s* pc, const double* dF) {
+  const int n = pc->n, b2 = pc->bs * pc->bs;
+  BSP_TRY(pc->dinv.alloc((size_t)std::max(n, 1) * b2));
+  BSP_TRY(pc->flags.alloc(std::max(n, 1)));
+  BSP_TRY(pc->ticket.alloc(1));
+  BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
+  BSP_TRY(build_factor_structure(pc, false));
+  BSP_TRY(run_factor(pc, FACT_ILU0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(), pc->f_diag.get(),
+                     pc->f_vals.get(), n));
+  const int64_t tot = pc->f_nnzb * b2;
+  if (tot > 0)
+    bsp::count_launch(), k_add_perm<<<grid_for(pc->h, tot, 256), 256, 0, pc->h->stream>>>(
+        pc->f_nnzb, b2, pc->d_perm.get(), dF, pc->f_vals.get());
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  BSP_TRY(run_factor(pc, FACT_DIAG, nullptr, pc->f_ptr.get(), pc->f_col.get(), pc->f_diag.get(), pc->f_vals.get(), n));
+  return make_lowp_copies(pc);
+}
+
 // ---------------------------------------------------------------- apply
 // z = M^{-1} r (z may alias r).  AT = double (FP64) or float (mixed precision).
 template <typename VT, typename AT>
@@ -1290,14 +1316,14 @@ int bsp_precond_export(bsp_precond_t pc, double* vals_host, int64_t capacity) {
   BSP_CUDA_TRY(cudaSetDevice(pc->device));
   const int b2 = pc->bs * pc->bs;
   bsp_handle_s* h = pc->h;
-  if (pc->kind == BSP_PC_ILU0 || pc->kind == BSP_PC_ICHOL0) {
-    // blocks in the caller's layout: ILU0 in A's block order; IChol0 in the
+  if (pc->kind == BSP_PC_ILU0 || pc->kind == BSP_PC_ICHOL0 || pc->kind == BSP_PC_LEARNED_LU) {
+    // blocks in the caller's layout: ILU0 / learned LU in A's block order; IChol0 in the
     // order of A.lowTri() (A's rows, blocks with col <= row in stored order)
     const int64_t nf = pc->f_nnzb;
     if (capacity < nf * b2) return BSP_INVALID;
     std::vector<double> f(nf * b2);
     BSP_CUDA_TRY(cudaMemcpy(f.data(), pc->f_vals.get(), f.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    if (pc->kind == BSP_PC_ILU0) {
+    if (pc->kind != BSP_PC_ICHOL0) {
       for (int64_t e = 0; e < nf; ++e)
         std::copy(f.begin() + e * b2, f.begin() + (e + 1) * b2, vals_host + pc->h_perm[e] * b2);
     } else {

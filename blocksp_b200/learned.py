@@ -1,0 +1,258 @@
+"""Learned block-LU preconditioner: host side of the network in learned.cu.
+
+The network (a 3-layer message-passing network, hidden width 32, over the block
+graph of A) is trained on the GPU by the library's own forward and backward
+kernels; this module drives it: parameter I/O, probe generation, the training
+loop, and ``LearnedLU(A, model)`` which builds the preconditioner, falling back
+to block ILU0 when the model did not beat ILU0's iteration count on its
+held-out validation systems.
+
+No reference counterpart (the reference's preconditioners end at IChol0,
+blocksp_preconditioners.hpp:364-538); the produced factors keep A's sparsity
+and are applied by the same triangular sweeps as ILU0 (ILU0::invmul order).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+from .api import Handle, Matrix, Precond, _ptr, default_handle
+
+LAYERS = 3
+HIDDEN = 32
+WEIGHTS = Path(__file__).resolve().parent / "weights" / "learned_convdiff_bs8.npz"
+
+
+def param_shapes(bs: int = 8, H: int = HIDDEN, layers: int = LAYERS) -> dict[str, tuple]:
+    b2 = bs * bs
+    shp = {"Wn": (H, b2 + 1), "bn": (H,), "We": (H, b2), "be": (H,)}
+    for l in range(layers):
+        shp.update({f"Wm{l}": (H, 2 * H), f"bm{l}": (H,), f"Wu{l}": (H, 2 * H), f"bu{l}": (H,)})
+    shp.update({"Wo": (b2, 3 * H), "bo": (b2,), "Wd": (b2, H), "bd": (b2,)})
+    return shp
+
+
+def flatten(params: dict[str, np.ndarray], bs: int = 8) -> np.ndarray:
+    return np.concatenate([np.asarray(params[k], dtype=np.float64).ravel() for k in param_shapes(bs)])
+
+
+def unflatten(flat: np.ndarray, bs: int = 8) -> dict[str, np.ndarray]:
+    out, off = {}, 0
+    for k, s in param_shapes(bs).items():
+        n = int(np.prod(s))
+        out[k] = np.array(flat[off:off + n]).reshape(s)
+        off += n
+    return out
+
+
+def init_params(bs: int = 8, seed: int = 0) -> dict[str, np.ndarray]:
+    """He-scaled encoders and message layers; zero decoders, so the initial
+    preconditioner is exactly block ILU0."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for k, s in param_shapes(bs).items():
+        if k.startswith("W") and k not in ("Wo", "Wd"):
+            out[k] = rng.standard_normal(s) * np.sqrt(2.0 / s[1])
+        else:
+            out[k] = np.zeros(s)
+    return out
+
+
+class LearnedModel:
+    """Device-resident network parameters with their Adam state."""
+
+    def __init__(self, handle: Handle | None = None, bs: int = 8, dtype: int = _lib.BSP_F32,
+                 params=None, meta: dict | None = None):
+        self.handle = handle or default_handle()
+        self.bs = bs
+        self.dtype = dtype
+        m = C.c_void_p()
+        check(self.handle.lib.bsp_learned_create(self.handle.h, bs, dtype, C.byref(m)), "bsp_learned_create",
+              self.handle.h)
+        self.m = m
+        self.handle.adopt(self)
+        cnt = C.c_int64()
+        check(self.handle.lib.bsp_learned_param_count(self.m, C.byref(cnt)), "bsp_learned_param_count")
+        self.n_params = cnt.value
+        self.meta = dict(meta or {})
+        self.set_params(params if params is not None else init_params(bs))
+
+    # -------------------------------------------------------------- parameters
+    def set_params(self, params) -> None:
+        flat = flatten(params, self.bs) if isinstance(params, dict) else np.asarray(params, dtype=np.float64)
+        flat = np.ascontiguousarray(flat, dtype=np.float64)
+        if flat.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {flat.size}")
+        check(self.handle.lib.bsp_learned_set_params(self.m, _ptr(flat), flat.size), "bsp_learned_set_params")
+
+    def params(self) -> dict[str, np.ndarray]:
+        flat = np.zeros(self.n_params)
+        check(self.handle.lib.bsp_learned_get_params(self.m, _ptr(flat), flat.size), "bsp_learned_get_params")
+        return unflatten(flat, self.bs)
+
+    def grads(self) -> dict[str, np.ndarray]:
+        flat = np.zeros(self.n_params)
+        check(self.handle.lib.bsp_learned_get_grads(self.m, _ptr(flat), flat.size), "bsp_learned_get_grads")
+        return unflatten(flat, self.bs)
+
+    def save(self, path: str | Path) -> None:
+        path = Path(path)
+        path.parent.mkdir(parents=True, exist_ok=True)
+        np.savez(path, params=flatten(self.params(), self.bs), meta=json.dumps(self.meta))
+
+    @classmethod
+    def load(cls, path: str | Path = WEIGHTS, handle: Handle | None = None, dtype: int = _lib.BSP_F32):
+        d = np.load(path)
+        meta = json.loads(str(d["meta"]))
+        return cls(handle, int(meta.get("bs", 8)), dtype, params=d["params"], meta=meta)
+
+    # -------------------------------------------------------------- kernels
+    def forward(self, A: Matrix):
+        """dF (nnzb, bs, bs) in A's block order, as a device tensor."""
+        import torch
+        dF = torch.empty((A.nnzb, self.bs, self.bs), dtype=torch.float64, device="cuda")
+        check(self.handle.lib.bsp_learned_forward(self.handle.h, self.m, A.m, _ptr(dF)), "bsp_learned_forward",
+              self.handle.h)
+        return dF
+
+    def loss_grad(self, A: Matrix, F0, probes) -> float:
+        loss = C.c_double()
+        check(self.handle.lib.bsp_learned_loss_grad(self.handle.h, self.m, A.m, _ptr(F0), int(probes.shape[0]),
+                                                    _ptr(probes), C.byref(loss)), "bsp_learned_loss_grad",
+              self.handle.h)
+        return loss.value
+
+    def adam_step(self, lr: float = 1e-4, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        check(self.handle.lib.bsp_learned_adam_step(self.handle.h, self.m, lr, beta1, beta2, eps),
+              "bsp_learned_adam_step", self.handle.h)
+
+    def precond(self, A: Matrix, precision: int = _lib.PREC_F64) -> Precond:
+        p = C.c_void_p()
+        check(self.handle.lib.bsp_learned_precond(self.handle.h, self.m, A.m, precision, C.byref(p)),
+              "bsp_learned_precond", self.handle.h)
+        return Precond.wrap(A, p, _lib.PC_LEARNED_LU)
+
+    def close(self) -> None:
+        if getattr(self, "m", None):
+            self.handle.lib.bsp_learned_destroy(self.m)
+            self.m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ilu_factors(A: Matrix, ilu: Precond):
+    """Block-ILU0 factors in A's block order (device tensor, FP64)."""
+    import torch
+    F0 = torch.empty((A.nnzb, A.bs, A.bs), dtype=torch.float64, device="cuda")
+    check(A.handle.lib.bsp_learned_ilu_factors(A.handle.h, ilu.p, _ptr(F0)), "bsp_learned_ilu_factors",
+          A.handle.h)
+    return F0
+
+
+def probes(A: Matrix, pc: Precond | None, b, K: int):
+    """K orthonormal Arnoldi vectors of M^-1 A started from M^-1 b (device)."""
+    import torch
+    bd = b if hasattr(b, "data_ptr") else torch.tensor(np.asarray(b, dtype=np.float64), device="cuda")
+    Q = torch.empty((K, A.n_rows * A.bs), dtype=torch.float64, device="cuda")
+    check(A.handle.lib.bsp_learned_probes(A.handle.h, A.m, pc.p if pc is not None else None, _ptr(bd), int(K),
+                                          _ptr(Q)), "bsp_learned_probes", A.handle.h)
+    return Q
+
+
+def LearnedLU(A: Matrix, model: LearnedModel | None, precision: int = _lib.PREC_F64) -> Precond:
+    """The learned preconditioner, or block ILU0 when the model is absent or its
+    validation showed no gain over ILU0's iteration count (the fallback)."""
+    from .api import ILU0
+    if model is None or not model.meta.get("beats_ilu0", False):
+        return ILU0(A, precision)
+    return model.precond(A, precision)
+
+
+# ------------------------------------------------------------------ training
+
+def solve_iters(A: Matrix, b, pc, tol: float = 1e-10, restart: int = 30, k: int = 10) -> tuple[int, float]:
+    """pGMRES(restart, k) iterations to the FP64 true residual tol, and that residual."""
+    from .api import pGMRES
+    _, info, _ = pGMRES(A, b, tol, pc, 5000, restart, k, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL)
+    return int(info["iters"]), float(info["true_rel_res"])
+
+
+def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, epochs: int = 1,
+          n_probes: int = 16, lr: float = 1e-4, handle: Handle | None = None, seed: int = 0,
+          log=print) -> LearnedModel:
+    """Train on convection-diffusion systems (systems.convection_diffusion_system)
+    with the GPU kernels; then validate against ILU0 on held-out seeds and
+    record whether the model beats ILU0's iteration count (the fallback gate)."""
+    import torch
+    from . import systems
+    from .api import ILU0
+    h = handle or default_handle()
+    model = LearnedModel(h, 8, _lib.BSP_F32, params=init_params(8, seed))
+    t0 = time.time()
+    history = []
+    for ep in range(epochs):
+        for si, s in enumerate(train_seeds):
+            sysm = systems.convection_diffusion_system(dims, 8, int(s))
+            A = Matrix.from_system(sysm, h)
+            ilu = ILU0(A)
+            F0 = ilu_factors(A, ilu)
+            Q = probes(A, ilu, torch.tensor(sysm.b, device="cuda"), n_probes)
+            for _ in range(steps_per_system):
+                loss = model.loss_grad(A, F0, Q)
+                model.adam_step(lr)
+                history.append(loss)
+            ilu.close()
+            A.close()
+            if si % 20 == 0:
+                log(f"epoch {ep} system {si} loss {history[-1]:.6e} ({time.time() - t0:.0f}s)")
+    val = []
+    for s in val_seeds:
+        sysm = systems.convection_diffusion_system(dims, 8, int(s))
+        A = Matrix.from_system(sysm, h)
+        ilu = ILU0(A)
+        it0, r0 = solve_iters(A, sysm.b, ilu)
+        lp = model.precond(A)
+        it1, r1 = solve_iters(A, sysm.b, lp)
+        val.append({"seed": int(s), "ilu0_iters": it0, "learned_iters": it1, "ilu0_res": r0, "learned_res": r1})
+        lp.close()
+        ilu.close()
+        A.close()
+        log(f"validation seed {s}: ILU0 {it0} iterations, learned {it1}")
+    beats = bool(val) and sum(v["learned_iters"] for v in val) < sum(v["ilu0_iters"] for v in val) and \
+        all(v["learned_res"] <= 1e-10 for v in val)
+    model.meta = {"bs": 8, "hidden": HIDDEN, "layers": LAYERS, "dims": list(dims),
+                  "train_seeds": [int(s) for s in train_seeds], "val_seeds": [int(s) for s in val_seeds],
+                  "steps_per_system": steps_per_system, "epochs": epochs, "n_probes": n_probes, "lr": lr,
+                  "loss_first": history[0] if history else None, "loss_last": history[-1] if history else None,
+                  "loss_history": history[:: max(1, len(history) // 200)], "validation": val,
+                  "beats_ilu0": beats, "train_seconds": time.time() - t0}
+    return model
+
+
+if __name__ == "__main__":  # pragma: no cover - the training run itself
+    import argparse
+    ap = argparse.ArgumentParser(description="train the learned preconditioner on the GPU")
+    ap.add_argument("--side", type=int, default=64)
+    ap.add_argument("--train", type=int, default=200)
+    ap.add_argument("--val", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=1)
+    ap.add_argument("--probes", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-4)
+    ap.add_argument("--out", default=str(WEIGHTS))
+    a = ap.parse_args()
+    tr = [10_000 + i for i in range(a.train)]
+    va = [20_000 + i for i in range(a.val)]
+    m = train(tr, va, (a.side,) * 3, a.steps, a.epochs, a.probes, a.lr)
+    m.save(a.out)
+    print(json.dumps({k: v for k, v in m.meta.items() if k != "loss_history"}))

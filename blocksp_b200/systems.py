@@ -190,6 +190,101 @@ def grid_system(dims: tuple[int, ...], bs: int, seed: int, skew: float = 0.0, nr
                      name=name or f"grid{'x'.join(map(str, dims))}_bs{bs}_s{seed}")
 
 
+def gaussian_field(rng: np.random.Generator, dims: tuple[int, ...], corr_len: float) -> np.ndarray:
+    """Stationary Gaussian random field on the cells, unit variance, covariance
+    ``exp(-r^2 / (2 corr_len^2))``: white noise (this module's normals, in idx
+    order) convolved with a separable Gaussian kernel of std ``corr_len/sqrt(2)``
+    (periodic wrap, taps to 3 std, each axis' taps scaled to unit L2 norm).
+    Returned in idx order (length prod(dims))."""
+    shape = tuple(reversed(dims))
+    w = normals(rng, int(np.prod(dims))).reshape(shape)
+    s = corr_len / math.sqrt(2.0)
+    rad = int(math.ceil(3.0 * s))
+    t = np.arange(-rad, rad + 1)
+    k = np.exp(-(t * t) / (2.0 * s * s))
+    k /= math.sqrt(float(np.sum(k * k)))
+    for a in range(len(shape)):
+        acc = np.zeros_like(w)
+        for tap, kt in zip(t, k):
+            acc += kt * np.roll(w, int(tap), axis=a)
+        w = acc
+    return w.reshape(-1)
+
+
+@dataclass
+class ConvDiffSpec:
+    """Per-system data of a convection-diffusion block system: cell
+    conductivities, the velocity and the block coupling matrix."""
+
+    dims: tuple[int, ...]
+    kappa: np.ndarray     # (n,) exp(sigma * field), idx order
+    velocity: np.ndarray  # (nd,)
+    M: np.ndarray         # (bs, bs) SPD coupling of the bs unknowns of a cell
+    b: np.ndarray         # (n * bs * nrhs,)
+
+
+def convection_diffusion_spec(dims: tuple[int, ...], bs: int, seed: int, sigma: float = 1.0,
+                              corr_len: float = 8.0, speed: float = 0.5, nrhs: int = 1) -> ConvDiffSpec:
+    """Draws, in order: the field's normals (n), the velocity direction's normals
+    (nd), G (bs x bs normals), then b ~ U[-1, 1]."""
+    dims = tuple(int(d) for d in dims)
+    n = int(np.prod(dims))
+    rng = rng_for(seed)
+    g = gaussian_field(rng, dims, corr_len)
+    kappa = np.exp(sigma * g)
+    u = normals(rng, len(dims))
+    vel = speed * u / math.sqrt(float(np.sum(u * u)))
+    G = normals(rng, bs * bs).reshape(bs, bs)
+    M = G @ G.T / bs + 0.1 * np.eye(bs)
+    b = 2.0 * rng.random(n * bs * nrhs) - 1.0
+    return ConvDiffSpec(dims, kappa, vel, M, b)
+
+
+def convection_diffusion_system(dims: tuple[int, ...], bs: int, seed: int, sigma: float = 1.0,
+                                corr_len: float = 8.0, speed: float = 0.5, diag_shift: float = 0.01,
+                                nrhs: int = 1, spec: ConvDiffSpec | None = None) -> BSRSystem:
+    """3D (or 2D) convection-diffusion block system with bs unknowns per cell.
+
+    Cell conductivities kappa = exp(sigma * g), g the unit-variance Gaussian
+    field above (correlation length corr_len cells); edge (p, q = p + e_ax)
+    conductivity is the harmonic mean ``2 kp kq / (kp + kq)``.  Diffusion couples
+    the bs unknowns through the SPD block M = G G^T / bs + 0.1 I; convection by
+    the constant velocity v (uniform direction, |v| = speed) is first-order
+    upwind on each unknown.  Per edge with c = v_ax:
+        A_pp += k_e M + max(-c, 0) I,   A_pq = -k_e M - max(-c, 0) I,
+        A_qq += k_e M + max(c, 0) I,    A_qp = -k_e M - max(c, 0) I,
+    then every diagonal block gets + diag_shift I.
+    """
+    dims = tuple(int(d) for d in dims)
+    sp = spec or convection_diffusion_spec(dims, bs, seed, sigma, corr_len, speed, nrhs)
+    nd = len(dims)
+    n = int(np.prod(dims))
+    shape = tuple(reversed(dims))
+    kap = sp.kappa.reshape(shape)
+    eye = np.eye(bs)
+    diag = np.zeros(shape + (bs, bs))
+    edge_blocks = []
+    for ax in range(nd):
+        arr_ax = nd - 1 - ax
+        lo = [slice(None)] * nd
+        hi = [slice(None)] * nd
+        lo[arr_ax] = slice(0, shape[arr_ax] - 1)
+        hi[arr_ax] = slice(1, shape[arr_ax])
+        kp, kq = kap[tuple(lo)], kap[tuple(hi)]
+        ke = 2.0 * kp * kq / (kp + kq)
+        KM = ke[..., None, None] * sp.M
+        c = float(sp.velocity[ax])
+        cp, cq = max(-c, 0.0), max(c, 0.0)
+        diag[tuple(lo)] += KM + cp * eye   # A_pp: edge towards +axis of p
+        diag[tuple(hi)] += KM + cq * eye   # A_qq: edge towards -axis of q
+        edge_blocks.append((-KM - cp * eye, -KM - cq * eye))
+    diag = diag.reshape(n, bs, bs)
+    diag += diag_shift * eye
+    row_ptr, col_idx, vals = assemble_grid(dims, bs, edge_blocks, diag)
+    return BSRSystem(n=n, bs=bs, row_ptr=row_ptr, col_idx=col_idx, vals=vals, b=sp.b.copy(), nrhs=nrhs,
+                     name=f"convdiff{'x'.join(map(str, dims))}_bs{bs}_s{seed}")
+
+
 # ---- the named workloads ----------------------------------------------------
 
 def config0(seed: int = 0, side: int = 64) -> BSRSystem:

@@ -1,0 +1,235 @@
+"""CPU oracle (numpy, FP64) of the learned block preconditioner's network.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/ to verify the GPU forward /
+backward kernels; never part of the product path.
+
+The reference has no learned component (it is new on this solve path); this
+module is the specification the CUDA kernels implement, written as plainly as
+possible, plus a finite-difference gradient check of the specification itself.
+
+Model (message passing over the block graph of A: nodes = block rows, one
+directed edge k = (i, j) per off-diagonal block A_ij, in CSR order):
+    s_i   = sqrt(mean(A_ii * A_ii))                        node scale
+    x_i   = [A_ii / s_i (bs*bs values), log s_i]            node input
+    a_k   = A_ij / sqrt(s_i s_j)                            edge input
+    h_i   = relu(Wn x_i + bn)                               node encoder
+    e_k   = relu(We a_k + be)                               edge encoder
+    L layers:  msg_k = relu(Wm [h_j; e_k] + bm)
+               m_i   = sum over edges k of row i of msg_k   (CSR order)
+               h_i  <- h_i + relu(Wu [h_i; m_i] + bu)
+    dF_k  = alpha sqrt(s_i s_j) (Wo [h_i; h_j; e_k] + bo)   off-diagonal block
+    dF_ii = alpha s_i (Wd h_i + bd)                         diagonal block
+The preconditioner is M = L U with L = unit lower + strict-lower blocks and U
+the upper blocks (diagonal included) of F = F_ILU0 + dF (A's pattern).
+
+Loss over probe vectors q_1..q_K (Krylov vectors of the ILU0-preconditioned
+operator, generated by the solver):
+    loss = (1/K) sum_k ||(L U - A) q_k||^2 / ||A q_k||^2
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+ALPHA = 0.01
+
+
+@dataclass
+class Graph:
+    n: int
+    row_ptr: np.ndarray   # CSR of A (all blocks)
+    col_idx: np.ndarray
+    diag_pos: np.ndarray  # block index of A_ii per row
+    e_blk: np.ndarray     # block index of each edge (off-diagonal blocks, CSR order)
+    e_row: np.ndarray
+    e_col: np.ndarray
+
+
+def graph_of(row_ptr, col_idx) -> Graph:
+    n = len(row_ptr) - 1
+    rows = np.repeat(np.arange(n), np.diff(row_ptr))
+    blk = np.arange(len(col_idx))
+    off = col_idx != rows
+    diag_pos = np.zeros(n, dtype=np.int64)
+    diag_pos[rows[~off]] = blk[~off]
+    return Graph(n, np.asarray(row_ptr), np.asarray(col_idx), diag_pos, blk[off], rows[off],
+                 np.asarray(col_idx)[off])
+
+
+def param_shapes(bs: int, H: int = 32, L: int = 3) -> dict[str, tuple]:
+    Fn, Fe, B2 = bs * bs + 1, bs * bs, bs * bs
+    shp = {"Wn": (H, Fn), "bn": (H,), "We": (H, Fe), "be": (H,)}
+    for l in range(L):
+        shp[f"Wm{l}"] = (H, 2 * H)
+        shp[f"bm{l}"] = (H,)
+        shp[f"Wu{l}"] = (H, 2 * H)
+        shp[f"bu{l}"] = (H,)
+    shp.update({"Wo": (B2, 3 * H), "bo": (B2,), "Wd": (B2, H), "bd": (B2,)})
+    return shp
+
+
+def init_params(bs: int, seed: int = 0, H: int = 32, L: int = 3) -> dict[str, np.ndarray]:
+    """He-style initial weights; the decoders start at zero so the initial
+    preconditioner is exactly ILU0."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for k, s in param_shapes(bs, H, L).items():
+        if k.startswith("W") and k not in ("Wo", "Wd"):
+            out[k] = rng.standard_normal(s) * np.sqrt(2.0 / s[1])
+        else:
+            out[k] = np.zeros(s)
+    return out
+
+
+def relu(x):
+    return np.maximum(x, 0.0)
+
+
+def features(g: Graph, vals: np.ndarray):
+    bs = vals.shape[1]
+    D = vals[g.diag_pos].reshape(g.n, bs * bs)
+    s = np.sqrt(np.mean(D * D, axis=1))
+    x = np.concatenate([D / s[:, None], np.log(s)[:, None]], axis=1)
+    a = vals[g.e_blk].reshape(-1, bs * bs) / np.sqrt(s[g.e_row] * s[g.e_col])[:, None]
+    return s, x, a
+
+
+def forward(p: dict, g: Graph, vals: np.ndarray, L: int = 3):
+    """Returns dF (nnzb, bs, bs) in A's block order and the cache for backward."""
+    bs = vals.shape[1]
+    s, x, a = features(g, vals)
+    h = relu(x @ p["Wn"].T + p["bn"])
+    e = relu(a @ p["We"].T + p["be"])
+    hs, msgs, ms, us = [h], [], [], []
+    for l in range(L):
+        msg = relu(np.concatenate([h[g.e_col], e], axis=1) @ p[f"Wm{l}"].T + p[f"bm{l}"])
+        m = np.zeros_like(h)
+        np.add.at(m, g.e_row, msg)
+        u = relu(np.concatenate([h, m], axis=1) @ p[f"Wu{l}"].T + p[f"bu{l}"])
+        h = h + u
+        msgs.append(msg)
+        ms.append(m)
+        us.append(u)
+        hs.append(h)
+    se = ALPHA * np.sqrt(s[g.e_row] * s[g.e_col])
+    din = np.concatenate([h[g.e_row], h[g.e_col], e], axis=1)
+    dF = np.zeros((len(g.col_idx), bs * bs))
+    dF[g.e_blk] = se[:, None] * (din @ p["Wo"].T + p["bo"])
+    dF[g.diag_pos] = (ALPHA * s)[:, None] * (h @ p["Wd"].T + p["bd"])
+    cache = dict(s=s, x=x, a=a, e=e, hs=hs, msgs=msgs, ms=ms, us=us, se=se, din=din)
+    return dF.reshape(-1, bs, bs), cache
+
+
+def lu_apply(g: Graph, F: np.ndarray, q: np.ndarray):
+    """(L U) q with L unit lower (strict-lower blocks of F), U the upper blocks;
+    returns (L U q, U q)."""
+    n, bs = g.n, F.shape[1]
+    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
+    qb = q.reshape(n, bs)
+    up = g.col_idx >= rows
+    y = np.zeros((n, bs))
+    np.add.at(y, rows[up], np.einsum("kab,kb->ka", F[up], qb[g.col_idx[up]]))
+    lo = ~up
+    w = y.copy()
+    np.add.at(w, rows[lo], np.einsum("kab,kb->ka", F[lo], y[g.col_idx[lo]]))
+    return w.ravel(), y.ravel()
+
+
+def bsr_apply(g: Graph, vals: np.ndarray, q: np.ndarray) -> np.ndarray:
+    n, bs = g.n, vals.shape[1]
+    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
+    out = np.zeros((n, bs))
+    np.add.at(out, rows, np.einsum("kab,kb->ka", vals, q.reshape(n, bs)[g.col_idx]))
+    return out.ravel()
+
+
+def loss_and_factor_grad(g: Graph, vals: np.ndarray, F: np.ndarray, Q: np.ndarray):
+    """loss and d loss / d F (nnzb, bs, bs) for probes Q (K, n*bs)."""
+    n, bs = g.n, vals.shape[1]
+    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
+    up = g.col_idx >= rows
+    lo = ~up
+    K = Q.shape[0]
+    loss = 0.0
+    gF = np.zeros_like(F)
+    for q in Q:
+        Aq = bsr_apply(g, vals, q)
+        w, y = lu_apply(g, F, q)
+        err = w - Aq
+        c = 1.0 / (K * float(Aq @ Aq))
+        loss += c * float(err @ err)
+        gw = (2.0 * c * err).reshape(n, bs)
+        yb = y.reshape(n, bs)
+        gF[lo] += np.einsum("ka,kb->kab", gw[rows[lo]], yb[g.col_idx[lo]])
+        gy = gw.copy()
+        np.add.at(gy, g.col_idx[lo], np.einsum("kab,ka->kb", F[lo], gw[rows[lo]]))
+        qb = q.reshape(n, bs)
+        gF[up] += np.einsum("ka,kb->kab", gy[rows[up]], qb[g.col_idx[up]])
+    return loss, gF
+
+
+def backward(p: dict, g: Graph, cache: dict, gdF: np.ndarray, L: int = 3) -> dict:
+    """Parameter gradients given d loss / d dF (nnzb, bs, bs)."""
+    B2 = gdF.shape[1] * gdF.shape[2]
+    gdF = gdF.reshape(-1, B2)
+    H = p["bn"].shape[0]
+    s, x, a, e, hs = cache["s"], cache["x"], cache["a"], cache["e"], cache["hs"]
+    grads = {}
+    # decoders
+    go = cache["se"][:, None] * gdF[g.e_blk]                 # (E, B2)
+    grads["Wo"] = go.T @ cache["din"]
+    grads["bo"] = go.sum(0)
+    gdin = go @ p["Wo"]                                      # (E, 3H)
+    gd = (ALPHA * s)[:, None] * gdF[g.diag_pos]              # (n, B2)
+    grads["Wd"] = gd.T @ hs[-1]
+    grads["bd"] = gd.sum(0)
+    dh = gd @ p["Wd"]
+    np.add.at(dh, g.e_row, gdin[:, :H])
+    np.add.at(dh, g.e_col, gdin[:, H:2 * H])
+    de = gdin[:, 2 * H:].copy()
+    # message-passing layers, last first
+    for l in reversed(range(L)):
+        h_in, m, u, msg = hs[l], cache["ms"][l], cache["us"][l], cache["msgs"][l]
+        gu = dh * (u > 0)
+        grads[f"Wu{l}"] = gu.T @ np.concatenate([h_in, m], axis=1)
+        grads[f"bu{l}"] = gu.sum(0)
+        gin = gu @ p[f"Wu{l}"]
+        dh_new = dh + gin[:, :H]
+        dm = gin[:, H:]
+        gpm = dm[g.e_row] * (msg > 0)
+        grads[f"Wm{l}"] = gpm.T @ np.concatenate([h_in[g.e_col], e], axis=1)
+        grads[f"bm{l}"] = gpm.sum(0)
+        gmi = gpm @ p[f"Wm{l}"]
+        np.add.at(dh_new, g.e_col, gmi[:, :H])
+        de += gmi[:, H:]
+        dh = dh_new
+    ge = de * (e > 0)
+    grads["We"] = ge.T @ a
+    grads["be"] = ge.sum(0)
+    gh = dh * (hs[0] > 0)
+    grads["Wn"] = gh.T @ x
+    grads["bn"] = gh.sum(0)
+    return grads
+
+
+def loss_fn(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3) -> float:
+    dF, _ = forward(p, g, vals, L)
+    return loss_and_factor_grad(g, vals, F0 + dF, Q)[0]
+
+
+def loss_and_grads(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3):
+    dF, cache = forward(p, g, vals, L)
+    loss, gF = loss_and_factor_grad(g, vals, F0 + dF, Q)
+    return loss, backward(p, g, cache, gF, L)
+
+
+def finite_difference(p: dict, g: Graph, vals, F0, Q, name: str, idx: tuple, h: float = 1e-6,
+                      L: int = 3) -> float:
+    """Central difference of the loss in one parameter entry."""
+    q = {k: v.copy() for k, v in p.items()}
+    q[name][idx] += h
+    lp = loss_fn(q, g, vals, F0, Q, L)
+    q[name][idx] -= 2 * h
+    lm = loss_fn(q, g, vals, F0, Q, L)
+    return (lp - lm) / (2 * h)

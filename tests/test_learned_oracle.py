@@ -1,0 +1,91 @@
+"""CPU checks of the learned-preconditioner specification (oracle/learned_oracle.py)
+and of the convection-diffusion generator it trains on.
+
+* the oracle's analytic gradients agree with central finite differences
+  (relative error <= 1e-5 on sampled entries of every parameter);
+* with zero decoders the network's correction is exactly zero (the initial
+  preconditioner is block ILU0) and the loss is ILU0's;
+* the generator follows its stated conventions (velocity magnitude, harmonic
+  edge conductivities, upwind blocks, SPD coupling, unit-variance field).
+"""
+import numpy as np
+
+from blocksp_b200 import learned, systems
+import oracle.blocksp_oracle as O
+import oracle.learned_oracle as LO
+
+
+def small_case(seed=7, dims=(4, 3, 3)):
+    s = systems.convection_diffusion_system(dims, 8, seed)
+    g = LO.graph_of(s.row_ptr, s.col_idx)
+    F0 = O.ILU0(O.BSR.from_system(s)).LU.vals
+    return s, g, F0
+
+
+def test_oracle_gradients_match_finite_differences():
+    s, g, F0 = small_case()
+    rng = np.random.default_rng(1)
+    p = LO.init_params(8, seed=3)
+    for k in p:
+        p[k] = p[k] + 0.05 * rng.standard_normal(p[k].shape)
+    Q = rng.standard_normal((3, s.n * 8))
+    _, gr = LO.loss_and_grads(p, g, s.vals, F0, Q)
+    worst = 0.0
+    for name in p:
+        for _ in range(2):
+            idx = tuple(int(rng.integers(0, d)) for d in p[name].shape)
+            fd = LO.finite_difference(p, g, s.vals, F0, Q, name, idx, h=1e-5)
+            an = gr[name][idx]
+            worst = max(worst, abs(fd - an) / max(1e-8, abs(fd) + abs(an)))
+    assert worst <= 1e-5, worst
+
+
+def test_zero_decoders_give_ilu0():
+    s, g, F0 = small_case()
+    p = LO.init_params(8, seed=0)
+    dF, _ = LO.forward(p, g, s.vals)
+    assert not np.any(dF)
+    rng = np.random.default_rng(2)
+    Q = rng.standard_normal((2, s.n * 8))
+    loss, _ = LO.loss_and_factor_grad(g, s.vals, F0, Q)
+    # ILU0's product matches A on the pattern, so the loss only sees fill-in
+    assert 0.0 < loss < 1.0
+
+
+def test_host_parameter_layout_matches_oracle():
+    assert learned.param_shapes(8) == LO.param_shapes(8)
+    assert list(learned.param_shapes(8)) == list(LO.param_shapes(8))
+    p = learned.init_params(8, seed=4)
+    back = learned.unflatten(learned.flatten(p))
+    assert all(np.array_equal(p[k], back[k]) for k in p)
+
+
+def test_generator_conventions():
+    dims = (5, 4, 3)
+    sp = systems.convection_diffusion_spec(dims, 8, 11)
+    assert abs(np.linalg.norm(sp.velocity) - 0.5) < 1e-15
+    assert np.all(np.linalg.eigvalsh(sp.M) > 0.0)
+    s = systems.convection_diffusion_system(dims, 8, 11, spec=sp)
+    A = s.to_dense()
+    nx, ny, _ = dims
+    kap = sp.kappa
+    # edge (p, q = p + 1) along x
+    ke = 2.0 * kap[0] * kap[1] / (kap[0] + kap[1])
+    c = sp.velocity[0]
+    assert np.allclose(A[0:8, 8:16], -ke * sp.M - max(-c, 0.0) * np.eye(8), rtol=0, atol=1e-14)
+    assert np.allclose(A[8:16, 0:8], -ke * sp.M - max(c, 0.0) * np.eye(8), rtol=0, atol=1e-14)
+    # corner cell 0: one edge towards +axis per axis, plus the shift
+    D = 0.01 * np.eye(8)
+    for ax, q in enumerate((1, nx, nx * ny)):
+        ke = 2.0 * kap[0] * kap[q] / (kap[0] + kap[q])
+        D = D + ke * sp.M + max(-sp.velocity[ax], 0.0) * np.eye(8)
+    assert np.allclose(A[:8, :8], D, rtol=0, atol=1e-12)
+
+
+def test_gaussian_field_statistics():
+    rng = systems.rng_for(5)
+    f = systems.gaussian_field(rng, (64, 64, 16), 8.0).reshape(16, 64, 64)
+    assert abs(f.std() - 1.0) < 0.35
+    # correlation at lag 8 along x near exp(-1/2)
+    a = (f * np.roll(f, 8, axis=2)).mean() / f.var()
+    assert 0.3 < a < 0.9
