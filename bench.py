@@ -297,6 +297,156 @@ def cpu_reference_sample(side: int, sample_iters: int, budget_s: float = 25.0) -
     return out
 
 
+# ----------------------------------------------------------------- batch workload
+
+BATCH_METRIC = "batched pCG+IChol0: time to FP64 relative residual 1e-10 for every system x RHS"
+
+
+def batch_bytes_per_iter(n: int, bs: int, nnzb: int, R: int) -> int:
+    """Algorithmic bytes of one batched pCG iteration of one system: A's blocks
+    and indices once (spmv), the strictly-lower IChol0 blocks and inverted
+    diagonals twice (forward and backward sweep), and 19 passes over an
+    n x R x bs vector (spmv 2, update 8 incl. sentinel refills, sweeps 4,
+    r.z 2, p update 3)."""
+    b2 = bs * bs * 8
+    lower = (nnzb - n) // 2
+    return nnzb * b2 + nnzb * 4 + (n + 1) * 4 + 2 * (lower * b2 + n * b2 + lower * 8) + 19 * n * R * bs * 8
+
+
+def batch_cpu_sample(specs, iters, budget_s: float = 25.0) -> dict | None:
+    """The reference's IChol0_pCG (one call per system per RHS, D = 1) timed on
+    a bounded sample of the batch's systems: the smallest systems of each block
+    size, first right-hand side; returns the per-(row x iteration) solve cost
+    and per-row set-up cost per block size."""
+    exe = ref_binary()
+    if exe is None:
+        return None
+    from blocksp_b200 import systems
+    out = {}
+    spent = 0.0
+    for bs in (4, 8):
+        cand = sorted((side, i) for i, (side, b, _) in enumerate(specs) if b == bs)[:2]
+        costs, setups = [], []
+        for side, i in cand:
+            if spent > budget_s:
+                break
+            s = systems.batch_system(side, bs, specs[i][2], nrhs=1)
+            with tempfile.TemporaryDirectory() as d:
+                f = Path(d) / "sys.bsps"
+                systems.write_bsr(f, s)
+                cmd = [str(exe), str(f), "--B", str(bs), "--D", "1", "--solver", "ichol0_pcg", "--tol", "1e-10",
+                       "--maxit", "2000", "--time"]
+                env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+                t0 = time.time()
+                r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=600)
+                spent += time.time() - t0
+            tm = {ln.split()[1]: float(ln.split()[2]) for ln in r.stdout.splitlines() if ln.startswith("TIME ")}
+            if "solve_s" not in tm:
+                continue
+            it = int(iters[i][0]) + 1
+            costs.append(tm["solve_s"] / (s.n * it))
+            setups.append(tm["setup_s"] / s.n)
+        if costs:
+            out[bs] = {"solve_per_row_iter_s": float(np.mean(costs)), "setup_per_row_s": float(np.mean(setups)),
+                       "systems": len(costs)}
+    return out or None
+
+
+def run_batch(args):
+    import torch
+    import blocksp_b200 as bsp
+    from blocksp_b200 import _lib, systems
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    h = bsp.Handle(0, stream=stream.cuda_stream)
+    lib = _lib.load()
+    specs = systems.batch_specs(seed=3, count=args.batch_count)
+    R = 4
+    t0 = time.time()
+    sl = [systems.batch_system(side, bs, seed, nrhs=R) for side, bs, seed in specs]
+    gen_s = time.time() - t0
+    t0 = time.time()
+    B = bsp.Batch(sl, h)
+    create_s = time.time() - t0
+    bh = np.concatenate([s.b for s in sl])
+    bd = torch.tensor(bh, device="cuda")
+    peak, peak_kind = read_peaks()
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    first = None
+    for _ in range(max(args.warmup, 3)):
+        x, info = B.pcg(bd, R, TOL, 2000)
+        first = first or info
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        l0 = lib.bsp_launch_count()
+        e0 = ev()
+        for _ in range(args.steps):
+            x, info = B.pcg(bd, R, TOL, 2000)
+        e1 = ev()
+        e1.synchronize()
+        launches = lib.bsp_launch_count() - l0
+    clocks = clk.summary()
+    solve_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    res = B.results()
+    # algorithmic bytes: every system active for (its slowest pair's iterations + 1)
+    total_bytes = 0
+    for i, s in enumerate(sl):
+        total_bytes += batch_bytes_per_iter(s.n, s.bs, s.nnzb, R) * (int(res["iters"][i].max()) + 1)
+    gbs = total_bytes / solve_s / 1e9
+    # e2e through the host-buffer entry point
+    t0 = time.perf_counter()
+    xh, _ = B.pcg(bh, R, TOL, 2000)
+    e2e_s = time.perf_counter() - t0
+    tun = B.tuning()
+    cpu = None
+    if not args.no_cpu_baseline:
+        cs = batch_cpu_sample(specs, res["iters"])
+        if cs is not None and all(bs in cs for bs in (4, 8)):
+            est = 0.0
+            for i, s in enumerate(sl):
+                c = cs[s.bs]
+                est += c["setup_per_row_s"] * s.n + c["solve_per_row_iter_s"] * s.n * float(
+                    np.sum(res["iters"][i] + 1))
+            cpu = {"value": est, "unit": "s", "cores": 1, "cores_available": os.cpu_count() or 1,
+                   "kind": "reference",
+                   "sample": "reference IChol0_pCG<T,bs,1> on the two smallest systems of each block size "
+                             f"(first RHS), per-row-iteration cost {cs[4]['solve_per_row_iter_s']:.3e} s (bs 4) / "
+                             f"{cs[8]['solve_per_row_iter_s']:.3e} s (bs 8), extrapolated over all "
+                             f"{len(sl)} systems x {R} RHS with the iteration counts of this solve"}
+    n_rows = int(sum(s.n for s in sl))
+    nnzb = int(sum(s.nnzb for s in sl))
+    line = {
+        "metric": BATCH_METRIC, "value": solve_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "dtype": "f64",
+        "data": "synthetic (seeded 2D 5-point block stencils)", "vs_baseline": None, "scaling": "weak",
+        "config": {"workload": f"{len(sl)} SPD 2D block systems, sides log-uniform 32..256, bs 4/8 by seed, "
+                               f"{R} RHS each; batched pCG + block IChol0, FP64, tol 1e-10",
+                   "systems": len(sl), "rhs": R, "block_rows": n_rows, "nnzb": nnzb,
+                   "matrix_gb": sum(s.vals.nbytes for s in sl) / 1e9,
+                   "l2": "inputs larger than L2"},
+        "iterations": {"max": int(res["iters"].max()), "mean": float(res["iters"].mean()),
+                       "graph_iters": info["graph_iters"], "converged_pairs": info["n_converged"],
+                       "pairs": info["n_pairs"]},
+        "setup": {"generate_s": gen_s, "create_s": create_s, "first_solve_autotune_capture_ms": first["setup_ms"]},
+        "tuning": tun,
+        "roofline": {"bound": "hbm", "kernel": "whole batched iteration (spmv + sweeps + vector passes)",
+                     "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes": total_bytes},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": bh.nbytes, "d2h_bytes_per_step": bh.nbytes},
+        "gpu_launches": launches // args.steps, "clocks": clocks, "cpu_baseline": cpu,
+    }
+    B.close()
+    h.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,7 +459,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="plain_f64,mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch"],
+                    help="cfg1: the headline line; batch: the 256-system batched pCG line")
+    ap.add_argument("--batch-count", type=int, default=256)
     args = ap.parse_args()
+    if args.workload == "batch":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batch leg reports its CPU baseline "
+                              "in its own cpu_baseline field"}))
+            return
+        run_batch(args)
+        return
     world, rank, local = dist_setup()
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "
                 f"1e-10; 3D {args.side}^3 7-point block stencil, 8x8 FP64 blocks, skew c=0.3")
