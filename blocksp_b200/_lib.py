@@ -117,6 +117,7 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_learned_adam_step": (_I, [_P, _P, _D, _D, _D, _D]),
     "bsp_learned_probes": (_I, [_P, _P, _P, _P, _I, _P]),
     "bsp_learned_precond": (_I, [_P, _P, _P, _I, C.POINTER(_P)]),
+    "bsp_learned_smooth": (_I, [_P, _P, _P, _I, _I, _P]),
 }
 
 _lib = None

@@ -13,11 +13,15 @@
 //   h = relu(Wn x + bn); e = relu(We a + be)
 //   per layer: msg_k = relu(Wm [h_j; e_k] + bm); m_i = sum_{k in row i} msg_k;
 //              h_i += relu(Wu [h_i; m_i] + bu)
-//   dF_ij = 0.01 sqrt(s_i s_j) (Wo [h_i; h_j; e_k] + bo);  dF_ii = 0.01 s_i (Wd h_i + bd)
-// M = L U with (L, U) the ILU0 factors plus dF.  Training minimises
-//   loss = (1/K) sum_k ||(L U - A) q_k||^2 / ||A q_k||^2
-// over probe vectors q_k = the Arnoldi vectors of the ILU0-preconditioned
-// operator started from M0^-1 b (the Krylov basis pGMRES itself builds).
+//   dF_ij = 0.01 c_ij (Wo [h_i; h_j; e_k] + bo);  dF_ii = 0.01 s_i (Wd h_i + bd)
+//   with c_ij = sqrt(s_i s_j) for upper blocks (U_ij ~ A_ij) and sqrt(s_i / s_j)
+//   for lower blocks (L_ij ~ A_ij U_jj^-1)
+// M = L U with (L, U) the ILU0 factors plus dF.  Training minimises the
+// left-preconditioned operator's distance from the identity on probes,
+//   loss = (1/K) sum_k ||M^-1 A q_k - q_k||^2,
+// q_k the orthonormal Arnoldi vectors of the ILU0-preconditioned operator
+// started from M0^-1 b (the Krylov basis pGMRES itself builds); its gradient
+// needs M^-1 and M^-T, both applied by the sync-free triangular sweeps.
 //
 // Kernels: every layer is "one warp per row (node or edge), one lane per
 // output unit" with the weights transposed into shared memory; they are
@@ -34,6 +38,10 @@
 #include "reduce.cuh"
 
 namespace bsp {
+int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha, const void* x, double beta,
+                const void* z, void* y, cudaStream_t s);
+int precond_build_learned(bsp_precond_s* pc, const double* dF);
+
 namespace lf {
 
 constexpr int H = 32;
@@ -42,7 +50,6 @@ constexpr double kAlpha = 0.01;
 constexpr int kB2 = 64;              // 8x8 blocks
 constexpr int kWarps = 8;            // warps per CTA of the row kernels
 constexpr int kGradBlocks = 2 * kB200SMs;
-constexpr int kLossThreads = 256;
 
 struct Graph {
   int n, E, nnzb;
@@ -55,12 +62,16 @@ struct Graph {
   const int* er_ptr;    // n+1: edges of row i
   const int* ec_ptr;    // n+1: edges whose column is j ...
   const int* ec_idx;    // ... listed here by increasing row
-  const int* lt_ptr;    // n+1: strictly-lower blocks (i, j), grouped by column j ...
-  const int* lt_row;    // ... their row i ...
-  const int* lt_blk;    // ... and block index
 };
 
 template <typename T> __device__ __forceinline__ T relu(T v) { return v > T(0) ? v : T(0); }
+
+// Output scale of the correction of block (i, j): the scale of U_ij for j > i,
+// of L_ij = A_ij U_jj^-1 for j < i.
+template <typename T> __device__ __forceinline__ T edge_scale(const T* s, int i, int j) {
+  const T si = s[i], sj = s[j];
+  return T(kAlpha) * (j < i ? sqrt(si / sj) : sqrt(si * sj));
+}
 
 // ------------------------------------------------------------------ row kernels
 // out(r, o) = sum_t W[o][t] in_r[t] + b[o], o < NOUT: one warp per row.
@@ -278,15 +289,14 @@ template <typename T> struct ResidOut {            // u = relu(v); h_next = h + 
     hn[(int64_t)r * H + o] = h[(int64_t)r * H + o] + uv;
   }
 };
-template <typename T> struct DecEdgeOut {          // dF[blk] = alpha sqrt(s_i s_j) v
+template <typename T> struct DecEdgeOut {          // dF[blk] = edge_scale v
   const T* s;
   const int* row;
   const int* col;
   const int* blk;
   double* dF;
   __device__ void store(int k, int o, T v) const {
-    const T sc = T(kAlpha) * sqrt(s[row[k]] * s[col[k]]);
-    dF[(int64_t)blk[k] * kB2 + o] = double(sc * v);
+    dF[(int64_t)blk[k] * kB2 + o] = double(edge_scale(s, row[k], col[k]) * v);
   }
 };
 template <typename T> struct DecDiagOut {
@@ -299,14 +309,14 @@ template <typename T> struct DecDiagOut {
 };
 
 // Gradient rows
-template <typename T> struct GEdgeDec {            // alpha sqrt(s_i s_j) gdF[blk[k]]
+template <typename T> struct GEdgeDec {            // edge_scale gdF[blk[k]]
   const T* s;
   const int* row;
   const int* col;
   const int* blk;
   const T* gdF;
   __device__ void load(int k, T* dst, int lane) const {
-    const T sc = T(kAlpha) * sqrt(s[row[k]] * s[col[k]]);
+    const T sc = edge_scale(s, row[k], col[k]);
     for (int o = lane; o < kB2; o += 32) dst[o] = sc * gdF[(int64_t)blk[k] * kB2 + o];
   }
 };
@@ -389,137 +399,56 @@ __global__ void k_gather_cols(Graph g, const T* __restrict__ gmh, T* __restrict_
 }
 
 // ------------------------------------------------------------------ loss
-// Vectors are [K][n][bs]; F = F0 + dF per block, A in FP64.
-template <typename T>
-__global__ void k_loss_upper(Graph g, int bs, int K, const double* __restrict__ F0, const double* __restrict__ dF,
-                             const T* __restrict__ q, T* __restrict__ y) {
-  const int64_t N = (int64_t)g.n * bs;
+// loss = (1/K) sum_k ||M^-1 A q_k - q_k||^2 (FP64; probes orthonormal).  With
+// z = M^-1 A q, g = (2/K)(z - q), w = U^-T g, lam = L^-T w, y = U z:
+//   d loss / d L_ij = -sum_k lam_k[i] y_k[j]^T   (strictly lower blocks)
+//   d loss / d U_ij = -sum_k   w_k[i] z_k[j]^T   (upper blocks, diagonal included)
+__global__ void k_diff(int64_t n, const double* __restrict__ z, const double* __restrict__ q, double* __restrict__ e) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    e[i] = z[i] - q[i];
+}
+__global__ void k_scale(int64_t n, double a, double* __restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+// y = U z over the factor's upper blocks (row-sorted factor structure)
+__global__ void k_upper_prod(int n, int bs, const int* __restrict__ fptr, const int* __restrict__ fcol,
+                             const int* __restrict__ fdiag, const double* __restrict__ f, const double* __restrict__ z,
+                             double* __restrict__ y) {
+  const int64_t N = (int64_t)n * bs;
   const int b2 = bs * bs;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N * K; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e / N);
-    const int64_t li = e % N;
-    const int i = (int)(li / bs), r = (int)(li % bs);
-    const T* qk = q + (int64_t)k * N;
-    T acc = T(0);
-    for (int b = g.row_ptr[i]; b < g.row_ptr[i + 1]; ++b) {
-      const int j = g.col_idx[b];
-      if (j < i) continue;
-      const int64_t o = (int64_t)b * b2 + r * bs;
-      for (int c = 0; c < bs; ++c) acc = fma(T(F0[o + c] + dF[o + c]), qk[(int64_t)j * bs + c], acc);
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / bs), r = (int)(e % bs);
+    double acc = 0.0;
+    for (int b = fdiag[i]; b < fptr[i + 1]; ++b) {
+      const int j = fcol[b];
+      const double* blk = f + (int64_t)b * b2 + r * bs;
+      for (int c = 0; c < bs; ++c) acc = fma(blk[c], z[(int64_t)j * bs + c], acc);
     }
     y[e] = acc;
   }
 }
-
-// err = y + Lstrict y - A q; per-(probe, CTA) partials of ||Aq||^2 and ||err||^2.
+// gradient of every factor block, written in A's block order (perm: factor -> A)
 template <typename T>
-__global__ void __launch_bounds__(kLossThreads) k_loss_lower(Graph g, int bs, int K, const double* __restrict__ F0,
-                                                             const double* __restrict__ dF,
-                                                             const double* __restrict__ Av,
-                                                             const T* __restrict__ q, const T* __restrict__ y,
-                                                             T* __restrict__ err, T* __restrict__ part) {
-  const int64_t N = (int64_t)g.n * bs;
-  const int b2 = bs * bs;
-  const int k = blockIdx.y;
-  const T* qk = q + (int64_t)k * N;
-  const T* yk = y + (int64_t)k * N;
-  T s_aq = T(0), s_err = T(0);
-  for (int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; li < N; li += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(li / bs), r = (int)(li % bs);
-    T w = yk[li], aq = T(0);
-    for (int b = g.row_ptr[i]; b < g.row_ptr[i + 1]; ++b) {
-      const int j = g.col_idx[b];
-      const int64_t o = (int64_t)b * b2 + r * bs;
-      for (int c = 0; c < bs; ++c) {
-        aq = fma(T(Av[o + c]), qk[(int64_t)j * bs + c], aq);
-        if (j < i) w = fma(T(F0[o + c] + dF[o + c]), yk[(int64_t)j * bs + c], w);
-      }
-    }
-    const T ev = w - aq;
-    err[(int64_t)k * N + li] = ev;
-    s_aq = fma(aq, aq, s_aq);
-    s_err = fma(ev, ev, s_err);
-  }
-  __shared__ T sh[2][kLossThreads];
-  sh[0][threadIdx.x] = s_aq;
-  sh[1][threadIdx.x] = s_err;
-  __syncthreads();
-  for (int w = kLossThreads / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-      sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
-      sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    part[((int64_t)k * gridDim.x + blockIdx.x) * 2 + 0] = sh[0][0];
-    part[((int64_t)k * gridDim.x + blockIdx.x) * 2 + 1] = sh[1][0];
-  }
-}
-
-// c_k = 1 / (K ||A q_k||^2); loss = sum c_k ||err_k||^2 (one thread).
-template <typename T>
-__global__ void k_loss_final(int K, int nb, const T* __restrict__ part, T* __restrict__ ck, double* __restrict__ loss) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double L = 0.0;
-  for (int k = 0; k < K; ++k) {
-    T aq = T(0), er = T(0);
-    for (int b = 0; b < nb; ++b) {
-      aq += part[((int64_t)k * nb + b) * 2 + 0];
-      er += part[((int64_t)k * nb + b) * 2 + 1];
-    }
-    const T c = T(1) / (T(K) * aq);
-    ck[k] = c;
-    L += double(c * er);
-  }
-  *loss = L;
-}
-
-// gy = gw + Lstrict^T gw with gw = 2 c_k err (column gather over the lower blocks)
-template <typename T>
-__global__ void k_loss_gy(Graph g, int bs, int K, const double* __restrict__ F0, const double* __restrict__ dF,
-                          const T* __restrict__ ck, const T* __restrict__ err, T* __restrict__ gy) {
-  const int64_t N = (int64_t)g.n * bs;
-  const int b2 = bs * bs;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N * K; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e / N);
-    const int64_t lj = e % N;
-    const int j = (int)(lj / bs), c = (int)(lj % bs);
-    const T* ek = err + (int64_t)k * N;
-    const T two_c = T(2) * ck[k];
-    T acc = two_c * ek[lj];
-    for (int t = g.lt_ptr[j]; t < g.lt_ptr[j + 1]; ++t) {
-      const int i = g.lt_row[t];
-      const int64_t o = (int64_t)g.lt_blk[t] * b2;
-      for (int r = 0; r < bs; ++r)
-        acc = fma(T(F0[o + r * bs + c] + dF[o + r * bs + c]), two_c * ek[(int64_t)i * bs + r], acc);
-    }
-    gy[e] = acc;
-  }
-}
-
-// gF[b] for every block: lower (j < i): sum_k gw_k[i] y_k[j]^T; else sum_k gy_k[i] q_k[j]^T
-template <typename T>
-__global__ void k_loss_gF(Graph g, int bs, int K, const T* __restrict__ ck, const T* __restrict__ err,
-                          const T* __restrict__ y, const T* __restrict__ gy, const T* __restrict__ q,
-                          T* __restrict__ gF) {
-  const int64_t N = (int64_t)g.n * bs;
-  const int b2 = bs * bs;
+__global__ void k_factor_grad(int n, int bs, int K, int64_t N, const int* __restrict__ fptr,
+                              const int* __restrict__ fcol, const int* __restrict__ fdiag,
+                              const int64_t* __restrict__ perm, const double* __restrict__ lam,
+                              const double* __restrict__ y, const double* __restrict__ w,
+                              const double* __restrict__ z, T* __restrict__ gdF) {
   const int lane = threadIdx.x & 31;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < g.n; i += (gridDim.x * blockDim.x) >> 5) {
-    for (int b = g.row_ptr[i]; b < g.row_ptr[i + 1]; ++b) {
-      const int j = g.col_idx[b];
-      const bool lower = j < i;
+  const int b2 = bs * bs;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
+    for (int b = fptr[i]; b < fptr[i + 1]; ++b) {
+      const int j = fcol[b];
+      const bool lower = b < fdiag[i];
+      const double* left = lower ? lam : w;
+      const double* right = lower ? y : z;
       for (int e = lane; e < b2; e += 32) {
         const int r = e / bs, c = e % bs;
-        T acc = T(0);
-        for (int k = 0; k < K; ++k) {
-          const int64_t base = (int64_t)k * N;
-          const T left = lower ? T(2) * ck[k] * err[base + (int64_t)i * bs + r] : gy[base + (int64_t)i * bs + r];
-          const T right = lower ? y[base + (int64_t)j * bs + c] : q[base + (int64_t)j * bs + c];
-          acc = fma(left, right, acc);
-        }
-        gF[(int64_t)b * b2 + e] = acc;
+        double acc = 0.0;
+        for (int k = 0; k < K; ++k)
+          acc = fma(left[(int64_t)k * N + (int64_t)i * bs + r], right[(int64_t)k * N + (int64_t)j * bs + c], acc);
+        gdF[perm[b] * b2 + e] = T(-acc);
       }
     }
   }
@@ -558,6 +487,10 @@ __global__ void k_normalize(int64_t n, const double* __restrict__ v, const doubl
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     q[i] = v[i] * s;
 }
+__global__ void k_sub_one(int64_t n, const double* __restrict__ t, double* __restrict__ v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] -= t[i];
+}
 __global__ void k_sub_proj(int64_t n, const double* __restrict__ a, const double* __restrict__ x,
                            double* __restrict__ y) {
   const double s = -*a;
@@ -581,7 +514,7 @@ struct ParamSlot {
 
 struct GraphBuf {
   const bsp_matrix_s* A = nullptr;
-  DevBuf<int> diag_pos, e_blk, e_row, e_col, er_ptr, ec_ptr, ec_idx, lt_ptr, lt_row, lt_blk;
+  DevBuf<int> diag_pos, e_blk, e_row, e_col, er_ptr, ec_ptr, ec_idx;
   int n = 0, E = 0;
   Graph view() const {
     Graph g{};
@@ -597,9 +530,6 @@ struct GraphBuf {
     g.er_ptr = er_ptr.get();
     g.ec_ptr = ec_ptr.get();
     g.ec_idx = ec_idx.get();
-    g.lt_ptr = lt_ptr.get();
-    g.lt_row = lt_row.get();
-    g.lt_blk = lt_blk.get();
     return g;
   }
 };
@@ -640,22 +570,6 @@ int build_graph(const bsp_matrix_s* A, GraphBuf& G) {
     std::vector<int> fill(ecp.begin(), ecp.end() - 1);
     for (int k = 0; k < E; ++k) eci[fill[ec[k]]++] = k;
   }
-  // strictly-lower blocks by column
-  std::vector<int> ltp(n + 1, 0), ltr, ltb;
-  for (int k = 0; k < E; ++k)
-    if (ec[k] < er[k]) ltp[ec[k] + 1]++;
-  for (int j = 0; j < n; ++j) ltp[j + 1] += ltp[j];
-  ltr.resize(ltp[n]);
-  ltb.resize(ltp[n]);
-  {
-    std::vector<int> fill(ltp.begin(), ltp.end() - 1);
-    for (int k = 0; k < E; ++k)
-      if (ec[k] < er[k]) {
-        const int t = fill[ec[k]]++;
-        ltr[t] = er[k];
-        ltb[t] = eb[k];
-      }
-  }
   G.A = A;
   G.n = n;
   G.E = E;
@@ -666,17 +580,14 @@ int build_graph(const bsp_matrix_s* A, GraphBuf& G) {
   BSP_TRY(upload_vec(G.er_ptr, erp));
   BSP_TRY(upload_vec(G.ec_ptr, ecp));
   BSP_TRY(upload_vec(G.ec_idx, eci));
-  BSP_TRY(upload_vec(G.lt_ptr, ltp));
-  BSP_TRY(upload_vec(G.lt_row, ltr));
-  BSP_TRY(upload_vec(G.lt_blk, ltb));
   return BSP_OK;
 }
 
 struct ModelBase {
   virtual ~ModelBase() = default;
   virtual int forward(bsp_handle_s* h, const bsp_matrix_s* A, double* dF) = 0;
-  virtual int loss_grad(bsp_handle_s* h, const bsp_matrix_s* A, const double* F0, int K, const double* probes,
-                        double* loss) = 0;
+  virtual int loss_grad(bsp_handle_s* h, const bsp_matrix_s* A, const bsp_precond_s* ilu, int K,
+                        const double* probes, double* loss) = 0;
   virtual int adam(bsp_handle_s* h, double lr, double b1, double b2, double eps) = 0;
   virtual int get(double* out, int64_t cnt, int which) = 0;
   virtual int set(const double* in, int64_t cnt) = 0;
@@ -763,8 +674,8 @@ template <typename T> struct Model : ModelBase {
   int64_t cached_nnzb = -1;
   DevBuf<T> s, x, a, e, hs, msgs, ms, us;   // hs: (L+1) n H; msgs: L E H; ms, us: L n H
   DevBuf<T> dh, dh2, dm, gdr, gdc, de, gmh, gdF;
-  DevBuf<T> q, y, err, gy, lpart, ck;
-  DevBuf<double> dF, dloss;
+  DevBuf<double> dF, lz, lw, llam, ly, lu, le, lsc;
+  std::unique_ptr<bsp_precond_s> work;   // learned LU of the cached matrix (ILU0 structure)
 
   explicit Model(bsp_learned_s* mm) : M(mm) {}
 
@@ -837,34 +748,51 @@ template <typename T> struct Model : ModelBase {
 
   int forward(bsp_handle_s* h, const bsp_matrix_s* A, double* out) override { return run_forward(h, A, out); }
 
-  int loss_grad(bsp_handle_s* h, const bsp_matrix_s* A, const double* F0, int K, const double* probes,
+  int loss_grad(bsp_handle_s* h, const bsp_matrix_s* A, const bsp_precond_s* ilu, int K, const double* probes,
                 double* loss_out) override {
     BSP_TRY(run_forward(h, A, nullptr));
-    const Graph gr = G.view();
     const int n = G.n, E = G.E, Es = std::max(E, 1), bs = 8;
     const int64_t N = (int64_t)n * bs;
-    BSP_TRY(ensure(q, N * K));
-    BSP_TRY(ensure(y, N * K));
-    BSP_TRY(ensure(err, N * K));
-    BSP_TRY(ensure(gy, N * K));
-    BSP_TRY(ensure(ck, K));
+    if (!work || work->A != A || work->n != n || work->f_nnzb != ilu->f_nnzb) {
+      work = std::make_unique<bsp_precond_s>();
+      work->h = h;
+      work->device = h->device;
+      work->A = const_cast<bsp_matrix_s*>(A);
+      work->kind = BSP_PC_LEARNED_LU;
+      work->n = n;
+      work->bs = bs;
+      work->precision = BSP_PREC_F64;
+      BSP_TRY(precond_learned_init(work.get()));
+    }
+    BSP_TRY(precond_learned_refresh(work.get(), ilu, dF.get()));
+    for (DevBuf<double>* b : {&lz, &lw, &llam, &ly}) BSP_TRY(ensure(*b, (size_t)N * K));
+    BSP_TRY(ensure(lu, (size_t)N));
+    BSP_TRY(ensure(le, (size_t)N));
+    BSP_TRY(ensure(lsc, (size_t)K));
     BSP_TRY(ensure(gdF, (size_t)A->nnzb * kB2));
     for (DevBuf<T>* b : {&dh, &dh2, &dm}) BSP_TRY(ensure(*b, (size_t)n * H));
     for (DevBuf<T>* b : {&gdr, &gdc, &de, &gmh}) BSP_TRY(ensure(*b, (size_t)Es * H));
-    BSP_TRY(ensure(dloss, 1));
-    const int lgrid = kB200SMs * 2;
-    BSP_TRY(ensure(lpart, (size_t)K * lgrid * 2));
-    const int eg = grid_for(h, N * K, 256);
-    bsp::count_launch(), k_cast<T><<<eg, 256, 0, h->stream>>>(N * K, probes, q.get());
-    bsp::count_launch(), k_loss_upper<T><<<eg, 256, 0, h->stream>>>(gr, bs, K, F0, dF.get(), q.get(), y.get());
-    bsp::count_launch(), k_loss_lower<T><<<dim3(lgrid, K), kLossThreads, 0, h->stream>>>(
-        gr, bs, K, F0, dF.get(), A->vals.get(), q.get(), y.get(), err.get(), lpart.get());
-    bsp::count_launch(), k_loss_final<T><<<1, 32, 0, h->stream>>>(K, lgrid, lpart.get(), ck.get(), dloss.get());
-    bsp::count_launch(), k_loss_gy<T><<<eg, 256, 0, h->stream>>>(gr, bs, K, F0, dF.get(), ck.get(), err.get(), gy.get());
+    const int eg = grid_for(h, N, 256);
+    bsp_matrix_s* Am = const_cast<bsp_matrix_s*>(A);
+    for (int k = 0; k < K; ++k) {
+      const double* q = probes + (int64_t)k * N;
+      double* z = lz.get() + (int64_t)k * N;
+      BSP_TRY(bsmv_launch(Am, 1, 0, BSP_F64, 1.0, q, 0.0, nullptr, lu.get(), h->stream));
+      BSP_TRY(precond_apply(work.get(), BSP_PREC_F64, lu.get(), z));
+      bsp::count_launch(), k_diff<<<eg, 256, 0, h->stream>>>(N, z, q, le.get());
+      BSP_TRY(bsp_dot_dev(h, N, le.get(), le.get(), lsc.get() + k));
+      bsp::count_launch(), k_scale<<<eg, 256, 0, h->stream>>>(N, 2.0 / K, le.get());
+      BSP_TRY(precond_apply_transposed(work.get(), le.get(), lw.get() + (int64_t)k * N, llam.get() + (int64_t)k * N));
+      bsp::count_launch(), k_upper_prod<<<eg, 256, 0, h->stream>>>(n, bs, work->f_ptr.get(), work->f_col.get(),
+                                                                   work->f_diag.get(), work->f_vals.get(), z,
+                                                                   ly.get() + (int64_t)k * N);
+    }
     const int ng = (int)std::min<int64_t>(ceil_div((int64_t)n * 32, 256), (int64_t)h->num_sms * 16);
-    bsp::count_launch(), k_loss_gF<T><<<ng, 256, 0, h->stream>>>(gr, bs, K, ck.get(), err.get(), y.get(), gy.get(),
-                                                                q.get(), gdF.get());
+    bsp::count_launch(), k_factor_grad<T><<<ng, 256, 0, h->stream>>>(n, bs, K, N, work->f_ptr.get(), work->f_col.get(),
+                                                                    work->f_diag.get(), work->d_perm.get(), llam.get(),
+                                                                    ly.get(), lw.get(), lz.get(), gdF.get());
     BSP_CUDA_TRY(cudaPeekAtLastError());
+    const Graph gr = G.view();
     // network backward: decoders
     const T* hL = hs.get() + (size_t)kLayers * n * H;
     const int so = 2 + 2 * kLayers;
@@ -905,8 +833,13 @@ template <typename T> struct Model : ModelBase {
     else
       BSP_CUDA_TRY(cudaMemsetAsync(Gp(1), 0, (size_t)(H * kB2 + H) * sizeof(T), h->stream));
     BSP_TRY((run_wgrad<T, kB2 + 1, H>(h, n, GMask<T>{dcur, hs.get()}, RowIn<T, kB2 + 1>{x.get()}, part.get(), Gp(0))));
-    BSP_CUDA_TRY(cudaMemcpyAsync(loss_out, dloss.get(), sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double> lk(K);
+    BSP_CUDA_TRY(cudaMemcpyAsync(lk.data(), lsc.get(), K * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    double L = 0.0;
+    for (int k = 0; k < K; ++k) L += lk[k];
+    *loss_out = L / K;
+    BSP_TRY(precond_check_status(work.get()));
     return BSP_OK;
   }
 
@@ -938,12 +871,6 @@ template <typename T> struct Model : ModelBase {
 };
 
 }  // namespace
-
-namespace bsp {
-int bsmv_launch(bsp_matrix_s* A, int nrhs, int transpose, int dtype, double alpha, const void* x, double beta,
-                const void* z, void* y, cudaStream_t s);
-int precond_build_learned(bsp_precond_s* pc, const double* dF);
-}  // namespace bsp
 
 // ================================================================= C ABI
 extern "C" {
@@ -1025,12 +952,13 @@ int bsp_learned_ilu_factors(bsp_handle_t h, bsp_precond_t ilu, double* F0) {
   return BSP_OK;
 }
 
-int bsp_learned_loss_grad(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, const double* F0, int n_probes,
+int bsp_learned_loss_grad(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, bsp_precond_t ilu, int n_probes,
                           const double* probes, double* loss) {
-  if (!h || !M || !A || !F0 || !probes || !loss || n_probes < 1 || n_probes > 65535 || A->bs != M->bs)
+  if (!h || !M || !A || !ilu || !probes || !loss || n_probes < 1 || A->bs != M->bs || ilu->A != A ||
+      ilu->kind != BSP_PC_ILU0)
     return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
-  return M->impl->loss_grad(h, A, F0, n_probes, probes, loss);
+  return M->impl->loss_grad(h, A, ilu, n_probes, probes, loss);
 }
 
 int bsp_learned_adam_step(bsp_handle_t h, bsp_learned_t M, double lr, double beta1, double beta2, double eps) {
@@ -1061,6 +989,34 @@ int bsp_learned_probes(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const d
     }
     BSP_TRY(bsp_dot_dev(h, N, v.get(), v.get(), sc.get() + 1));
     bsp::count_launch(), k_normalize<<<g, 256, 0, h->stream>>>(N, v.get(), sc.get() + 1, probes + (int64_t)j * N);
+  }
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return BSP_OK;
+}
+
+int bsp_learned_smooth(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int K, int steps, double* vecs) {
+  if (!h || !A || !pc || !vecs || K < 1 || steps < 0) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  const int64_t N = (int64_t)A->n_rows * A->bs;
+  DevBuf<double> t, sc;
+  BSP_TRY(t.alloc(N));
+  BSP_TRY(sc.alloc(2));
+  const int g = grid_for(h, N, 256);
+  for (int k = 0; k < K; ++k) {
+    double* v = vecs + (int64_t)k * N;
+    // e <- e - M^-1 A e: the error of the preconditioned stationary iteration
+    for (int s = 0; s < steps; ++s) {
+      BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, v, 0.0, nullptr, t.get(), h->stream));
+      BSP_TRY(precond_apply(pc, BSP_PREC_F64, t.get(), t.get()));
+      bsp::count_launch(), k_sub_one<<<g, 256, 0, h->stream>>>(N, t.get(), v);
+    }
+    for (int i = 0; i < k; ++i) {
+      BSP_TRY(bsp_dot_dev(h, N, vecs + (int64_t)i * N, v, sc.get()));
+      bsp::count_launch(), k_sub_proj<<<g, 256, 0, h->stream>>>(N, sc.get(), vecs + (int64_t)i * N, v);
+    }
+    BSP_TRY(bsp_dot_dev(h, N, v, v, sc.get() + 1));
+    bsp::count_launch(), k_normalize<<<g, 256, 0, h->stream>>>(N, v, sc.get() + 1, v);
   }
   BSP_CUDA_TRY(cudaPeekAtLastError());
   BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));

@@ -1180,6 +1180,145 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
   }
 }
 
+// Transposed structures and tasks for M^-T (LU-type factors).
+static int build_transposed(bsp_precond_s* pc) {
+  const bsp_matrix_s* A = pc->A;
+  const int n = A->n_rows;
+  // the factor's row-sorted structure (the order analyse_factor_structure uses)
+  std::vector<int> ptr(n + 1, 0), col;
+  col.reserve(A->nnzb);
+  std::vector<int> row;
+  for (int i = 0; i < n; ++i) {
+    row.assign(A->h_col_idx.begin() + A->h_row_ptr[i], A->h_col_idx.begin() + A->h_row_ptr[i + 1]);
+    std::sort(row.begin(), row.end());
+    col.insert(col.end(), row.begin(), row.end());
+    ptr[i + 1] = (int)col.size();
+  }
+  // per column: strictly-upper entries (rows i < j) and strictly-lower (rows j > i)
+  std::vector<std::vector<std::pair<int, int64_t>>> up(n), lo(n);
+  for (int i = 0; i < n; ++i)
+    for (int e = ptr[i]; e < ptr[i + 1]; ++e) {
+      const int j = col[e];
+      if (j > i) up[j].emplace_back(i, e);
+      else if (j < i) lo[j].emplace_back(i, e);
+    }
+  auto flatten = [&](const std::vector<std::vector<std::pair<int, int64_t>>>& lists, DevBuf<int>& dptr,
+                     DevBuf<int>& drow, DevBuf<int64_t>& dblk) -> int {
+    std::vector<int> p(n + 1, 0), r;
+    std::vector<int64_t> b;
+    for (int c = 0; c < n; ++c) {
+      for (auto& pr : lists[c]) {
+        r.push_back(pr.first);
+        b.push_back(pr.second);
+      }
+      p[c + 1] = (int)r.size();
+    }
+    if (r.empty()) {
+      r.push_back(0);
+      b.push_back(0);
+    }
+    BSP_TRY(upload(dptr, p));
+    BSP_TRY(upload(drow, r));
+    BSP_TRY(upload(dblk, b));
+    return BSP_OK;
+  };
+  BSP_TRY(flatten(up, pc->tu_ptr, pc->tu_row, pc->tu_blk));
+  BSP_TRY(flatten(lo, pc->tl_ptr, pc->tl_row, pc->tl_blk));
+  std::vector<int> order, trow, tlen;
+  auto up_deps = [&](int j, auto&& f) {
+    for (auto& pr : up[j]) f(pr.first);
+  };
+  auto lo_deps = [&](int i, auto&& f) {
+    for (auto& pr : lo[i]) f(pr.first);
+  };
+  level_order(n, true, up_deps, order);
+  BSP_TRY(upload(pc->order_tu, order));
+  pc->n_task_tu = build_tasks(n, true, up_deps, trow, tlen);
+  BSP_TRY(upload(pc->task_tu_row, trow));
+  BSP_TRY(upload(pc->task_tu_len, tlen));
+  level_order(n, false, lo_deps, order);
+  BSP_TRY(upload(pc->order_tl, order));
+  pc->n_task_tl = build_tasks(n, false, lo_deps, trow, tlen);
+  BSP_TRY(upload(pc->task_tl_row, trow));
+  BSP_TRY(upload(pc->task_tl_len, tlen));
+  pc->has_trans = true;
+  return BSP_OK;
+}
+
+// out = M^-T g = L^-T (U^-T g): a forward sweep over U's columns with the
+// transposed inverted diagonal, then a backward sweep over L's columns (unit
+// diagonal).  FP64; g, w and out must be distinct.
+int precond_apply_transposed(bsp_precond_s* pc, const double* g, double* w, double* out) {
+  if (pc->kind != BSP_PC_ILU0 && pc->kind != BSP_PC_LEARNED_LU) return BSP_INVALID;
+  if (!pc->has_trans) BSP_TRY(build_transposed(pc));
+  bsp_handle_s* h = pc->h;
+  const int n = pc->n, bs = pc->bs;
+  const int64_t nv = (int64_t)n * bs;
+  SweepP<double, double> p{};
+  p.n = n;
+  p.flags = pc->flags.get();
+  p.vals = pc->f_vals.get();
+  p.dinv = pc->dinv.get();
+  p.range = RANGE_ALL;
+  // U^T w = g, forward
+  p.ptr = pc->tu_ptr.get();
+  p.idx = pc->tu_row.get();
+  p.blk = pc->tu_blk.get();
+  p.order = pc->order_tu.get();
+  p.task_row = pc->task_tu_row.get();
+  p.task_len = pc->task_tu_len.get();
+  p.n_tasks = pc->n_task_tu;
+  p.task_dir = 1;
+  p.rhs = g;
+  p.x = w;
+  BSP_TRY(fill_sentinel(h, w, nv));
+  BSP_TRY((launch_sweep<double, double, true, POST_DT>(h, bs, p, pc->ticket.get())));
+  // L^T out = w, backward
+  p.ptr = pc->tl_ptr.get();
+  p.idx = pc->tl_row.get();
+  p.blk = pc->tl_blk.get();
+  p.order = pc->order_tl.get();
+  p.task_row = pc->task_tl_row.get();
+  p.task_len = pc->task_tl_len.get();
+  p.n_tasks = pc->n_task_tl;
+  p.task_dir = -1;
+  p.rhs = w;
+  p.x = out;
+  BSP_TRY(fill_sentinel(h, out, nv));
+  return launch_sweep<double, double, true, POST_NONE>(h, bs, p, pc->ticket.get());
+}
+
+__global__ void k_copy_add_perm(int64_t nblk, int b2, const int64_t* __restrict__ perm, const double* __restrict__ f0,
+                                const double* __restrict__ dF, double* __restrict__ f) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nblk * b2; e += (int64_t)gridDim.x * blockDim.x)
+    f[e] = f0[e] + dF[perm[e / b2] * b2 + e % b2];
+}
+
+// Structure of a learned-LU preconditioner whose factors are set by
+// precond_learned_refresh (no factorisation).
+int precond_learned_init(bsp_precond_s* pc) {
+  const int n = pc->n, b2 = pc->bs * pc->bs;
+  BSP_TRY(pc->dinv.alloc((size_t)std::max(n, 1) * b2));
+  BSP_TRY(pc->flags.alloc(std::max(n, 1)));
+  BSP_TRY(pc->ticket.alloc(1));
+  BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
+  return build_factor_structure(pc, false);
+}
+
+// work's factors = ilu's factors + dF (A order); work shares ilu's structure
+// (both built on the same matrix) and gets fresh diagonal inverses.
+int precond_learned_refresh(bsp_precond_s* work, const bsp_precond_s* ilu, const double* dF) {
+  if (work->f_nnzb != ilu->f_nnzb || work->n != ilu->n || work->bs != ilu->bs) return BSP_INVALID;
+  const int b2 = work->bs * work->bs;
+  const int64_t tot = work->f_nnzb * b2;
+  if (tot > 0)
+    bsp::count_launch(), k_copy_add_perm<<<grid_for(work->h, tot, 256), 256, 0, work->h->stream>>>(
+        work->f_nnzb, b2, work->d_perm.get(), ilu->f_vals.get(), dF, work->f_vals.get());
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return run_factor(work, FACT_DIAG, nullptr, work->f_ptr.get(), work->f_col.get(), work->f_diag.get(),
+                    work->f_vals.get(), work->n);
+}
+
 // z = M^{-1} r.  precision selects the stored factors (FP64 / FP32 / BF16);
 // vec64 selects FP64 vectors (the Krylov path, always FP64 accumulation) or
 // FP32 vectors (low-precision vectors, FP32 accumulation).

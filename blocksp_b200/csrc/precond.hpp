@@ -36,6 +36,14 @@ struct bsp_precond_s {
   // sync-free state
   bsp::DevBuf<int> flags;
   bsp::DevBuf<unsigned> ticket;
+  // transposed solves M^-T = L^-T U^-T of an LU-type factor (built on demand):
+  // tu lists, per column j, the strictly-upper blocks (i, j); tl, per column i,
+  // the strictly-lower blocks (j, i); each with its own chain tasks
+  bool has_trans = false;
+  bsp::DevBuf<int> tu_ptr, tu_row, tl_ptr, tl_row, order_tu, order_tl, task_tu_row, task_tu_len, task_tl_row,
+      task_tl_len;
+  bsp::DevBuf<int64_t> tu_blk, tl_blk;
+  int n_task_tu = 0, n_task_tl = 0;
   // apply scratch: sweep outputs (pre-filled with the sentinel), SOR ping-pong
   // iterates and the copy of an in-place right-hand side
   bsp::DevBuf<double> s64[3];
@@ -47,4 +55,10 @@ int grid_for(const bsp_handle_s* h, int64_t n, int threads);
 int precond_build(bsp_precond_s* pc);
 int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z);
 int precond_check_status(bsp_precond_s* pc);
+// out = M^-T g for an ILU0 / learned-LU preconditioner (FP64); w receives U^-T g.
+int precond_apply_transposed(bsp_precond_s* pc, const double* g, double* w, double* out);
+// learned LU: structure only (no factorisation), then
+// f = ilu's factors + dF (A's block order) with dinv recomputed
+int precond_learned_init(bsp_precond_s* pc);
+int precond_learned_refresh(bsp_precond_s* work, const bsp_precond_s* ilu, const double* dF);
 }  // namespace bsp

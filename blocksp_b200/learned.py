@@ -121,9 +121,11 @@ class LearnedModel:
               self.handle.h)
         return dF
 
-    def loss_grad(self, A: Matrix, F0, probes) -> float:
+    def loss_grad(self, A: Matrix, ilu: Precond, probes) -> float:
+        """loss = (1/K) sum_k ||M^-1 A q_k - q_k||^2 for M = the ILU0 factors of
+        ``ilu`` corrected by the network; keeps the parameter gradient."""
         loss = C.c_double()
-        check(self.handle.lib.bsp_learned_loss_grad(self.handle.h, self.m, A.m, _ptr(F0), int(probes.shape[0]),
+        check(self.handle.lib.bsp_learned_loss_grad(self.handle.h, self.m, A.m, ilu.p, int(probes.shape[0]),
                                                     _ptr(probes), C.byref(loss)), "bsp_learned_loss_grad",
               self.handle.h)
         return loss.value
@@ -169,6 +171,30 @@ def probes(A: Matrix, pc: Precond | None, b, K: int):
     return Q
 
 
+def smooth_probes(A: Matrix, pc: Precond, K: int, steps: int, seed: int = 0):
+    """K orthonormal smoothed error vectors: random vectors after `steps`
+    iterations of e <- e - M^-1 A e (the slow modes of the preconditioned
+    iteration, which dominate the Krylov solve's iteration count)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    V = torch.tensor(rng.standard_normal((K, A.n_rows * A.bs)), device="cuda")
+    check(A.handle.lib.bsp_learned_smooth(A.handle.h, A.m, pc.p, int(K), int(steps), _ptr(V)),
+          "bsp_learned_smooth", A.handle.h)
+    return V
+
+
+def training_probes(A: Matrix, ilu: Precond, b, n_arnoldi: int, n_smooth: int, smooth_steps: int, seed: int):
+    """Probe set of a training step: Arnoldi vectors of the ILU0-preconditioned
+    operator from M0^-1 b plus smoothed error vectors (each set orthonormal)."""
+    import torch
+    parts = []
+    if n_arnoldi:
+        parts.append(probes(A, ilu, b, n_arnoldi))
+    if n_smooth:
+        parts.append(smooth_probes(A, ilu, n_smooth, smooth_steps, seed))
+    return torch.cat(parts).contiguous()
+
+
 def LearnedLU(A: Matrix, model: LearnedModel | None, precision: int = _lib.PREC_F64) -> Precond:
     """The learned preconditioner, or block ILU0 when the model is absent or its
     validation showed no gain over ILU0's iteration count (the fallback)."""
@@ -189,7 +215,7 @@ def solve_iters(A: Matrix, b, pc, tol: float = 1e-10, restart: int = 30, k: int 
 
 def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, epochs: int = 1,
           n_probes: int = 16, lr: float = 1e-4, handle: Handle | None = None, seed: int = 0,
-          log=print) -> LearnedModel:
+          n_smooth: int = 8, smooth_steps: int = 20, log=print) -> LearnedModel:
     """Train on convection-diffusion systems (systems.convection_diffusion_system)
     with the GPU kernels; then validate against ILU0 on held-out seeds and
     record whether the model beats ILU0's iteration count (the fallback gate)."""
@@ -205,10 +231,10 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
             sysm = systems.convection_diffusion_system(dims, 8, int(s))
             A = Matrix.from_system(sysm, h)
             ilu = ILU0(A)
-            F0 = ilu_factors(A, ilu)
-            Q = probes(A, ilu, torch.tensor(sysm.b, device="cuda"), n_probes)
+            Q = training_probes(A, ilu, torch.tensor(sysm.b, device="cuda"), n_probes - n_smooth, n_smooth,
+                                smooth_steps, int(s))
             for _ in range(steps_per_system):
-                loss = model.loss_grad(A, F0, Q)
+                loss = model.loss_grad(A, ilu, Q)
                 model.adam_step(lr)
                 history.append(loss)
             ilu.close()
@@ -233,6 +259,7 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
     model.meta = {"bs": 8, "hidden": HIDDEN, "layers": LAYERS, "dims": list(dims),
                   "train_seeds": [int(s) for s in train_seeds], "val_seeds": [int(s) for s in val_seeds],
                   "steps_per_system": steps_per_system, "epochs": epochs, "n_probes": n_probes, "lr": lr,
+                  "n_smooth": n_smooth, "smooth_steps": smooth_steps,
                   "loss_first": history[0] if history else None, "loss_last": history[-1] if history else None,
                   "loss_history": history[:: max(1, len(history) // 200)], "validation": val,
                   "beats_ilu0": beats, "train_seconds": time.time() - t0}
@@ -249,10 +276,13 @@ if __name__ == "__main__":  # pragma: no cover - the training run itself
     ap.add_argument("--epochs", type=int, default=1)
     ap.add_argument("--probes", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-4)
+    ap.add_argument("--smooth", type=int, default=8)
+    ap.add_argument("--smooth-steps", type=int, default=20)
     ap.add_argument("--out", default=str(WEIGHTS))
     a = ap.parse_args()
     tr = [10_000 + i for i in range(a.train)]
     va = [20_000 + i for i in range(a.val)]
-    m = train(tr, va, (a.side,) * 3, a.steps, a.epochs, a.probes, a.lr)
+    m = train(tr, va, (a.side,) * 3, a.steps, a.epochs, a.probes, a.lr, n_smooth=a.smooth,
+              smooth_steps=a.smooth_steps)
     m.save(a.out)
     print(json.dumps({k: v for k, v in m.meta.items() if k != "loss_history"}))

@@ -298,8 +298,9 @@ int bsp_batch_results(bsp_batch_t B, int nrhs, int* iters, int* state, double* f
  * block-ILU0 factors; M = L U is stored in the ILU0 structures
  * (BSP_PC_LEARNED_LU) and applied by the same triangular sweeps.  The network
  * is trained on the GPU with this library's own forward/backward kernels on
- *   loss = (1/K) sum_k ||(L U - A) q_k||^2 / ||A q_k||^2,
- * q_k the Arnoldi vectors of the ILU0-preconditioned operator from M0^-1 b.
+ *   loss = (1/K) sum_k ||M^-1 A q_k - q_k||^2,
+ * q_k the orthonormal Arnoldi vectors of the ILU0-preconditioned operator
+ * from M0^-1 b (its gradient uses M^-1 and M^-T, both by triangular sweeps).
  * Parameters are packed per layer as W (out x in, row-major) then b, in the
  * order encoder-node, encoder-edge, (message, update) x 3, decoder-edge,
  * decoder-diagonal.  dtype BSP_F32 trains/infers in FP32, BSP_F64 in FP64. */
@@ -316,13 +317,18 @@ int bsp_learned_get_grads(bsp_learned_t M, double* grads, int64_t count);
 int bsp_learned_forward(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, double* dF);
 /* ILU0 factors of an ILU0 preconditioner in A's block order (device) */
 int bsp_learned_ilu_factors(bsp_handle_t h, bsp_precond_t ilu, double* F0);
-/* loss for F = F0 + dF and probes (device, K vectors of n*bs); keeps the gradient */
-int bsp_learned_loss_grad(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, const double* F0, int n_probes,
+/* loss for the factors of `ilu` (BSP_PC_ILU0 on A) plus dF, over probes
+ * (device, K orthonormal vectors of n*bs); keeps the parameter gradient */
+int bsp_learned_loss_grad(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, bsp_precond_t ilu, int n_probes,
                           const double* probes, double* loss);
 int bsp_learned_adam_step(bsp_handle_t h, bsp_learned_t M, double lr, double beta1, double beta2, double eps);
 /* K orthonormal Arnoldi vectors of M^-1 A from M^-1 b (device; pc may be NULL) */
 int bsp_learned_probes(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b, int K,
                        double* probes);
+/* In place on K device vectors (n*bs each): `steps` iterations of
+ * e <- e - M^-1 A e (the error of the preconditioned stationary iteration,
+ * which keeps the slow modes), then orthonormalisation. */
+int bsp_learned_smooth(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int K, int steps, double* vecs);
 /* Builds the learned preconditioner of A (ILU0 + network correction). */
 int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int precision, bsp_precond_t* out);
 

@@ -17,14 +17,22 @@ directed edge k = (i, j) per off-diagonal block A_ij, in CSR order):
     L layers:  msg_k = relu(Wm [h_j; e_k] + bm)
                m_i   = sum over edges k of row i of msg_k   (CSR order)
                h_i  <- h_i + relu(Wu [h_i; m_i] + bu)
-    dF_k  = alpha sqrt(s_i s_j) (Wo [h_i; h_j; e_k] + bo)   off-diagonal block
+    dF_k  = alpha c_k (Wo [h_i; h_j; e_k] + bo)             off-diagonal block
     dF_ii = alpha s_i (Wd h_i + bd)                         diagonal block
+with c_k = sqrt(s_i s_j) for an upper block (j > i, the scale of U_ij ~ A_ij)
+and c_k = sqrt(s_i / s_j) for a lower block (j < i, the scale of
+L_ij ~ A_ij U_jj^-1).
 The preconditioner is M = L U with L = unit lower + strict-lower blocks and U
 the upper blocks (diagonal included) of F = F_ILU0 + dF (A's pattern).
 
-Loss over probe vectors q_1..q_K (Krylov vectors of the ILU0-preconditioned
-operator, generated by the solver):
-    loss = (1/K) sum_k ||(L U - A) q_k||^2 / ||A q_k||^2
+Loss over orthonormal probe vectors q_1..q_K (Arnoldi vectors of the
+ILU0-preconditioned operator, generated by the solver): the distance of the
+left-preconditioned operator from the identity on them,
+    loss = (1/K) sum_k ||M^-1 A q_k - q_k||^2.
+With z = M^-1 A q, g = (2/K)(z - q), w = U^-T g, lam = L^-T w, y = U z:
+    d loss / d L_ij = -sum_k lam_k[i] y_k[j]^T  (strictly lower blocks)
+    d loss / d U_ij = -sum_k   w_k[i] z_k[j]^T  (upper blocks)
+Here written with dense matrices (small test systems only).
 """
 from __future__ import annotations
 
@@ -112,7 +120,8 @@ def forward(p: dict, g: Graph, vals: np.ndarray, L: int = 3):
         ms.append(m)
         us.append(u)
         hs.append(h)
-    se = ALPHA * np.sqrt(s[g.e_row] * s[g.e_col])
+    si, sj = s[g.e_row], s[g.e_col]
+    se = ALPHA * np.where(g.e_col < g.e_row, np.sqrt(si / sj), np.sqrt(si * sj))
     din = np.concatenate([h[g.e_row], h[g.e_col], e], axis=1)
     dF = np.zeros((len(g.col_idx), bs * bs))
     dF[g.e_blk] = se[:, None] * (din @ p["Wo"].T + p["bo"])
@@ -121,51 +130,46 @@ def forward(p: dict, g: Graph, vals: np.ndarray, L: int = 3):
     return dF.reshape(-1, bs, bs), cache
 
 
-def lu_apply(g: Graph, F: np.ndarray, q: np.ndarray):
-    """(L U) q with L unit lower (strict-lower blocks of F), U the upper blocks;
-    returns (L U q, U q)."""
+def dense_of(g: Graph, blocks: np.ndarray) -> np.ndarray:
+    n, bs = g.n, blocks.shape[1]
+    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
+    D = np.zeros((n * bs, n * bs))
+    for b, (i, j) in enumerate(zip(rows, g.col_idx)):
+        D[i * bs:(i + 1) * bs, j * bs:(j + 1) * bs] = blocks[b]
+    return D
+
+
+def lu_dense(g: Graph, F: np.ndarray):
+    """L (unit lower, strict-lower blocks of F) and U (upper blocks of F)."""
     n, bs = g.n, F.shape[1]
     rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
-    qb = q.reshape(n, bs)
-    up = g.col_idx >= rows
-    y = np.zeros((n, bs))
-    np.add.at(y, rows[up], np.einsum("kab,kb->ka", F[up], qb[g.col_idx[up]]))
-    lo = ~up
-    w = y.copy()
-    np.add.at(w, rows[lo], np.einsum("kab,kb->ka", F[lo], y[g.col_idx[lo]]))
-    return w.ravel(), y.ravel()
-
-
-def bsr_apply(g: Graph, vals: np.ndarray, q: np.ndarray) -> np.ndarray:
-    n, bs = g.n, vals.shape[1]
-    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
-    out = np.zeros((n, bs))
-    np.add.at(out, rows, np.einsum("kab,kb->ka", vals, q.reshape(n, bs)[g.col_idx]))
-    return out.ravel()
+    lower = g.col_idx < rows
+    Fl = np.where(lower[:, None, None], F, 0.0)
+    Fu = np.where(lower[:, None, None], 0.0, F)
+    return np.eye(n * bs) + dense_of(g, Fl), dense_of(g, Fu)
 
 
 def loss_and_factor_grad(g: Graph, vals: np.ndarray, F: np.ndarray, Q: np.ndarray):
     """loss and d loss / d F (nnzb, bs, bs) for probes Q (K, n*bs)."""
     n, bs = g.n, vals.shape[1]
     rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
-    up = g.col_idx >= rows
-    lo = ~up
     K = Q.shape[0]
-    loss = 0.0
+    A = dense_of(g, vals)
+    L, U = lu_dense(g, F)
+    Z = np.linalg.solve(L @ U, A @ Q.T)          # (N, K)
+    E = Z - Q.T
+    loss = float(np.sum(E * E)) / K
+    G = 2.0 * E / K
+    W = np.linalg.solve(U.T, G)
+    Lam = np.linalg.solve(L.T, W)
+    Y = U @ Z
     gF = np.zeros_like(F)
-    for q in Q:
-        Aq = bsr_apply(g, vals, q)
-        w, y = lu_apply(g, F, q)
-        err = w - Aq
-        c = 1.0 / (K * float(Aq @ Aq))
-        loss += c * float(err @ err)
-        gw = (2.0 * c * err).reshape(n, bs)
-        yb = y.reshape(n, bs)
-        gF[lo] += np.einsum("ka,kb->kab", gw[rows[lo]], yb[g.col_idx[lo]])
-        gy = gw.copy()
-        np.add.at(gy, g.col_idx[lo], np.einsum("kab,ka->kb", F[lo], gw[rows[lo]]))
-        qb = q.reshape(n, bs)
-        gF[up] += np.einsum("ka,kb->kab", gy[rows[up]], qb[g.col_idx[up]])
+    for b, (i, j) in enumerate(zip(rows, g.col_idx)):
+        si, sj = slice(i * bs, (i + 1) * bs), slice(j * bs, (j + 1) * bs)
+        if j < i:
+            gF[b] = -Lam[si] @ Y[sj].T
+        else:
+            gF[b] = -W[si] @ Z[sj].T
     return loss, gF
 
 

@@ -2,8 +2,9 @@
 
 * forward correction dF: FP64 kernels within 1e-12 relative of the oracle,
   FP32 kernels within 1e-4;
-* loss and every parameter gradient: FP64 within 1e-10 relative (per
-  parameter tensor, max-norm), FP32 within 2e-3;
+* loss (1/K) sum ||M^-1 A q - q||^2 and every parameter gradient: FP64 within
+  1e-9 relative (per parameter tensor, max-norm), FP32 network within 2e-3
+  (the triangular solves of the loss are FP64 in both);
 * probes: orthonormal Arnoldi vectors of the ILU0-preconditioned operator,
   equal to the oracle's Arnoldi process within 1e-9;
 * zero decoders reproduce block ILU0 bit for bit;
@@ -35,8 +36,8 @@ def case(handle):
     g = LO.graph_of(s.row_ptr, s.col_idx)
     rng = np.random.default_rng(5)
     p = LO.init_params(8, seed=9)
-    for k in p:
-        p[k] = p[k] + 0.05 * rng.standard_normal(p[k].shape)
+    for k in p:  # small decoders keep M = LU well conditioned
+        p[k] = p[k] + (0.005 if k in ("Wo", "bo", "Wd", "bd") else 0.05) * rng.standard_normal(p[k].shape)
     yield s, A, Ao, ilu_o, g, p
     A.close()
 
@@ -51,7 +52,7 @@ def test_forward_matches_oracle(handle, case, dtype, tol):
     m.close()
 
 
-@pytest.mark.parametrize("dtype,ltol,gtol", [(_lib.BSP_F64, 1e-11, 1e-10), (_lib.BSP_F32, 1e-4, 2e-3)])
+@pytest.mark.parametrize("dtype,ltol,gtol", [(_lib.BSP_F64, 1e-10, 1e-9), (_lib.BSP_F32, 1e-4, 2e-3)])
 def test_loss_and_gradients_match_oracle(handle, case, torch_cuda, dtype, ltol, gtol):
     torch = torch_cuda
     s, A, _, ilu_o, g, p = case
@@ -60,10 +61,10 @@ def test_loss_and_gradients_match_oracle(handle, case, torch_cuda, dtype, ltol, 
     F0 = learned.ilu_factors(A, ilu)
     assert rel(F0.cpu().numpy(), ilu_o.LU.vals) <= 1e-13
     rng = np.random.default_rng(6)
-    Qh = rng.standard_normal((3, s.n * 8))
+    Qh = np.linalg.qr(rng.standard_normal((s.n * 8, 3)))[0].T.copy()
     Q = torch.tensor(Qh, device="cuda")
     m = learned.LearnedModel(handle, 8, dtype, params=p)
-    loss = m.loss_grad(A, F0, Q)
+    loss = m.loss_grad(A, ilu, Q)
     ref_loss, ref_g = LO.loss_and_grads(p, g, s.vals, F0.cpu().numpy(), Qh)
     assert abs(loss - ref_loss) <= ltol * abs(ref_loss)
     gr = m.grads()
@@ -119,12 +120,11 @@ def test_training_lowers_the_loss(handle, torch_cuda):
     s = systems.convection_diffusion_system((12, 12, 12), 8, 41)
     A = bsp.Matrix.from_system(s, handle)
     ilu = bsp.ILU0(A)
-    F0 = learned.ilu_factors(A, ilu)
     Q = learned.probes(A, ilu, s.b, 8)
     m = learned.LearnedModel(handle, 8, _lib.BSP_F32)
     losses = []
     for _ in range(30):
-        losses.append(m.loss_grad(A, F0, Q))
+        losses.append(m.loss_grad(A, ilu, Q))
         m.adam_step(1e-4)
     assert losses[-1] < losses[0], losses
     # the trained correction is applied by the same sweeps and still solves

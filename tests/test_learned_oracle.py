@@ -26,9 +26,9 @@ def test_oracle_gradients_match_finite_differences():
     s, g, F0 = small_case()
     rng = np.random.default_rng(1)
     p = LO.init_params(8, seed=3)
-    for k in p:
-        p[k] = p[k] + 0.05 * rng.standard_normal(p[k].shape)
-    Q = rng.standard_normal((3, s.n * 8))
+    for k in p:  # small decoders keep M = LU well conditioned
+        p[k] = p[k] + (0.005 if k in ("Wo", "bo", "Wd", "bd") else 0.05) * rng.standard_normal(p[k].shape)
+    Q = np.linalg.qr(rng.standard_normal((s.n * 8, 3)))[0].T
     _, gr = LO.loss_and_grads(p, g, s.vals, F0, Q)
     worst = 0.0
     for name in p:
@@ -46,10 +46,10 @@ def test_zero_decoders_give_ilu0():
     dF, _ = LO.forward(p, g, s.vals)
     assert not np.any(dF)
     rng = np.random.default_rng(2)
-    Q = rng.standard_normal((2, s.n * 8))
+    Q = np.linalg.qr(rng.standard_normal((s.n * 8, 2)))[0].T
     loss, _ = LO.loss_and_factor_grad(g, s.vals, F0, Q)
-    # ILU0's product matches A on the pattern, so the loss only sees fill-in
-    assert 0.0 < loss < 1.0
+    # ILU0's M^-1 A differs from I only through the dropped fill-in
+    assert 0.0 < loss < 2.0
 
 
 def test_host_parameter_layout_matches_oracle():
