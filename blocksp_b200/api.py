@@ -33,13 +33,34 @@ def _ptr(a) -> int | None:
 class Handle:
     """A device + stream context (one per CUDA stream, not thread-safe)."""
 
+    # cudaStreamLegacy: the legacy default stream, torch's default stream
+    LEGACY_STREAM = 1
+
     def __init__(self, device: int = 0, stream: int | None = None):
+        """stream: a CUDA stream handle (e.g. ``torch.cuda.Stream().cuda_stream``).
+        By default the handle runs on torch's current stream of ``device``, so
+        calls on torch tensors are ordered with the caller's torch work (a
+        private stream would let torch read a tensor the library is still
+        writing)."""
         self.lib = _lib.load()
+        if stream is None:
+            stream = self._torch_stream(device)
         h = C.c_void_p()
         check(self.lib.bsp_handle_create(device, stream, C.byref(h)), "bsp_handle_create")
         self.h = h
         self.device = device
         self._children = weakref.WeakSet()  # objects that must be released first
+
+    @classmethod
+    def _torch_stream(cls, device: int) -> int | None:
+        try:
+            import torch
+            if not torch.cuda.is_available():
+                return None
+            s = torch.cuda.current_stream(device).cuda_stream
+            return s if s else cls.LEGACY_STREAM
+        except Exception:
+            return None
 
     def adopt(self, obj) -> None:
         self._children.add(obj)
