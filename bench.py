@@ -447,6 +447,148 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- mixed / learned workloads
+
+def _solve_variant(bsp, _lib, A, b, stream, make_pc, precision):
+    """One timed solve: preconditioner set-up + refined pGMRES(30, k=10) to the
+    FP64 true relative residual 1e-10."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pc = make_pc()
+    e1.record(stream)
+    x, info, _ = bsp.pGMRES(A, b, TOL, pc, 20000, 30, 10, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL,
+                            precision=precision, inner_tol=1e-6)
+    e2.record(stream)
+    e2.synchronize()
+    kind = pc.kind
+    pc.close()
+    return x, {"setup_s": e0.elapsed_time(e1) / 1e3, "solve_s": e1.elapsed_time(e2) / 1e3,
+               "total_s": e0.elapsed_time(e2) / 1e3, "iters": info["iters"], "refinements": info["n_outer"],
+               "true_rel_res": info["true_rel_res"], "status": info["status"], "precond_kind": kind}
+
+
+def reference_x(s, B, D, budget_s=900.0):
+    """The reference's own FP64 solve (ILU0_pGMRES(30, 10) to 1e-10, the build
+    without fast-math) of system s on this host, for solution errors."""
+    exe = ROOT / "oracle" / "_ref" / "ref_solve_hist"
+    if not exe.exists():
+        return None, None
+    from blocksp_b200 import systems
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "sys.bsps"
+        xo = Path(d) / "x.vec"
+        systems.write_bsr(f, s)
+        cmd = [str(exe), str(f), "--B", str(B), "--D", str(D), "--solver", "ilu0_pgmres", "--tol", "1e-10",
+               "--maxit", "20000", "--restart", "30", "--k", "10", "--x", str(xo), "--time"]
+        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+        t0 = time.time()
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=budget_s)
+        el = time.time() - t0
+        if r.returncode != 0 or not xo.exists():
+            return None, el
+        raw = xo.read_bytes()
+        return np.frombuffer(raw[8:], dtype="<f8").copy(), el
+
+
+def run_mixed(args):
+    """cfg2: the 64^3 bs-8 system and the 48^3 bs-16 system, pGMRES-DR + ILU0 to
+    the FP64 true residual 1e-10 with the inner work in FP64, FP32 storage or
+    BF16 storage (FP64 vectors, refinement, Arnoldi and least squares), and each
+    result's relative error against the reference's FP64 CPU solution."""
+    import torch
+    import blocksp_b200 as bsp
+    from blocksp_b200 import _lib, systems
+    stream = torch.cuda.Stream()
+    h = bsp.Handle(0, stream=stream.cuda_stream)
+    out = {}
+    with ClockSampler(0) as clk:
+        for name, s, B, D in (("3d64_bs8", systems.config1(seed=1, side=64), 4, 2),
+                              ("3d48_bs16", systems.config2b(seed=2, side=48), 8, 2)):
+            A = bsp.Matrix.from_system(s, h)
+            b = torch.tensor(s.b, device="cuda")
+            res = {}
+            xs = {}
+            for vname, prec in (("f64", _lib.PREC_F64), ("f32_storage", _lib.PREC_F32),
+                                ("bf16_storage", _lib.PREC_BF16)):
+                for _ in range(max(args.warmup, 1)):
+                    _solve_variant(bsp, _lib, A, b, stream, lambda: bsp.ILU0(A), prec)
+                runs = [_solve_variant(bsp, _lib, A, b, stream, lambda: bsp.ILU0(A), prec) for _ in range(args.steps)]
+                xs[vname] = runs[-1][0].cpu().numpy()
+                r = runs[-1][1]
+                r["total_s"] = statistics.mean(v[1]["total_s"] for v in runs)
+                res[vname] = r
+            xref, ref_s = (reference_x(s, B, D) if not args.no_cpu_baseline else (None, None))
+            for vname in res:
+                res[vname]["rel_err_vs_gpu_f64"] = float(np.abs(xs[vname] - xs["f64"]).max() /
+                                                         np.abs(xs["f64"]).max())
+                if xref is not None:
+                    res[vname]["rel_err_vs_reference_f64"] = float(np.abs(xs[vname] - xref).max() /
+                                                                   np.abs(xref).max())
+            out[name] = {"n_block_rows": s.n, "bs": s.bs, "nnzb": s.nnzb, "variants": res,
+                         "reference_solve_wall_s": ref_s}
+            A.close()
+    best = min(out["3d64_bs8"]["variants"].items(), key=lambda kv: kv[1]["total_s"])
+    line = {"metric": "mixed precision: time to FP64 true relative residual 1e-10 (pGMRES-DR + ILU0)",
+            "value": best[1]["total_s"], "unit": "s", "higher_is_better": False, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "dtype": "f64 outer / f32 or bf16 inner storage",
+            "data": "synthetic (seeded 3D 7-point block stencils)", "vs_baseline": None,
+            "config": {"workload": "cfg2: 64^3 8x8 and 48^3 16x16 block systems, skew 0.3",
+                       "best_variant_3d64": best[0]},
+            "systems": out, "clocks": clk.summary()}
+    h.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_learned(args):
+    """cfg4 ablation: held-out 3D convection-diffusion systems (8x8 blocks,
+    log-normal conductivity, random velocity) at side^3, pGMRES(30, k=10) to the
+    FP64 true residual 1e-10 with block ILU0, with the trained network's
+    factors (forced), and with LearnedLU (the learned factors only when the
+    model's validation beat ILU0, else ILU0), in FP64 and with FP32 storage."""
+    import torch
+    import blocksp_b200 as bsp
+    from blocksp_b200 import _lib, learned, systems
+    stream = torch.cuda.Stream()
+    h = bsp.Handle(0, stream=stream.cuda_stream)
+    model = learned.LearnedModel.load(handle=h)
+    seeds = [30000 + i for i in range(args.learned_seeds)]
+    dims = (args.learned_side,) * 3
+    per = []
+    with ClockSampler(0) as clk:
+        for sd in seeds:
+            s = systems.convection_diffusion_system(dims, 8, sd)
+            A = bsp.Matrix.from_system(s, h)
+            b = torch.tensor(s.b, device="cuda")
+            row = {"seed": sd}
+            for vname, mk, prec in (
+                    ("ilu0_f64", lambda: bsp.ILU0(A), _lib.PREC_F64),
+                    ("ilu0_f32", lambda: bsp.ILU0(A), _lib.PREC_F32),
+                    ("learned_forced_f64", lambda: model.precond(A), _lib.PREC_F64),
+                    ("learned_forced_f32", lambda: model.precond(A), _lib.PREC_F32),
+                    ("learned_with_fallback_f64", lambda: learned.LearnedLU(A, model), _lib.PREC_F64)):
+                _solve_variant(bsp, _lib, A, b, stream, mk, prec)  # warm-up
+                row[vname] = _solve_variant(bsp, _lib, A, b, stream, mk, prec)[1]
+            per.append(row)
+            A.close()
+    names = [k for k in per[0] if k != "seed"]
+    summary = {k: {"total_s": float(np.mean([r[k]["total_s"] for r in per])),
+                   "iters": float(np.mean([r[k]["iters"] for r in per]))} for k in names}
+    line = {"metric": "learned preconditioner ablation: time to FP64 true relative residual 1e-10",
+            "value": summary["learned_with_fallback_f64"]["total_s"], "unit": "s", "higher_is_better": False,
+            "n_gpus": 1, "dtype": "f64 (f32 storage variants marked)", "vs_baseline": None,
+            "data": f"synthetic held-out seeds {seeds} (training used 10000-10199, validation 20000-20003)",
+            "config": {"workload": f"cfg4: 3D {dims[0]}^3 convection-diffusion, 8x8 blocks, pGMRES(30, k=10)",
+                       "model_beats_ilu0_on_validation": bool(model.meta.get("beats_ilu0", False)),
+                       "model_validation": model.meta.get("validation")},
+            "summary": summary, "per_seed": per, "clocks": clk.summary()}
+    model.close()
+    h.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,16 +601,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="plain_f64,mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch"],
-                    help="cfg1: the headline line; batch: the 256-system batched pCG line")
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch", "mixed", "learned"],
+                    help="cfg1: the headline line; batch: 256-system batched pCG; mixed: cfg2 precision "
+                         "variants; learned: cfg4 ablation")
     ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--learned-side", type=int, default=96)
+    ap.add_argument("--learned-seeds", type=int, default=2)
     args = ap.parse_args()
-    if args.workload == "batch":
+    if args.workload != "cfg1":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the batch leg reports its CPU baseline "
-                              "in its own cpu_baseline field"}))
+            print(json.dumps({"impl": "reference", "unavailable": f"the {args.workload} leg reports its CPU "
+                              "reference inside its own line"}))
             return
-        run_batch(args)
+        {"batch": run_batch, "mixed": run_mixed, "learned": run_learned}[args.workload](args)
         return
     world, rank, local = dist_setup()
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "

@@ -535,10 +535,11 @@ int true_residual(bsp_handle_s* h, bsp_matrix_s* A, const double* b, const doubl
 
 
 // ------------------------------------------------------------------ pCG
-// Stored copy the inner operator reads: FP64 for the reference method, FP32
-// blocks (FP64 vectors, FP64 accumulation) for both mixed modes; the BF16
-// mode keeps A in FP32 and stores only the preconditioner factors in BF16.
-static int op_dtype_of(int op_prec) { return op_prec == BSP_PREC_F64 ? BSP_F64 : BSP_F32_STORE; }
+// Stored copy of A the inner operator reads: FP64 for the reference method,
+// FP32 or BF16 storage (FP64 vectors and accumulation) for the mixed modes.
+static int op_dtype_of(int op_prec) {
+  return op_prec == BSP_PREC_F64 ? BSP_F64 : op_prec == BSP_PREC_F32 ? BSP_F32_STORE : BSP_BF16_STORE;
+}
 
 int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b, double* x,
               const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info,
@@ -808,7 +809,7 @@ int refine_solve(bool gmres, bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc
   const int64_t len = (int64_t)A->n_rows * A->bs;
   const int prec = o->precision;
   if (prec != BSP_PREC_F64) {
-    BSP_TRY(bsp_matrix_make_lowp(A, BSP_F32));
+    BSP_TRY(bsp_matrix_make_lowp(A, prec == BSP_PREC_F32 ? BSP_F32 : BSP_BF16));
     if (pc) BSP_TRY(precond_ensure_precision(pc, prec));
   }
   DevBuf<double> r, d, work;
