@@ -126,6 +126,16 @@ def dist_setup():
     return world, rank, local
 
 
+def pinned_copy(a: np.ndarray) -> np.ndarray:
+    """numpy view of a page-locked host copy of a (host<->device copies from
+    pinned memory run at link speed and do not stage through a bounce buffer)."""
+    import torch
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
 def max_over_ranks(v: float, world: int) -> float:
     if world == 1:
         return v
@@ -246,14 +256,27 @@ def run_gpu(args, world, rank, local):
         return {"n": n, "bs": bs, "nnzb": nnzb, "results": results, "best": best, "e2e_s": float("nan"),
                 "bsmv_ms": bsmv_ms, "ilu_ms": ilu_ms, "levels": levels, "peak": peak,
                 "peak_kind": peak_kind, "clocks": clocks, "launches": launches, "x_norm": 0.0}
+    # Inputs in pinned host memory (numpy views of page-locked tensors); one
+    # untimed call, then the mean over the timed calls.  Each call uploads the
+    # matrix and right-hand side, builds ILU0, solves and reads x back.
+    rp_h, ci_h, va_h, b_h = (
+        pinned_copy(a) for a in (sysm.row_ptr.astype(np.int32), sysm.col_idx.astype(np.int32), sysm.vals, sysm.b))
+
+    def e2e_call():
+        A2 = bsp.Matrix(rp_h, ci_h, va_h, bs, handle=h)
+        pc2 = bsp.ILU0(A2)
+        out = bsp.pGMRES(A2, b_h, TOL, pc2, 5000, 30, 10, stop_rule=_lib.STOP_TRUE_RESIDUAL,
+                         precision=variants[best])
+        pc2.close()
+        A2.close()
+        return out
+
+    e2e_call()
+    e2e_steps = max(1, args.steps)
     t0 = time.perf_counter()
-    A2 = bsp.Matrix(sysm.row_ptr, sysm.col_idx, sysm.vals, bs, handle=h)
-    pc2 = bsp.ILU0(A2)
-    xh = bsp.pGMRES(A2, sysm.b, TOL, pc2, 5000, 30, 10, stop_rule=_lib.STOP_TRUE_RESIDUAL,
-                    precision=variants[best])
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    pc2.close()
-    A2.close()
+    for _ in range(e2e_steps):
+        xh = e2e_call()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
     A.close()
     h.close()
     return {
@@ -369,7 +392,7 @@ def run_batch(args):
     t0 = time.time()
     B = bsp.Batch(sl, h)
     create_s = time.time() - t0
-    bh = np.concatenate([s.b for s in sl])
+    bh = pinned_copy(np.concatenate([s.b for s in sl]))
     bd = torch.tensor(bh, device="cuda")
     peak, peak_kind = read_peaks()
 

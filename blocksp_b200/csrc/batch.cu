@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(kBSweepThreads) k_bt_sweep(const BSweepP p) {
           for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[r][v]);
         unsigned spins = 0;
         while (pending) {
-          __nanosleep(32);
+          poll_pause(spins);
           pending = false;
 #pragma unroll
           for (int r = 0; r < R; ++r) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -69,6 +70,12 @@ struct SymbolicCache {
   DevBuf<int64_t> d_perm, t_blk;
 };
 
+// Non-owning view of a scratch buffer (handle scratch; see bsp_handle_s).
+template <typename T> struct Span {
+  T* p = nullptr;
+  T* get() const { return p; }
+};
+
 // Device time between construction and stop_ms() on one stream.
 struct EventTimer {
   cudaEvent_t a = nullptr, b = nullptr;
@@ -103,6 +110,21 @@ struct bsp_handle_s {
   int epoch = 0;  // sync-free sweep epoch (flags hold the epoch of their last write)
   // staging buffers of the host-buffer entry points (grow-only, reused)
   bsp::DevBuf<double> stage_in, stage_out;
+  // Grow-only device scratch of the solvers, by purpose.  Every call on a
+  // handle is stream-ordered (and the solvers return after their work), so a
+  // buffer is free again when the next call that uses it is enqueued; reuse
+  // avoids cudaMalloc/cudaFree (a device-wide synchronisation) per solve.
+  std::map<std::string, bsp::DevBuf<unsigned char>> scratch_bufs;
+  template <typename T> int scratch(const std::string& tag, size_t count, T** out) {
+    auto& b = scratch_bufs[tag];
+    const size_t bytes = (count ? count : 1) * sizeof(T);
+    if (b.n < bytes) {
+      const int st = b.alloc(bytes);
+      if (st) return st;
+    }
+    *out = reinterpret_cast<T*>(b.p);
+    return 0;
+  }
   int stage(size_t n_in, size_t n_out) {
     if (stage_in.n < n_in) { int s = stage_in.alloc(n_in); if (s) return s; }
     if (stage_out.n < n_out) { int s = stage_out.alloc(n_out); if (s) return s; }
@@ -129,7 +151,43 @@ struct bsp_matrix_s {
   bool has_transpose = false;
   // symbolic analyses for ILU0 (full pattern), IChol0 (lower pattern), SOR/Diag
   bsp::SymbolicCache sym_ilu, sym_ichol, sym_sor;
+  // device memory of destroyed preconditioners of this matrix, handed to the
+  // next one built on it (factor copies, inverted diagonals, scratch)
+  std::vector<bsp::DevBuf<unsigned char>> bin;
 };
+
+namespace bsp {
+constexpr size_t kBinMax = 64;
+// d <- count elements, from A's bin when a buffer of fitting size is there.
+template <typename T> int take(bsp_matrix_s* A, DevBuf<T>& d, size_t count) {
+  count = count ? count : 1;
+  const size_t bytes = count * sizeof(T);
+  int best = -1;
+  for (size_t i = 0; i < A->bin.size(); ++i)
+    if (A->bin[i].n >= bytes && A->bin[i].n <= 2 * bytes + (1u << 20) &&
+        (best < 0 || A->bin[i].n < A->bin[best].n))
+      best = (int)i;
+  if (best < 0) return d.alloc(count);
+  d.release();
+  d.p = reinterpret_cast<T*>(A->bin[best].p);
+  d.n = count;
+  A->bin[best].p = nullptr;
+  A->bin[best].n = 0;
+  A->bin.erase(A->bin.begin() + best);
+  return BSP_OK;
+}
+// Hands d's memory to A's bin (the caller has made sure no work uses it).
+template <typename T> void give(bsp_matrix_s* A, DevBuf<T>& d) {
+  if (!d.p) return;
+  DevBuf<unsigned char> r;
+  r.p = reinterpret_cast<unsigned char*>(d.p);
+  r.n = d.n * sizeof(T);
+  d.p = nullptr;
+  d.n = 0;
+  A->bin.push_back(std::move(r));
+  if (A->bin.size() > kBinMax) A->bin.erase(A->bin.begin());
+}
+}  // namespace bsp
 
 // Uploads a validated structure and allocates (uninitialised) FP64 values.
 int matrix_create_struct(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb, const int* row_ptr,

@@ -499,10 +499,6 @@ __global__ void k_gm_pure_restart(GPtrs g) {
 }
 
 // ------------------------------------------------------------------ host helpers
-struct Vec {  // device vector pool entry
-  DevBuf<double> b;
-};
-
 static int read_head(bsp_handle_s* h, const KHead* d, KHead* out) {
   BSP_CUDA_TRY(cudaMemcpyAsync(out, d, sizeof(KHead), cudaMemcpyDeviceToHost, h->stream));
   BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -547,14 +543,14 @@ int pcg_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double*
   const int op_dtype = op_dtype_of(op_prec);
   const int64_t len = (int64_t)A->n_rows * A->bs;
   const int hcap = std::max(2, o->max_iters + 3);
-  DevBuf<double> vr, vp, vz, vAp, dhist;
-  DevBuf<KHead> dhead;
-  BSP_TRY(vr.alloc(len));
-  BSP_TRY(vp.alloc(len));
-  BSP_TRY(vz.alloc(len));
-  BSP_TRY(vAp.alloc(len));
-  BSP_TRY(dhist.alloc(hcap));
-  BSP_TRY(dhead.alloc(1));
+  Span<double> vr, vp, vz, vAp, dhist;
+  Span<KHead> dhead;
+  BSP_TRY(h->scratch("pcg.r", len, &vr.p));
+  BSP_TRY(h->scratch("pcg.p", len, &vp.p));
+  BSP_TRY(h->scratch("pcg.z", len, &vz.p));
+  BSP_TRY(h->scratch("pcg.Ap", len, &vAp.p));
+  BSP_TRY(h->scratch("pcg.hist", hcap, &dhist.p));
+  BSP_TRY(h->scratch("pcg.head", 1, &dhead.p));
   BSP_CUDA_TRY(cudaMemsetAsync(dhead.get(), 0, sizeof(KHead), h->stream));
   EventTimer tm(h->stream);
   const int g = grid_for(h, len, 256);
@@ -620,11 +616,11 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
   // restart, allocated once.  Unrestarted: grown in chunks as the space grows.
   constexpr int kChunk = 16;
   const int n_spare = restart > 0 ? std::min(k_req, m) + 2 : 0;
-  std::vector<DevBuf<double>> chunks;
+  int n_chunks = 0;
   std::vector<double*> qptr, spare;
-  DevBuf<double*> dq, dspare;
-  BSP_TRY(dq.alloc(m + 1));
-  BSP_TRY(dspare.alloc(std::max(n_spare, 1)));
+  Span<double*> dq, dspare;
+  BSP_TRY(h->scratch("gmres.qtab", m + 1, &dq.p));
+  BSP_TRY(h->scratch("gmres.sparetab", std::max(n_spare, 1), &dspare.p));
   auto upload_tables = [&]() -> int {
     const int cnt = std::min<int>((int)qptr.size(), m + 1);
     BSP_CUDA_TRY(cudaMemcpyAsync(dq.get(), qptr.data(), cnt * sizeof(double*), cudaMemcpyHostToDevice, h->stream));
@@ -636,37 +632,36 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     bool grew = false;
     while ((int)qptr.size() < count) {
       const int nv = restart > 0 ? (m + 1 + n_spare) : kChunk;
-      DevBuf<double> c;
-      BSP_TRY(c.alloc((size_t)nv * len));
+      double* c = nullptr;
+      BSP_TRY(h->scratch("gmres.basis." + std::to_string(n_chunks++), (size_t)nv * len, &c));
       for (int t = 0; t < nv; ++t) {
-        double* ptr = c.get() + (size_t)t * len;
+        double* ptr = c + (size_t)t * len;
         if (restart > 0 && t > m) spare.push_back(ptr);
         else qptr.push_back(ptr);
       }
-      chunks.push_back(std::move(c));
       grew = true;
     }
     if (grew) BSP_TRY(upload_tables());
     return BSP_OK;
   };
-  DevBuf<double> vv, vx0, vr0;
-  BSP_TRY(vv.alloc(len));
-  BSP_TRY(vx0.alloc(len));
-  BSP_TRY(vr0.alloc(len));
+  Span<double> vv, vx0, vr0;
+  BSP_TRY(h->scratch("gmres.v", len, &vv.p));
+  BSP_TRY(h->scratch("gmres.x0", len, &vx0.p));
+  BSP_TRY(h->scratch("gmres.r0", len, &vr0.p));
   // small dense state
   const int hcap = std::max(4, o->max_iters + 2 + (restart > 0 ? o->max_iters / restart + 2 : 0));
   const size_t HM = (size_t)(m + 1) * m;
   const size_t nrot_cap = (size_t)(m + 1) * (m + 2) / 2 + m + 8;
-  DevBuf<double> dsm;
+  Span<double> dsm;
   size_t dr = restart > 0 ? (size_t)m * m * 3 + (size_t)(m + 1) * (m + 2) + 8 * (size_t)m + 64 + HM : 0;
   const size_t total = 2 * HM + 3 * (size_t)(m + 2) + hcap + dr;
-  BSP_TRY(dsm.alloc(total));
-  DevBuf<sd::Rot> drots;
-  BSP_TRY(drots.alloc(nrot_cap));
-  DevBuf<int> dint;
-  BSP_TRY(dint.alloc(1 + 2 * (size_t)m + 8));
-  DevBuf<KHead> dhead;
-  BSP_TRY(dhead.alloc(1));
+  BSP_TRY(h->scratch("gmres.dense", total, &dsm.p));
+  Span<sd::Rot> drots;
+  BSP_TRY(h->scratch("gmres.rots", nrot_cap, &drots.p));
+  Span<int> dint;
+  BSP_TRY(h->scratch("gmres.int", 1 + 2 * (size_t)m + 8, &dint.p));
+  Span<KHead> dhead;
+  BSP_TRY(h->scratch("gmres.head", 1, &dhead.p));
   BSP_CUDA_TRY(cudaMemsetAsync(dsm.get(), 0, total * sizeof(double), h->stream));
   BSP_CUDA_TRY(cudaMemsetAsync(dhead.get(), 0, sizeof(KHead), h->stream));
   GPtrs gp{};
@@ -812,10 +807,10 @@ int refine_solve(bool gmres, bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc
     BSP_TRY(bsp_matrix_make_lowp(A, prec == BSP_PREC_F32 ? BSP_F32 : BSP_BF16));
     if (pc) BSP_TRY(precond_ensure_precision(pc, prec));
   }
-  DevBuf<double> r, d, work;
-  BSP_TRY(r.alloc(len));
-  BSP_TRY(d.alloc(len));
-  BSP_TRY(work.alloc(len));
+  Span<double> r, d, work;
+  BSP_TRY(h->scratch("refine.r", len, &r.p));
+  BSP_TRY(h->scratch("refine.d", len, &d.p));
+  BSP_TRY(h->scratch("refine.work", len, &work.p));
   const int g = grid_for(h, len, 256);
   EventTimer tm(h->stream);
   double* sc = h->ws.scalars.get();
@@ -939,9 +934,9 @@ int bsp_true_residual_dev(bsp_handle_t h, bsp_matrix_t A, const double* b, const
                           double* rel_res_host) {
   if (!h || !A || !b || !x || !rel_res_host) return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
-  DevBuf<double> w;
-  BSP_TRY(w.alloc((size_t)A->n_rows * A->bs));
-  return true_residual(h, A, b, x, w.get(), rel_res_host);
+  double* w = nullptr;
+  BSP_TRY(h->scratch("true_residual.w", (size_t)A->n_rows * A->bs, &w));
+  return true_residual(h, A, b, x, w, rel_res_host);
 }
 
 }  // extern "C"

@@ -43,7 +43,7 @@ __device__ __forceinline__ void wait_flag(const int* f, int epoch, DevStatus* st
   if (ld_acquire(f) == epoch) return;
   unsigned spins = 0;
   while (ld_acquire(f) != epoch) {
-    __nanosleep(40);
+    poll_pause(spins);
     if ((++spins & 255u) == 0u) {
       if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;  // already failed
       if (spins > kSpinLimit) {
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
       unsigned spins = 0;
       while (pending) {
-        __nanosleep(32);
+        poll_pause(spins);
         if constexpr (!TRANS) {
 #pragma unroll
           for (int v = 0; v < V; ++v) xv[v] = ld_poll(p.x + (int64_t)j * BS + c0 + v);
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_generic(const SweepP<VT
           if (poll) {
             unsigned spins = 0;
             while (is_sentinel(xc)) {  // row j of this sweep not final yet
-              __nanosleep(32);
+              poll_pause(spins);
               xc = ld_poll(src + (int64_t)j * bs + c);
               if ((++spins & 255u) == 0u) {
                 if (*reinterpret_cast<volatile int*>(&p.st->code) != 0) break;
@@ -666,8 +666,10 @@ template <typename T> static int upload(DevBuf<T>& d, const std::vector<T>& v) {
   return BSP_OK;
 }
 
-template <typename T> static int copy_dev(DevBuf<T>& dst, const DevBuf<T>& src, cudaStream_t s) {
-  BSP_TRY(dst.alloc(src.n ? src.n : 1));
+template <typename T>
+static int copy_dev(DevBuf<T>& dst, const DevBuf<T>& src, cudaStream_t s, bsp_matrix_s* recycle = nullptr) {
+  if (recycle) BSP_TRY(take(recycle, dst, src.n ? src.n : 1));
+  else BSP_TRY(dst.alloc(src.n ? src.n : 1));
   if (src.n) BSP_CUDA_TRY(cudaMemcpyAsync(dst.get(), src.get(), src.n * sizeof(T), cudaMemcpyDeviceToDevice, s));
   return BSP_OK;
 }
@@ -675,7 +677,7 @@ template <typename T> static int copy_dev(DevBuf<T>& dst, const DevBuf<T>& src, 
 // Preconditioner <-> the matrix's cached symbolic analysis (device-to-device copies).
 static int sym_transfer(bsp_precond_s* pc, SymbolicCache& C, bool save) {
   cudaStream_t s = pc->h->stream;
-#define BSP_SYM_FIELD(f) BSP_TRY(save ? copy_dev(C.f, pc->f, s) : copy_dev(pc->f, C.f, s));
+#define BSP_SYM_FIELD(f) BSP_TRY(save ? copy_dev(C.f, pc->f, s) : copy_dev(pc->f, C.f, s, pc->A));
   BSP_SYM_FIELD(f_ptr) BSP_SYM_FIELD(f_col) BSP_SYM_FIELD(f_diag) BSP_SYM_FIELD(d_perm)
   BSP_SYM_FIELD(order_lo) BSP_SYM_FIELD(order_up) BSP_SYM_FIELD(task_lo_row) BSP_SYM_FIELD(task_lo_len)
   BSP_SYM_FIELD(task_up_row) BSP_SYM_FIELD(task_up_len) BSP_SYM_FIELD(t_ptr) BSP_SYM_FIELD(t_row)
@@ -904,7 +906,7 @@ static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
     BSP_TRY(sym_transfer(pc, C, true));
   }
   const int b2 = pc->bs * pc->bs;
-  BSP_TRY(pc->f_vals.alloc(pc->f_nnzb * b2));
+  BSP_TRY(take(pc->A, pc->f_vals, pc->f_nnzb * b2));
   bsp::count_launch(), k_gather_blocks<<<grid_for(pc->h, pc->f_nnzb * b2, 256), 256, 0, pc->h->stream>>>(
       pc->f_nnzb, b2, pc->d_perm.get(), pc->A->vals.get(), pc->f_vals.get());
   BSP_CUDA_TRY(cudaPeekAtLastError());
@@ -966,17 +968,17 @@ static int make_lowp_copies(bsp_precond_s* pc) {
   const int64_t nd = (int64_t)pc->n * b2;
   const int64_t nf = pc->f_nnzb * b2;
   if (pc->precision == BSP_PREC_F32) {
-    BSP_TRY(pc->dinv32.alloc(nd));
+    BSP_TRY(take(pc->A, pc->dinv32, nd));
     bsp::count_launch(), k_convert<float><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv32.get());
     if (nf > 0) {
-      BSP_TRY(pc->f_vals32.alloc(nf));
+      BSP_TRY(take(pc->A, pc->f_vals32, nf));
       bsp::count_launch(), k_convert<float><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals32.get());
     }
   } else {
-    BSP_TRY(pc->dinv16.alloc(nd));
+    BSP_TRY(take(pc->A, pc->dinv16, nd));
     bsp::count_launch(), k_convert<__nv_bfloat16><<<grid_for(pc->h, nd, 256), 256, 0, pc->h->stream>>>(nd, pc->dinv.get(), pc->dinv16.get());
     if (nf > 0) {
-      BSP_TRY(pc->f_vals16.alloc(nf));
+      BSP_TRY(take(pc->A, pc->f_vals16, nf));
       bsp::count_launch(), k_convert<__nv_bfloat16><<<grid_for(pc->h, nf, 256), 256, 0, pc->h->stream>>>(nf, pc->f_vals.get(), pc->f_vals16.get());
     }
   }
@@ -986,9 +988,9 @@ static int make_lowp_copies(bsp_precond_s* pc) {
 
 int precond_build(bsp_precond_s* pc) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
-  BSP_TRY(pc->dinv.alloc((size_t)std::max(n, 1) * b2));
-  BSP_TRY(pc->flags.alloc(std::max(n, 1)));
-  BSP_TRY(pc->ticket.alloc(1));
+  BSP_TRY(take(pc->A, pc->dinv, (size_t)std::max(n, 1) * b2));
+  BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
+  BSP_TRY(take(pc->A, pc->ticket, 1));
   BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
   switch (pc->kind) {
     case BSP_PC_NONE:
@@ -1026,9 +1028,9 @@ __global__ void k_add_perm(int64_t nblk, int b2, const int64_t* __restrict__ per
 // order; the diagonal inverses are recomputed from the corrected U_ii.
 int precond_build_learned(bsp_precond_s* pc, const double* dF) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
-  BSP_TRY(pc->dinv.alloc((size_t)std::max(n, 1) * b2));
-  BSP_TRY(pc->flags.alloc(std::max(n, 1)));
-  BSP_TRY(pc->ticket.alloc(1));
+  BSP_TRY(take(pc->A, pc->dinv, (size_t)std::max(n, 1) * b2));
+  BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
+  BSP_TRY(take(pc->A, pc->ticket, 1));
   BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
   BSP_TRY(build_factor_structure(pc, false));
   BSP_TRY(run_factor(pc, FACT_ILU0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(), pc->f_diag.get(),
@@ -1298,9 +1300,9 @@ __global__ void k_copy_add_perm(int64_t nblk, int b2, const int64_t* __restrict_
 // precond_learned_refresh (no factorisation).
 int precond_learned_init(bsp_precond_s* pc) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
-  BSP_TRY(pc->dinv.alloc((size_t)std::max(n, 1) * b2));
-  BSP_TRY(pc->flags.alloc(std::max(n, 1)));
-  BSP_TRY(pc->ticket.alloc(1));
+  BSP_TRY(take(pc->A, pc->dinv, (size_t)std::max(n, 1) * b2));
+  BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
+  BSP_TRY(take(pc->A, pc->ticket, 1));
   BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
   return build_factor_structure(pc, false);
 }
@@ -1328,7 +1330,7 @@ int precond_apply_typed(bsp_precond_s* pc, int precision, bool vec64, const void
   if (precision == BSP_PREC_BF16 && !pc->dinv16.get()) return BSP_INVALID;
   if (precision == BSP_PREC_F64 || vec64) {
     for (auto& s : pc->s64)
-      if (s.n < nv) BSP_TRY(s.alloc(nv));
+      if (s.n < nv) BSP_TRY(take(pc->A, s, nv));
     double *a = pc->s64[0].get(), *b = pc->s64[1].get(), *c = pc->s64[2].get();
     if (precision == BSP_PREC_F64)
       return apply_typed<double, double>(pc, (const double*)r, (double*)z, pc->f_vals.get(),
@@ -1340,7 +1342,7 @@ int precond_apply_typed(bsp_precond_s* pc, int precision, bool vec64, const void
                                               pc->dinv16.get(), pc->A->vals16.get(), a, b, c);
   }
   for (auto& s : pc->s32)
-    if (s.n < nv) BSP_TRY(s.alloc(nv));
+    if (s.n < nv) BSP_TRY(take(pc->A, s, nv));
   float *a = pc->s32[0].get(), *b = pc->s32[1].get(), *c = pc->s32[2].get();
   if (precision == BSP_PREC_F32)
     return apply_typed<float, float>(pc, (const float*)r, (float*)z, pc->f_vals32.get(),
@@ -1427,6 +1429,22 @@ int bsp_precond_create(bsp_handle_t h, bsp_matrix_t A, const bsp_precond_params*
 int bsp_precond_destroy(bsp_precond_t pc) {
   if (!pc) return BSP_OK;
   cudaSetDevice(pc->device);
+  // the matrix outlives its preconditioners: its bin keeps their device memory
+  // for the next preconditioner built on it (no cudaFree / cudaMalloc pair)
+  if (pc->A && cudaDeviceSynchronize() == cudaSuccess) {
+    bsp_matrix_s* A = pc->A;
+    give(A, pc->f_vals); give(A, pc->f_vals32); give(A, pc->f_vals16);
+    give(A, pc->dinv); give(A, pc->dinv32); give(A, pc->dinv16);
+    give(A, pc->f_ptr); give(A, pc->f_col); give(A, pc->f_diag); give(A, pc->d_perm);
+    give(A, pc->t_ptr); give(A, pc->t_row); give(A, pc->t_blk); give(A, pc->a_diag);
+    give(A, pc->order_lo); give(A, pc->order_up);
+    give(A, pc->task_lo_row); give(A, pc->task_lo_len); give(A, pc->task_up_row); give(A, pc->task_up_len);
+    give(A, pc->flags);
+    for (int i = 0; i < 3; ++i) {
+      give(A, pc->s64[i]);
+      give(A, pc->s32[i]);
+    }
+  }
   delete pc;
   return BSP_OK;
 }

@@ -26,4 +26,12 @@ __device__ __forceinline__ float ld_poll(const float* p) {
   return v;
 }
 
+// Pause between polls of a value another group is about to publish: the first
+// polls re-read at once (the producer is usually a few hundred cycles away),
+// later ones back off so long waits do not flood L2 with re-reads.
+constexpr unsigned kSpinFree = 32;
+__device__ __forceinline__ void poll_pause(unsigned spins) {
+  if (spins >= kSpinFree) __nanosleep(spins >= 1024 ? 256 : 32);
+}
+
 }  // namespace bsp
