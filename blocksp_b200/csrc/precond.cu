@@ -26,6 +26,14 @@
 // requirement.  The factorisation uses per-row ready flags that hold the
 // epoch of the launch that last wrote them, so they never need clearing.
 //
+// A row's own inputs are staged ahead of it, so only the cross-chain values
+// remain on the dependency path: each group keeps a shared-memory ring with
+// the chain's next D rows (matrix blocks, inverted diagonal, right-hand side,
+// old iterate), filled by per-lane cp.async copies; the chain's structure
+// (entry ranges, column and block indices) is loaded one window of G rows
+// ahead, one row per lane, and handed out by shuffles; the chain's previous
+// row is passed on in registers.
+//
 // The factorisation is row-oriented (IKJ): row k applies the eliminations of
 // rows i < k in increasing i, exactly the sequence of updates the reference's
 // right-looking loop applies to each block (k, j), so the factors are the same.
@@ -35,6 +43,7 @@
 #include "precond.hpp"
 #include "reduce.cuh"
 #include "sentinel.cuh"
+#include "stage.cuh"
 
 namespace bsp {
 
@@ -94,6 +103,7 @@ template <typename VT, typename AT> struct SweepP {
   const int* task_len;
   int task_dir;
   int n_tasks;
+  int stage_vec;  // rhs and xold are 16-byte aligned: staged with the blocks (set at launch)
 };
 
 template <typename VT, typename AT>
@@ -107,16 +117,53 @@ __device__ __forceinline__ void row_range(const SweepP<VT, AT>& p, int i, int& b
 }
 
 constexpr int kSweepThreads = 256;
+constexpr int kSlotBudget = 12288;  // staging bytes per group of lanes
+
+// Shared-memory ring of one group of lanes: D slots, each holding one row's
+// first NPF blocks, its inverted diagonal block, right-hand side and old
+// iterate, filled by per-lane asynchronous copies D rows ahead of their use.
+// Every lane copies exactly the 16-byte chunks (and vector values) it reads
+// later, so a lane only ever waits for its own copies.
+template <int BS, typename VT, typename AT, bool TRANS, int POST> struct SweepCfg {
+  using M = BlockMap<BS, VT>;
+  static constexpr int G = M::G, P = M::P, CPB = M::CPB;
+  static constexpr int GPC = kSweepThreads / G;
+  static constexpr int NPF = (P == 1) ? 4 : (P == 2 ? 2 : 1);  // entries staged per row
+  static constexpr bool kUseD = POST != POST_NONE;
+  static constexpr int XR = TRANS ? M::V : P;          // rhs values a lane reads per row
+  static constexpr int BB = CPB * 16;                  // bytes of one block
+  static constexpr int LRB = XR * (int)sizeof(AT);     // rhs bytes of one lane
+  static_assert(!TRANS || LRB % 16 == 0, "transposed rhs pieces are whole 16-byte chunks");
+  static constexpr int OFF_D = NPF * BB;
+  static constexpr int OFF_R = OFF_D + (kUseD ? BB : 0);
+  static constexpr int OFF_O = OFF_R + (G * LRB + 15) / 16 * 16;
+  static constexpr int SB = OFF_O + (POST == POST_SOR ? (G * P * (int)sizeof(AT) + 15) / 16 * 16 : 0);
+  static constexpr int D0 = (4 * SB <= kSlotBudget) ? 4 : (3 * SB <= kSlotBudget ? 3 : 2);
+  static constexpr int D = D0 < G ? D0 : G;  // lookahead stays within the next structure window
+  static constexpr size_t kSmem = (size_t)GPC * D * SB;
+};
 
 template <int BS, typename VT, typename AT, bool TRANS, int POST>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p) {
+  // Launch parameters used on the per-row path, held in registers.
+  const int* __restrict__ const idx_ = p.idx;
+  const int64_t* __restrict__ const blk_ = p.blk;
+  const int range_ = p.range, dep_dir_ = p.dep_dir, task_dir_ = p.task_dir;
+  const VT* __restrict__ const dinv_ = p.dinv;
+  const AT* __restrict__ const rhs_ = p.rhs;
+  const AT* __restrict__ const xold_ = p.xold;
+  AT* const x_ = p.x;
+  const AT w_ = p.w;
+  DevStatus* const st_ = p.st;
   using M = BlockMap<BS, VT>;
+  using C = SweepCfg<BS, VT, AT, TRANS, POST>;
   using CV = typename Chunk<VT>::vec;
   constexpr int V = M::V, G = M::G, P = M::P, CPR = M::CPR, RPP = M::RPP, CPB = M::CPB;
-  constexpr int GPC = kSweepThreads / G;
-  // entries whose blocks are loaded ahead (for the next row of the chain)
-  constexpr int NPF = (P == 1) ? 4 : (P == 2 ? 2 : 1);
-  constexpr bool kUseD = POST != POST_NONE;
+  constexpr int GPC = C::GPC, NPF = C::NPF, D = C::D, SB = C::SB, BB = C::BB;
+  constexpr bool kUseD = C::kUseD;
+  constexpr int XV = TRANS ? P : V;  // x values a lane reads per entry
+  constexpr int XR = TRANS ? V : P;  // rhs values a lane reads per row
+  extern __shared__ __align__(128) unsigned char sweep_smem[];
   __shared__ AT sm_s[GPC][BS];
   __shared__ AT sm_x[GPC][BS];  // the group's previous row of its chain
   const int gl = threadIdx.x % G;
@@ -128,8 +175,104 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
   const CV* vb = reinterpret_cast<const CV*>(p.vals);
   AT* s = sm_s[gid];
   AT* xs = sm_x[gid];
+  unsigned char* ring = sweep_smem + (size_t)gid * D * SB;
   const int n_tasks = p.task_row ? p.n_tasks : p.n;
+  const bool stage_vec = p.stage_vec != 0;
 
+  // Fill slot `slot` with row r, whose first entries are b0.. (block indices
+  // bx) of the range [b0, b1): one commit group per row and lane.
+  auto issue = [&](int r, int slot, int b0, int b1, const int64_t (&bx)[NPF]) {
+    unsigned char* dst = ring + slot * SB;
+#pragma unroll
+    for (int u = 0; u < NPF; ++u)
+      if (b0 + u < b1) {
+#pragma unroll
+        for (int q = 0; q < P; ++q) cp_async16(dst + u * BB + (q * G + gl) * 16, vb + bx[u] * CPB + q * G + gl);
+      }
+    if constexpr (kUseD) {
+      const CV* db = reinterpret_cast<const CV*>(dinv_) + (int64_t)r * CPB;
+#pragma unroll
+      for (int q = 0; q < P; ++q) cp_async16(dst + C::OFF_D + (q * G + gl) * 16, db + q * G + gl);
+    }
+    if (stage_vec) {
+      unsigned char* rd = dst + C::OFF_R + gl * C::LRB;
+      if constexpr (!TRANS) {
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+          cp_async_small<sizeof(AT)>(rd + q * sizeof(AT), rhs_ + (int64_t)r * BS + q * RPP + gl / CPR);
+      } else {
+#pragma unroll
+        for (int k = 0; k < C::LRB / 16; ++k)
+          cp_async16(rd + 16 * k, reinterpret_cast<const unsigned char*>(rhs_ + (int64_t)r * BS + c0) + 16 * k);
+      }
+      if constexpr (POST == POST_SOR) {
+        if (xold_) {
+          unsigned char* od = dst + C::OFF_O + gl * P * sizeof(AT);
+#pragma unroll
+          for (int q = 0; q < P; ++q)
+            cp_async_small<sizeof(AT)>(od + q * sizeof(AT), xold_ + (int64_t)r * BS + q * RPP + gl / CPR);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  // Entry classes: 0 skip, 1 the chain's previous row (shared memory),
+  // 2 a row of this sweep (polled until it is no longer the sentinel),
+  // 3 the previous iterate (SOR, final values).
+  auto classify_j = [&](int j, int r, int pv) -> int {
+    if (range_ == RANGE_SPLIT) {
+      if (j == r) return 0;
+      const bool dep = (dep_dir_ < 0) ? (j < r) : (j > r);
+      if (!dep) return xold_ ? 3 : 0;
+    }
+    return j == pv ? 1 : 2;
+  };
+  auto classify = [&](int e, int r, int pv, int& j) -> int {
+    j = __ldg(idx_ + e);
+    return classify_j(j, r, pv);
+  };
+  // The chain's previous row, as this lane reads it (kind 1 entries).
+  AT xp[XV];
+  auto load_x = [&](int kind, int j, AT (&xv)[XV]) {
+    const AT* src = kind == 3 ? xold_ : x_;
+    if (kind == 1) {
+#pragma unroll
+      for (int v = 0; v < XV; ++v) xv[v] = xp[v];
+    } else if constexpr (!TRANS) {
+      ld_vec_cg<V>(src + (int64_t)j * BS + c0, xv);
+    } else {
+#pragma unroll
+      for (int q = 0; q < P; ++q) xv[q] = __ldcg(src + (int64_t)j * BS + q * RPP + gl / CPR);
+    }
+  };
+  auto poll_x = [&](int j, AT (&xv)[XV], int who) {
+    bool pending = false;
+#pragma unroll
+    for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
+    unsigned spins = 0;
+    while (pending) {
+      poll_pause(spins);
+      if constexpr (!TRANS) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) xv[v] = ld_poll(x_ + (int64_t)j * BS + c0 + v);
+      } else {
+#pragma unroll
+        for (int q = 0; q < P; ++q) xv[q] = ld_poll(x_ + (int64_t)j * BS + q * RPP + gl / CPR);
+      }
+      pending = false;
+#pragma unroll
+      for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
+      if (pending && (++spins & 255u) == 0u) {
+        if (*reinterpret_cast<volatile int*>(&st_->code) != 0) break;  // already failed
+        if (spins > kSpinLimit) {
+          set_status(st_, BSP_TIMEOUT, who);
+          break;
+        }
+      }
+    }
+  };
+
+  unsigned cons = 0;  // rows consumed from this group's ring
   while (true) {
     int t = 0;
     if (gl == 0) t = (int)atomicAdd(p.ticket, 1u);
@@ -143,101 +286,104 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       i0 = p.order ? __ldg(p.order + t) : t;
       len = 1;
     }
-    // Matrix blocks and inverted diagonals do not depend on the sweep, so the
-    // loads for row step+1 of the chain are issued while row step computes.
-    CV nf[NPF][P], nd[P];
-    int nbeg, nend;
-    auto prefetch = [&](int r, int& b0, int& b1) {
-      row_range(p, r, b0, b1);
+    // Row structure of the chain (entry range, first column and block
+    // indices), one row per lane in windows of G rows, loaded a window ahead
+    // and handed out by shuffles: no structure load sits on a row's path.
+    struct Win {
+      int b0, b1;
+      int jx[NPF];
+      int64_t bx[NPF];
+    };
+    auto load_window = [&](int w, Win& o) {
+      const int k = w * G + gl;
+      o.b0 = o.b1 = 0;
+      if (k < len) row_range(p, i0 + k * task_dir_, o.b0, o.b1);
 #pragma unroll
       for (int u = 0; u < NPF; ++u) {
-        if (b0 + u < b1) {
-          const int64_t b = p.blk ? __ldg(p.blk + b0 + u) : (int64_t)(b0 + u);
-#pragma unroll
-          for (int q = 0; q < P; ++q) nf[u][q] = ld_stream(vb + b * CPB + q * G + gl);
-        }
-      }
-      if constexpr (kUseD) {
-        const CV* db = reinterpret_cast<const CV*>(p.dinv) + (int64_t)r * CPB;
-#pragma unroll
-        for (int q = 0; q < P; ++q) nd[q] = ld_stream(db + q * G + gl);
+        const bool in = o.b0 + u < o.b1;
+        o.jx[u] = in ? __ldg(idx_ + o.b0 + u) : -1;
+        o.bx[u] = in ? (blk_ ? __ldg(blk_ + o.b0 + u) : (int64_t)(o.b0 + u)) : 0;
       }
     };
-    prefetch(i0, nbeg, nend);
+    auto row_of = [&](const Win& w, int k, int& b0, int& b1, int (&jx)[NPF], int64_t (&bx)[NPF]) {
+      const int src = gbase + k % G;
+      b0 = __shfl_sync(gmask, w.b0, src);
+      b1 = __shfl_sync(gmask, w.b1, src);
+#pragma unroll
+      for (int u = 0; u < NPF; ++u) {
+        jx[u] = __shfl_sync(gmask, w.jx[u], src);
+        bx[u] = __shfl_sync(gmask, w.bx[u], src);
+      }
+    };
+    Win cur, nxt;
+    load_window(0, cur);
+    if (len > G) load_window(1, nxt);
+    // Matrix blocks, inverted diagonals, right-hand sides and old iterates do
+    // not depend on the sweep: the ring holds the chain's next D rows.
+    // (every lane commits exactly one copy group per ring position, empty
+    // past the chain's end, so row s is complete once D - 1 groups remain)
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      if (k < len) {  // uniform over the group (the shuffles need every lane)
+        int b0, b1, jx[NPF];
+        int64_t bx[NPF];
+        row_of(cur, k, b0, b1, jx, bx);
+        issue(i0 + k * task_dir_, (int)((cons + k) % D), b0, b1, bx);
+      } else {
+        cp_async_commit();
+      }
+    }
    for (int step = 0; step < len; ++step) {
-    const int i = i0 + step * p.task_dir;
-    const int prev = step > 0 ? i - p.task_dir : -1;
-    const int beg = nbeg, end = nend;
+    if (step > 0 && step % G == 0) {  // next structure window
+      cur = nxt;
+      if ((step / G + 1) * G < len) load_window(step / G + 1, nxt);
+    }
+    const int i = i0 + step * task_dir_;
+    const int prev = step > 0 ? i - task_dir_ : -1;
+    int beg, end, jr[NPF];
+    int64_t br[NPF];
+    row_of(cur, step, beg, end, jr, br);
+    const int slot = (int)(cons % D);
+    cp_async_wait<D - 1>();
+    ++cons;
+    const unsigned char* sl = ring + slot * SB;
+    const CV* sblk = reinterpret_cast<const CV*>(sl);
     CV pf[NPF][P], pd[P];
+    AT rh[XR], xo[P];
 #pragma unroll
     for (int u = 0; u < NPF; ++u)
+      if (beg + u < end) {
 #pragma unroll
-      for (int q = 0; q < P; ++q) pf[u][q] = nf[u][q];
+        for (int q = 0; q < P; ++q) pf[u][q] = sblk[u * CPB + q * G + gl];
+      }
+    if constexpr (kUseD) {
+      const CV* sd = reinterpret_cast<const CV*>(sl + C::OFF_D);
 #pragma unroll
-    for (int q = 0; q < P; ++q) pd[q] = nd[q];
-    if (step + 1 < len) prefetch(i + p.task_dir, nbeg, nend);
+      for (int q = 0; q < P; ++q) pd[q] = sd[q * G + gl];
+    }
+    if (stage_vec) {
+      const AT* rl = reinterpret_cast<const AT*>(sl + C::OFF_R) + gl * C::XR;
+#pragma unroll
+      for (int v = 0; v < XR; ++v) rh[v] = rl[v];
+    } else if constexpr (!TRANS) {
+#pragma unroll
+      for (int q = 0; q < P; ++q) rh[q] = __ldcg(rhs_ + (int64_t)i * BS + q * RPP + gl / CPR);
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rh[v] = __ldcg(rhs_ + (int64_t)i * BS + c0 + v);
+    }
+    if constexpr (POST == POST_SOR) {
+      const AT* ol = reinterpret_cast<const AT*>(sl + C::OFF_O) + gl * P;
+#pragma unroll
+      for (int q = 0; q < P; ++q)
+        xo[q] = !xold_ ? AT(0) : stage_vec ? ol[q] : __ldcg(xold_ + (int64_t)i * BS + q * RPP + gl / CPR);
+    }
     AT acc[P];
     AT tac[V];
 #pragma unroll
     for (int q = 0; q < P; ++q) acc[q] = AT(0);
 #pragma unroll
     for (int v = 0; v < V; ++v) tac[v] = AT(0);
-    // Entry classes: 0 skip, 1 the chain's previous row (shared memory),
-    // 2 a row of this sweep (polled until it is no longer the sentinel),
-    // 3 the previous iterate (SOR, final values).
-    constexpr int XV = TRANS ? P : V;  // x values a lane reads per entry
-    auto classify = [&](int e, int& j) -> int {
-      j = __ldg(p.idx + e);
-      if (p.range == RANGE_SPLIT) {
-        if (j == i) return 0;
-        const bool dep = (p.dep_dir < 0) ? (j < i) : (j > i);
-        if (!dep) return p.xold ? 3 : 0;
-      }
-      return j == prev ? 1 : 2;
-    };
-    auto load_x = [&](int kind, int j, AT (&xv)[XV]) {
-      const AT* src = kind == 3 ? p.xold : p.x;
-      if constexpr (!TRANS) {
-        if (kind == 1) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) xv[v] = xs[c0 + v];
-        } else {
-          ld_vec_cg<V>(src + (int64_t)j * BS + c0, xv);
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-          const int r = q * RPP + gl / CPR;
-          xv[q] = kind == 1 ? xs[r] : __ldcg(src + (int64_t)j * BS + r);
-        }
-      }
-    };
-    auto poll_x = [&](int j, AT (&xv)[XV]) {
-      bool pending = false;
-#pragma unroll
-      for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
-      unsigned spins = 0;
-      while (pending) {
-        poll_pause(spins);
-        if constexpr (!TRANS) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) xv[v] = ld_poll(p.x + (int64_t)j * BS + c0 + v);
-        } else {
-#pragma unroll
-          for (int q = 0; q < P; ++q) xv[q] = ld_poll(p.x + (int64_t)j * BS + q * RPP + gl / CPR);
-        }
-        pending = false;
-#pragma unroll
-        for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
-        if (pending && (++spins & 255u) == 0u) {
-          if (*reinterpret_cast<volatile int*>(&p.st->code) != 0) break;  // already failed
-          if (spins > kSpinLimit) {
-            set_status(p.st, BSP_TIMEOUT, i);
-            break;
-          }
-        }
-      }
-    };
     auto fma_entry = [&](const CV (&a)[P], const AT (&xv)[XV]) {
       if constexpr (!TRANS) {
 #pragma unroll
@@ -264,27 +410,28 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       int kind[NPF], jj[NPF];
 #pragma unroll
       for (int u = 0; u < NPF; ++u) {
-        kind[u] = (beg + u < end) ? classify(beg + u, jj[u]) : 0;
+        jj[u] = jr[u];
+        kind[u] = (beg + u < end) ? classify_j(jj[u], i, prev) : 0;
         if (kind[u]) load_x(kind[u], jj[u], xv[u]);
       }
 #pragma unroll
       for (int u = 0; u < NPF; ++u) {
-        if (kind[u] == 2) poll_x(jj[u], xv[u]);
+        if (kind[u] == 2) poll_x(jj[u], xv[u], i);
         if (kind[u]) fma_entry(pf[u], xv[u]);
       }
     }
     for (int e = beg + NPF; e < end; ++e) {
       int j;
-      const int kind = classify(e, j);
+      const int kind = classify(e, i, prev, j);
       if (!kind) continue;
-      const int64_t b = p.blk ? __ldg(p.blk + e) : (int64_t)e;
+      const int64_t b = blk_ ? __ldg(blk_ + e) : (int64_t)e;
       CV a[P];
 #pragma unroll
       for (int q = 0; q < P; ++q) a[q] = ld_stream(vb + b * CPB + q * G + gl);
-      AT xv[XV];
-      load_x(kind, j, xv);
-      if (kind == 2) poll_x(j, xv);
-      fma_entry(a, xv);
+      AT xe[XV];
+      load_x(kind, j, xe);
+      if (kind == 2) poll_x(j, xe, i);
+      fma_entry(a, xe);
     }
     // s = rhs_i - sum  (in shared memory, BS values per group)
     if constexpr (!TRANS) {
@@ -294,7 +441,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
 #pragma unroll
         for (int q = 0; q < P; ++q) {
           const int r = q * RPP + gl / CPR;
-          s[r] = __ldcg(p.rhs + (int64_t)i * BS + r) - acc[q];
+          s[r] = rh[q] - acc[q];
         }
       }
     } else {
@@ -304,14 +451,14 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         for (int o = CPR; o < G; o <<= 1) tac[v] += __shfl_xor_sync(gmask, tac[v], o);
       if (gl < CPR) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) s[c0 + v] = __ldcg(p.rhs + (int64_t)i * BS + c0 + v) - tac[v];
+        for (int v = 0; v < V; ++v) s[c0 + v] = rh[v] - tac[v];
       }
     }
     __syncwarp(gmask);
     // post-operation and write-back of row i
     if constexpr (POST == POST_NONE) {
       for (int r = gl; r < BS; r += G) {
-        p.x[(int64_t)i * BS + r] = s[r];
+        x_[(int64_t)i * BS + r] = s[r];
         xs[r] = s[r];
       }
     } else if constexpr (POST == POST_D || POST == POST_SOR) {
@@ -335,10 +482,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
           AT val = o[q];
           if constexpr (POST == POST_SOR) {
             // x(im) += -w * x(im) + w * ph   (preconditioners.hpp:161-165)
-            const AT xo = p.xold ? __ldcg(p.xold + (int64_t)i * BS + r) : AT(0);
-            val = xo + (-p.w * xo + p.w * val);
+            val = xo[q] + (-w_ * xo[q] + w_ * val);
           }
-          p.x[(int64_t)i * BS + r] = val;
+          x_[(int64_t)i * BS + r] = val;
           xs[r] = val;
         }
       }
@@ -362,15 +508,37 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       if (gl < CPR) {
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          p.x[(int64_t)i * BS + c0 + v] = o[v];
+          x_[(int64_t)i * BS + c0 + v] = o[v];
           xs[c0 + v] = o[v];
         }
       }
     }
     // Row i is published by its values themselves: readers poll the 8-byte
     // words until they are no longer the sentinel, so no flag or fence is
-    // needed.  The barrier keeps shared memory consistent for the next row.
+    // needed.  The barrier keeps shared memory consistent for the next row,
+    // which takes row i from registers (read here, before the refill copies
+    // are issued).
     __syncwarp(gmask);
+    if constexpr (!TRANS) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) xp[v] = xs[c0 + v];
+    } else {
+#pragma unroll
+      for (int q = 0; q < P; ++q) xp[q] = xs[q * RPP + gl / CPR];
+    }
+    // Every value taken from the slot has been consumed: refill it with row
+    // step + D of the chain.
+    {
+      const int s2 = step + D;
+      if (s2 < len) {  // uniform over the group
+        int b0, b1, jx[NPF];
+        int64_t bx[NPF];
+        row_of((s2 / G == step / G) ? cur : nxt, s2, b0, b1, jx, bx);
+        issue(i + D * task_dir_, slot, b0, b1, bx);
+      } else {
+        cp_async_commit();
+      }
+    }
    }
   }
 }
@@ -776,9 +944,15 @@ static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* 
 // ---------------------------------------------------------------- sweep launch
 template <int BS, typename VT, typename AT, bool TRANS, int POST>
 static int launch_sweep_t(bsp_handle_s* h, const SweepP<VT, AT>& p) {
-  static int grid = 0;
-  if (!grid) grid = persistent_grid(h, k_sweep<BS, VT, AT, TRANS, POST>, kSweepThreads, 0);
-  bsp::count_launch(), k_sweep<BS, VT, AT, TRANS, POST><<<grid, kSweepThreads, 0, h->stream>>>(p);
+  constexpr size_t smem = SweepCfg<BS, VT, AT, TRANS, POST>::kSmem;
+  static int per_sm = 0;
+  if (!per_sm) {
+    BSP_CUDA_TRY(cudaFuncSetAttribute(k_sweep<BS, VT, AT, TRANS, POST>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    per_sm = persistent_grid(h, k_sweep<BS, VT, AT, TRANS, POST>, kSweepThreads, smem) / h->num_sms;
+  }
+  bsp::count_launch(),
+      k_sweep<BS, VT, AT, TRANS, POST><<<h->num_sms * per_sm, kSweepThreads, smem, h->stream>>>(p);
   return BSP_OK;
 }
 
@@ -787,15 +961,18 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
   p.epoch = ++h->epoch;
   p.ticket = ticket;
   p.st = h->ws.status.get();
+  // 16-byte staging copies need aligned vectors (the matrix blocks always are)
+  p.stage_vec = (reinterpret_cast<uintptr_t>(p.rhs) % 16 == 0) &&
+                (p.xold == nullptr || reinterpret_cast<uintptr_t>(p.xold) % 16 == 0);
   BSP_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), h->stream));
   constexpr int V = Chunk<VT>::V;
   bool done = false;
   // blocks of more than 4 chunk passes per lane (bs 32 in FP64) would not fit
-  // the double-buffered registers: they use the generic kernel
+  // the per-lane registers of the staged kernel: they use the generic kernel
 #define BSP_SWEEP_CASE(B)                                          \
   case B:                                                          \
-    if constexpr (B % V == 0 && (B * B / V) / ((B * B / V) < 32 ? (B * B / V) : 32) <= 4) { \
-      launch_sweep_t<B, VT, AT, TRANS, POST>(h, p);                \
+    if constexpr (B % V == 0 && B * B / V <= 128) {               \
+      BSP_TRY((launch_sweep_t<B, VT, AT, TRANS, POST>(h, p)));     \
       done = true;                                                 \
     }                                                              \
     break;
