@@ -305,14 +305,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
         o.bx[u] = in ? (blk_ ? __ldg(blk_ + o.b0 + u) : (int64_t)(o.b0 + u)) : 0;
       }
     };
-    auto row_of = [&](const Win& w, int k, int& b0, int& b1, int (&jx)[NPF], int64_t (&bx)[NPF]) {
+    // Row k of window w: entry range, and (with_j) the first column indices.
+    // Block indices are shuffled only for indirect structures; contiguous
+    // ones use b0 + u.
+    auto row_of = [&](const Win& w, int k, bool with_j, int& b0, int& b1, int (&jx)[NPF],
+                      int64_t (&bx)[NPF]) {
       const int src = gbase + k % G;
       b0 = __shfl_sync(gmask, w.b0, src);
       b1 = __shfl_sync(gmask, w.b1, src);
 #pragma unroll
       for (int u = 0; u < NPF; ++u) {
-        jx[u] = __shfl_sync(gmask, w.jx[u], src);
-        bx[u] = __shfl_sync(gmask, w.bx[u], src);
+        if (with_j) jx[u] = __shfl_sync(gmask, w.jx[u], src);
+        bx[u] = blk_ ? __shfl_sync(gmask, w.bx[u], src) : (int64_t)(b0 + u);
       }
     };
     Win cur, nxt;
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       if (k < len) {  // uniform over the group (the shuffles need every lane)
         int b0, b1, jx[NPF];
         int64_t bx[NPF];
-        row_of(cur, k, b0, b1, jx, bx);
+        row_of(cur, k, false, b0, b1, jx, bx);
         issue(i0 + k * task_dir_, (int)((cons + k) % D), b0, b1, bx);
       } else {
         cp_async_commit();
@@ -342,7 +346,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
     const int prev = step > 0 ? i - task_dir_ : -1;
     int beg, end, jr[NPF];
     int64_t br[NPF];
-    row_of(cur, step, beg, end, jr, br);
+    row_of(cur, step, true, beg, end, jr, br);
     const int slot = (int)(cons % D);
     cp_async_wait<D - 1>();
     ++cons;
@@ -533,7 +537,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       if (s2 < len) {  // uniform over the group
         int b0, b1, jx[NPF];
         int64_t bx[NPF];
-        row_of((s2 / G == step / G) ? cur : nxt, s2, b0, b1, jx, bx);
+        row_of((s2 / G == step / G) ? cur : nxt, s2, false, b0, b1, jx, bx);
         issue(i + D * task_dir_, slot, b0, b1, bx);
       } else {
         cp_async_commit();
