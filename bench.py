@@ -113,7 +113,10 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """Process group of a torchrun launch (one rank per GPU).  The path does
+    not shard, so the group only carries the barrier and the max-over-ranks
+    timing; ``gloo`` runs the same host logic without GPUs."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -121,8 +124,9 @@ def dist_setup():
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
     return world, rank, local
 
 
@@ -141,7 +145,8 @@ def max_over_ranks(v: float, world: int) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -630,6 +635,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--learned-side", type=int, default=96)
     ap.add_argument("--learned-seeds", type=int, default=2)
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend under torchrun (gloo: the rank logic on CPU only)")
     args = ap.parse_args()
     if args.workload != "cfg1":
         if args.impl == "reference":
@@ -638,7 +645,7 @@ def main():
             return
         {"batch": run_batch, "mixed": run_mixed, "learned": run_learned}[args.workload](args)
         return
-    world, rank, local = dist_setup()
+    world, rank, local = dist_setup(args.dist_backend)
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "
                 f"1e-10; 3D {args.side}^3 7-point block stencil, 8x8 FP64 blocks, skew c=0.3")
     cores = os.cpu_count() or 1
