@@ -68,6 +68,11 @@ class Handle:
     def sync(self) -> None:
         check(self.lib.bsp_handle_sync(self.h), "bsp_handle_sync", self.h)
 
+    def set_spin_limit(self, polls: int = 1 << 22) -> None:
+        """Polls a device-side wait makes before it gives up with TIMEOUT
+        (default 2^22); a small value makes waits run out on purpose."""
+        check(self.lib.bsp_handle_set_spin_limit(self.h, int(polls)), "bsp_handle_set_spin_limit", self.h)
+
     @property
     def stream(self) -> int:
         return self.lib.bsp_handle_stream(self.h) or 0

@@ -155,6 +155,12 @@ int bsp_handle_create(int device, void* stream, bsp_handle_t* out) {
   return BSP_OK;
 }
 
+int bsp_handle_set_spin_limit(bsp_handle_t h, unsigned polls) {
+  if (!h || polls < 1) return BSP_INVALID;
+  h->spin_limit = polls;
+  return BSP_OK;
+}
+
 int bsp_handle_destroy(bsp_handle_t h) {
   if (!h) return BSP_OK;
   {

@@ -401,6 +401,7 @@ struct BContP {
   int* counter;   // iterations executed
   int* running;   // 1 while any pair runs (read by the host-driven mode)
   int cap;        // hard bound on iterations
+  const DevStatus* dev_st;  // device error word: a failed sweep ends the loop
 };
 
 // Decides whether another iteration runs; sets the graph's loop condition.
@@ -414,7 +415,9 @@ __global__ void k_bt_continue(BContP c, cudaGraphConditionalHandle hnd, int use_
     // replay after the end changes nothing)
     const int it = *c.counter + ((bump && *c.running) ? 1 : 0);
     *c.counter = it;
-    const int run = any && it < c.cap;
+    // a sweep that timed out (or any other device failure) ends the loop at
+    // once: the host reads the status after the launch
+    const int run = any && it < c.cap && *reinterpret_cast<const volatile int*>(&c.dev_st->code) == 0;
     *c.running = run;
     if (use_cond) cudaGraphSetConditional(hnd, run ? 1u : 0u);
   }
@@ -455,6 +458,7 @@ struct BSweepP {
   double* x;
   unsigned* ticket;
   DevStatus* st;
+  unsigned spin_limit;  // polls before a wait gives up with BSP_TIMEOUT
 };
 
 constexpr int kBSweepThreads = 256;
@@ -572,12 +576,12 @@ __global__ void __launch_bounds__(kBSweepThreads) k_bt_sweep(const BSweepP p) {
               pending |= is_sentinel(xv[r][v]);
             }
           }
-          if (pending && (++spins & 255u) == 0u) {
-            if (*reinterpret_cast<volatile int*>(&p.st->code) != 0) break;
-            if (spins > kSpinLimit) {
+          if (pending) {
+            if (++spins > p.spin_limit) {
               set_status(p.st, BSP_TIMEOUT, i);
               break;
             }
+            if ((spins & 255u) == 0u && *reinterpret_cast<volatile int*>(&p.st->code) != 0) break;
           }
         }
       };
@@ -829,6 +833,7 @@ BSweepP sweep_params(bsp_batch_s* B, BatchGroup& g, bool fwd) {
   p.dinv = pc->dinv.get();
   p.vals = pc->f_vals.get();
   p.st = B->h->ws.status.get();
+  p.spin_limit = B->h->spin_limit;
   if (fwd) {
     p.n_tasks = pc->n_task_lo;
     p.task_row = pc->task_lo_row.get();
@@ -949,6 +954,7 @@ BContP cont_params(bsp_batch_s* B, int max_iters) {
   c.counter = B->counter.get();
   c.running = B->counter.get() + 1;
   c.cap = max_iters + 2;
+  c.dev_st = B->h->ws.status.get();
   return c;
 }
 

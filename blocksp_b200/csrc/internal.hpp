@@ -56,6 +56,8 @@ struct Workspace {
   DevBuf<DevStatus> status;  // device error word
 };
 
+struct StreamSym;
+
 // Structure-only analysis behind a preconditioner (sorted factor pattern,
 // permutation, dependency levels, chain tasks).  It depends on the matrix
 // pattern alone, so it is computed once per matrix and kind and reused by
@@ -68,6 +70,8 @@ struct SymbolicCache {
   DevBuf<int> f_ptr, f_col, f_diag, order_lo, order_up, task_lo_row, task_lo_len, task_up_row,
       task_up_len, t_ptr, t_row, a_diag;
   DevBuf<int64_t> d_perm, t_blk;
+  // streamed layouts of the two sweeps (block sizes the streamed kernel takes)
+  std::shared_ptr<StreamSym> ss_lo, ss_up;
 };
 
 // Non-owning view of a scratch buffer (handle scratch; see bsp_handle_s).
@@ -108,6 +112,8 @@ struct bsp_handle_s {
   bsp::Workspace ws;
   std::string last_error;
   int epoch = 0;  // sync-free sweep epoch (flags hold the epoch of their last write)
+  // polls a device wait makes before it gives up with BSP_TIMEOUT
+  unsigned spin_limit = bsp::kSpinLimit;
   // staging buffers of the host-buffer entry points (grow-only, reused)
   bsp::DevBuf<double> stage_in, stage_out;
   // Grow-only device scratch of the solvers, by purpose.  Every call on a

@@ -37,7 +37,9 @@ ScratchAddr g_addr[kNoAllocMaxDevices];
 std::mutex g_addr_mu;
 
 // The names above are host-side stand-ins; the kernel needs the device
-// addresses, resolved once per device with that device current.
+// addresses, resolved once per device with that device current.  They stay
+// cached until exit, so they are stale after a cudaDeviceReset of that device
+// (the header says so: no calls on a device after resetting it).
 int scratch_for_current_device(ScratchAddr* out) {
   int dev = 0;
   BSP_CUDA_TRY(cudaGetDevice(&dev));

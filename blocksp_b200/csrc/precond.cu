@@ -44,22 +44,21 @@
 #include "reduce.cuh"
 #include "sentinel.cuh"
 #include "stage.cuh"
+#include "sweep_stream.hpp"
 
 namespace bsp {
 
 // ----------------------------------------------------------------- device wait
-__device__ __forceinline__ void wait_flag(const int* f, int epoch, DevStatus* st, int who) {
+__device__ __forceinline__ void wait_flag(const int* f, int epoch, DevStatus* st, int who, unsigned limit) {
   if (ld_acquire(f) == epoch) return;
   unsigned spins = 0;
   while (ld_acquire(f) != epoch) {
-    poll_pause(spins);
-    if ((++spins & 255u) == 0u) {
-      if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;  // already failed
-      if (spins > kSpinLimit) {
-        set_status(st, BSP_TIMEOUT, who);
-        return;
-      }
+    if (++spins > limit) {
+      set_status(st, BSP_TIMEOUT, who);
+      return;
     }
+    if ((spins & 255u) == 0u && *reinterpret_cast<volatile int*>(&st->code) != 0) return;  // already failed
+    poll_pause(spins);
   }
 }
 
@@ -95,6 +94,7 @@ template <typename VT, typename AT> struct SweepP {
   int epoch;
   unsigned* ticket;
   DevStatus* st;
+  unsigned spin_limit;  // polls before a wait gives up with BSP_TIMEOUT
   // Chains: task t covers rows task_row[t], task_row[t] + task_dir, ... (task_len[t]
   // rows), each depending on the one before it; the group keeps the previous
   // row's result in shared memory instead of waiting for its flag.  Null
@@ -262,12 +262,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(const SweepP<VT, AT> p)
       pending = false;
 #pragma unroll
       for (int v = 0; v < XV; ++v) pending |= is_sentinel(xv[v]);
-      if (pending && (++spins & 255u) == 0u) {
-        if (*reinterpret_cast<volatile int*>(&st_->code) != 0) break;  // already failed
-        if (spins > kSpinLimit) {
+      if (pending) {
+        if (++spins > p.spin_limit) {
           set_status(st_, BSP_TIMEOUT, who);
           break;
         }
+        if ((spins & 255u) == 0u && *reinterpret_cast<volatile int*>(&st_->code) != 0) break;  // already failed
       }
     }
   };
@@ -591,13 +591,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_generic(const SweepP<VT
             while (is_sentinel(xc)) {  // row j of this sweep not final yet
               poll_pause(spins);
               xc = ld_poll(src + (int64_t)j * bs + c);
-              if ((++spins & 255u) == 0u) {
-                if (*reinterpret_cast<volatile int*>(&p.st->code) != 0) break;
-                if (spins > kSpinLimit) {
-                  set_status(p.st, BSP_TIMEOUT, i);
-                  break;
-                }
+              if (++spins > p.spin_limit) {
+                set_status(p.st, BSP_TIMEOUT, i);
+                break;
               }
+              if ((spins & 255u) == 0u && *reinterpret_cast<volatile int*>(&p.st->code) != 0) break;
             }
           }
           acc = fma(m, xc, acc);
@@ -641,6 +639,7 @@ struct FactorP {
   int epoch;
   unsigned* ticket;
   DevStatus* st;
+  unsigned spin_limit;
 };
 
 constexpr int kFactorWarps = 4;
@@ -661,7 +660,7 @@ __global__ void __launch_bounds__(kFactorWarps * 32) k_factor(const FactorP p) {
     const int k = p.order ? __ldg(p.order + t) : t;
     const int beg = __ldg(p.ptr + k), dg = __ldg(p.diag + k), end = __ldg(p.ptr + k + 1);
     if (p.mode != FACT_DIAG) {
-      for (int e = beg; e < dg; ++e) wait_flag(p.flags + __ldg(p.col + e), p.epoch, p.st, k);
+      for (int e = beg; e < dg; ++e) wait_flag(p.flags + __ldg(p.col + e), p.epoch, p.st, k, p.spin_limit);
       for (int e = beg; e < dg; ++e) {
         const int i = __ldg(p.col + e);
         warp_copy_in(sA, p.vals + (int64_t)e * b2, b2);
@@ -856,6 +855,8 @@ static int sym_transfer(bsp_precond_s* pc, SymbolicCache& C, bool save) {
   BSP_SYM_FIELD(t_blk) BSP_SYM_FIELD(a_diag)
 #undef BSP_SYM_FIELD
   if (save) {
+    C.ss_lo = pc->ss_lo;
+    C.ss_up = pc->ss_up;
     C.h_perm = pc->h_perm;
     C.f_nnzb = pc->f_nnzb;
     C.n_lev_lo = pc->n_lev_lo;
@@ -864,6 +865,8 @@ static int sym_transfer(bsp_precond_s* pc, SymbolicCache& C, bool save) {
     C.n_task_up = pc->n_task_up;
     C.valid = true;
   } else {
+    pc->ss_lo = C.ss_lo;
+    pc->ss_up = C.ss_up;
     pc->h_perm = C.h_perm;
     pc->f_nnzb = C.f_nnzb;
     pc->n_lev_lo = C.n_lev_lo;
@@ -929,6 +932,7 @@ static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* 
   fp.epoch = ++h->epoch;
   fp.ticket = pc->ticket.get();
   fp.st = h->ws.status.get();
+  fp.spin_limit = h->spin_limit;
   const size_t smem = (size_t)kFactorWarps * 5 * pc->bs * pc->bs * sizeof(double);
   BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BSP_CUDA_TRY(cudaMemsetAsync(pc->ticket.get(), 0, sizeof(unsigned), h->stream));
@@ -965,6 +969,7 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
   p.epoch = ++h->epoch;
   p.ticket = ticket;
   p.st = h->ws.status.get();
+  p.spin_limit = h->spin_limit;
   // 16-byte staging copies need aligned vectors (the matrix blocks always are)
   p.stage_vec = (reinterpret_cast<uintptr_t>(p.rhs) % 16 == 0) &&
                 (p.xold == nullptr || reinterpret_cast<uintptr_t>(p.xold) % 16 == 0);
@@ -1040,6 +1045,17 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
   pc->n_lev_lo = level_order(n, true, lower_deps, order);
   BSP_TRY(upload(pc->order_lo, order));
   BSP_TRY(make_tasks(pc, true, n, lower_deps));
+  // streamed layouts of both sweeps (ILU0: unit L, then U with U_ii^-1;
+  // IChol0: L with L_ii^-1, then L^T with L_ii^-T)
+  const bool streamed = stream_supported(pc->bs);
+  std::vector<RowEntries> ent;
+  if (streamed) {
+    ent.assign(n, RowEntries());
+    for (int i = 0; i < n; ++i)
+      for (int e = ptr[i]; e < diag[i]; ++e) ent[i].emplace_back(col[e], (int64_t)e);
+    pc->ss_lo = std::make_shared<StreamSym>();
+    BSP_TRY(stream_build(n, true, stream_warps(pc->bs), ent, false, lower_only, false, *pc->ss_lo));
+  }
   if (!lower_only) {
     auto upper_deps = [&](int i, auto&& f) {
       for (int e = diag[i] + 1; e < ptr[i + 1]; ++e) f(col[e]);
@@ -1047,6 +1063,14 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
     pc->n_lev_up = level_order(n, false, upper_deps, order);
     BSP_TRY(upload(pc->order_up, order));
     BSP_TRY(make_tasks(pc, false, n, upper_deps));
+    if (streamed) {
+      for (int i = 0; i < n; ++i) {
+        ent[i].clear();
+        for (int e = diag[i] + 1; e < ptr[i + 1]; ++e) ent[i].emplace_back(col[e], (int64_t)e);
+      }
+      pc->ss_up = std::make_shared<StreamSym>();
+      BSP_TRY(stream_build(n, false, stream_warps(pc->bs), ent, false, true, false, *pc->ss_up));
+    }
   } else {
     // L^T backward: row i depends on rows j > i with L_ji present
     std::vector<int> tp(n + 1, 0);
@@ -1069,6 +1093,14 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
     pc->n_lev_up = level_order(n, false, trans_deps, order);
     BSP_TRY(upload(pc->order_up, order));
     BSP_TRY(make_tasks(pc, false, n, trans_deps));
+    if (streamed) {
+      for (int i = 0; i < n; ++i) {
+        ent[i].clear();
+        for (int t = tp[i]; t < tp[i + 1]; ++t) ent[i].emplace_back(trow[t], tblk[t]);
+      }
+      pc->ss_up = std::make_shared<StreamSym>();
+      BSP_TRY(stream_build(n, false, stream_warps(pc->bs), ent, true, true, true, *pc->ss_up));
+    }
     BSP_TRY(upload(pc->t_ptr, tp));
     BSP_TRY(upload(pc->t_row, trow));
     BSP_TRY(upload(pc->t_blk, tblk));
@@ -1143,6 +1175,11 @@ static int build_diag_inverse(bsp_precond_s* pc) {
                     pc->A->vals.get(), pc->n);
 }
 
+// The factors changed: every streamed copy of them is stale.
+static void stream_invalidate(bsp_precond_s* pc) {
+  for (int k = 0; k < 3; ++k) pc->sv_lo[k].valid = pc->sv_up[k].valid = false;
+}
+
 static int make_lowp_copies(bsp_precond_s* pc) {
   if (pc->precision == BSP_PREC_F64) return BSP_OK;
   const int b2 = pc->bs * pc->bs;
@@ -1169,6 +1206,7 @@ static int make_lowp_copies(bsp_precond_s* pc) {
 
 int precond_build(bsp_precond_s* pc) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
+  stream_invalidate(pc);
   BSP_TRY(take(pc->A, pc->dinv, (size_t)std::max(n, 1) * b2));
   BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
   BSP_TRY(take(pc->A, pc->ticket, 1));
@@ -1209,6 +1247,7 @@ __global__ void k_add_perm(int64_t nblk, int b2, const int64_t* __restrict__ per
 // order; the diagonal inverses are recomputed from the corrected U_ii.
 int precond_build_learned(bsp_precond_s* pc, const double* dF) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
+  stream_invalidate(pc);
   BSP_TRY(take(pc->A, pc->dinv, (size_t)std::max(n, 1) * b2));
   BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
   BSP_TRY(take(pc->A, pc->ticket, 1));
@@ -1244,6 +1283,33 @@ template <typename AT> static int fill_sentinel(bsp_handle_s* h, AT* x, int64_t 
         count, reinterpret_cast<unsigned*>(x));
   BSP_CUDA_TRY(cudaPeekAtLastError());
   return BSP_OK;
+}
+
+template <typename VT> constexpr int prec_of() {
+  return std::is_same<VT, double>::value ? BSP_PREC_F64 : std::is_same<VT, float>::value ? BSP_PREC_F32 : BSP_PREC_BF16;
+}
+
+// z = M^{-1} r through the streamed sweeps (sa: scratch for the forward
+// result).  The stream values of the precision are gathered on first use.
+template <typename VT>
+static int apply_streamed(bsp_precond_s* pc, const double* r, double* z, double* sa) {
+  bsp_handle_s* h = pc->h;
+  constexpr int prec = prec_of<VT>();
+  StreamVals& lo = pc->sv_lo[prec];
+  StreamVals& up = pc->sv_up[prec];
+  for (auto* sv : {&lo, &up}) {
+    if (sv->valid) continue;
+    const StreamSym& S = sv == &lo ? *pc->ss_lo : *pc->ss_up;
+    const size_t vb = stream_val_bytes(S, pc->bs, prec), db = stream_dval_bytes(S, pc->bs, prec);
+    if (sv->vals.n < vb) BSP_TRY(take(pc->A, sv->vals, vb));
+    if (db && sv->dvals.n < db) BSP_TRY(take(pc->A, sv->dvals, db));
+    BSP_TRY(stream_gather(h, S, pc->bs, prec, pc->f_vals.get(), pc->dinv.get(), *sv));
+  }
+  const int64_t nv = (int64_t)pc->n * pc->bs;
+  BSP_TRY(fill_sentinel(h, sa, nv));
+  BSP_TRY(stream_sweep(h, *pc->ss_lo, pc->bs, prec, lo, r, sa, pc->ticket.get()));
+  BSP_TRY(fill_sentinel(h, z, nv));
+  return stream_sweep(h, *pc->ss_up, pc->bs, prec, up, sa, z, pc->ticket.get());
 }
 
 // z = M^{-1} r (z may alias r).  Every sweep with dependencies writes into a
@@ -1310,6 +1376,9 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
     }
     case BSP_PC_ILU0:
     case BSP_PC_LEARNED_LU: {
+      if constexpr (std::is_same<AT, double>::value) {
+        if (pc->ss_lo && pc->ss_up) return apply_streamed<VT>(pc, r, z, sa);
+      }
       p.ptr = pc->f_ptr.get();
       p.idx = pc->f_col.get();
       p.diag = pc->f_diag.get();
@@ -1334,6 +1403,9 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
     }
     case BSP_PC_ICHOL0:
     case BSP_PC_LEARNED_LLT: {
+      if constexpr (std::is_same<AT, double>::value) {
+        if (pc->ss_lo && pc->ss_up) return apply_streamed<VT>(pc, r, z, sa);
+      }
       p.ptr = pc->f_ptr.get();
       p.idx = pc->f_col.get();
       p.diag = pc->f_diag.get();
@@ -1492,6 +1564,7 @@ int precond_learned_init(bsp_precond_s* pc) {
 // (both built on the same matrix) and gets fresh diagonal inverses.
 int precond_learned_refresh(bsp_precond_s* work, const bsp_precond_s* ilu, const double* dF) {
   if (work->f_nnzb != ilu->f_nnzb || work->n != ilu->n || work->bs != ilu->bs) return BSP_INVALID;
+  stream_invalidate(work);
   const int b2 = work->bs * work->bs;
   const int64_t tot = work->f_nnzb * b2;
   if (tot > 0)
@@ -1624,6 +1697,8 @@ int bsp_precond_destroy(bsp_precond_t pc) {
     for (int i = 0; i < 3; ++i) {
       give(A, pc->s64[i]);
       give(A, pc->s32[i]);
+      give(A, pc->sv_lo[i].vals); give(A, pc->sv_lo[i].dvals);
+      give(A, pc->sv_up[i].vals); give(A, pc->sv_up[i].dvals);
     }
   }
   delete pc;

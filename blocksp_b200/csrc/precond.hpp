@@ -2,6 +2,7 @@
 // single-system, batched and learned solvers).
 #pragma once
 #include "internal.hpp"
+#include "sweep_stream.hpp"
 
 struct bsp_precond_s {
   bsp_handle_t h = nullptr;
@@ -48,6 +49,12 @@ struct bsp_precond_s {
   // iterates and the copy of an in-place right-hand side
   bsp::DevBuf<double> s64[3];
   bsp::DevBuf<float> s32[3];
+  // streamed sweeps (ILU0 / IChol0 and the learned factors, FP64 vectors):
+  // the layout, shared with the matrix's symbolic cache, and its values per
+  // precision (index BSP_PREC_*), gathered from f_vals / dinv on first use
+  // after every change of the factors
+  std::shared_ptr<bsp::StreamSym> ss_lo, ss_up;
+  bsp::StreamVals sv_lo[3], sv_up[3];
 };
 
 namespace bsp {

@@ -1,0 +1,81 @@
+// sweep_stream.hpp — the streamed triangular sweep: host-side interface.
+//
+// A sweep of a block triangular factor (ILU0: unit-L forward, U backward with
+// the inverted diagonal; IChol0: L forward with L_ii^-1, L^T backward with
+// L_ii^-T) computes, in the reference's natural row order,
+//     x_r = D_r (rhs_r - sum_e B_e x_{j_e})
+// (blocksp_preconditioners.hpp:294-349 ILU0::invmul, :432-489 IChol0::invmul),
+// with D_r the identity for the unit-L sweep.  The streamed form lays every
+// block the sweep reads out once, in the order the device consumes it:
+//   * rows are grouped into chains (runs of consecutive rows, each depending
+//     on the one before; at most kStreamCmax rows), chains into super-tasks of
+//     W consecutive chains (one CTA, one warp per chain);
+//   * super-tasks are sorted by dependency level (the ticket order);
+//   * per row the entries are ordered external rows first, rows of the same
+//     super-task next, the chain's previous row last, and each entry carries a
+//     code: >= 0 an external row (published through global memory), -1 the
+//     chain's previous row (registers), <= -2 a row of another chain of the
+//     same CTA (shared memory);
+//   * the blocks (transposed where the sweep reads B^T) and the D blocks are
+//     stored contiguously in that order, in the precision of the solve.
+// What a row computes is unchanged; only when it runs and where its inputs
+// come from differ from the reference's loop.
+#pragma once
+#include <memory>
+#include <vector>
+#include "internal.hpp"
+
+namespace bsp {
+
+constexpr int kStreamEmax = 3;   // entries of a row staged in shared memory
+constexpr int kStreamCmax = 64;  // rows per chain (longer runs are split)
+
+// Symbolic part of one streamed sweep (depends on the matrix pattern only).
+struct StreamSym {
+  int n = 0, n_super = 0, n_chains = 0, W = 0, dir = 1;
+  int n_levels = 0;
+  int64_t n_ent = 0;
+  bool trans_blocks = false, has_d = false, trans_d = false;
+  DevBuf<int> super_beg;   // n_super + 1: chains of each super-task (ticket order)
+  DevBuf<int4> chains;     // {row0, len, q0 (first stream row), e0 (first entry)}
+  DevBuf<int4> rec;        // per stream row: {code0, code1, code2, n_entries}
+  DevBuf<int> codes;       // per entry (rows with more than kStreamEmax entries)
+  DevBuf<int64_t> src_blk; // per entry: block index in the factor's value array
+  DevBuf<int> q_row;       // per stream row: its block row (D gather)
+};
+
+// Entries of row i of the sweep: calls f(j, factor_block_index) per entry.
+using RowEntries = std::vector<std::pair<int, int64_t>>;
+
+// Builds the streamed layout of a sweep over n rows.  ent[i] lists row i's
+// entries; ascending: forward sweep (dependencies j < i).
+int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>& ent, bool trans_blocks,
+                 bool has_d, bool trans_d, StreamSym& S);
+
+// Block size, precision and warp count the streamed kernel supports.
+bool stream_supported(int bs);
+int stream_warps(int bs);
+
+// Per-precision values of one streamed sweep.
+struct StreamVals {
+  DevBuf<unsigned char> vals, dvals;  // blocks, D blocks (VT)
+  bool valid = false;
+};
+
+// Bytes of the stream's blocks and D blocks in precision prec.
+size_t stream_val_bytes(const StreamSym& S, int bs, int prec);
+size_t stream_dval_bytes(const StreamSym& S, int bs, int prec);
+
+// Gathers the stream's values (into buffers of at least the sizes above)
+// from the factor (FP64, factor entry order) and
+// the D blocks from dinv (FP64, row order), converted to the precision
+// `prec` (BSP_PREC_F64 / F32 / BF16).
+int stream_gather(bsp_handle_s* h, const StreamSym& S, int bs, int prec, const double* fvals,
+                  const double* dinv, StreamVals& out);
+
+// x = sweep(rhs) on h's stream.  x must hold the sentinel on entry; the
+// ticket is reset by this call.  prec selects the value type of `V`.
+int stream_sweep(bsp_handle_s* h, const StreamSym& S, int bs, int prec, const StreamVals& V,
+                 const double* rhs, double* x, unsigned* ticket);
+
+}  // namespace bsp

@@ -136,6 +136,14 @@ int bsp_handle_create(int device, void* stream, bsp_handle_t* out);
 int bsp_handle_destroy(bsp_handle_t h);
 int bsp_handle_sync(bsp_handle_t h);
 void* bsp_handle_stream(bsp_handle_t h);
+/* Failure detection (no counterpart in the reference, which never waits on
+ * another thread): every device-side wait of the sync-free sweeps and
+ * factorisations polls at most `polls` times (default 2^22, with a nanosleep
+ * back-off) before it gives up, records BSP_TIMEOUT with the block row, and
+ * returns; the launch then completes and the call reports BSP_TIMEOUT.  A
+ * small value makes the waits of a large sweep run out on purpose (tests).
+ * Applies to launches made after the call; polls >= 1. */
+int bsp_handle_set_spin_limit(bsp_handle_t h, unsigned polls);
 const char* bsp_status_string(int status);
 const char* bsp_last_error(bsp_handle_t h);
 int bsp_device_count(int* count);
@@ -194,8 +202,11 @@ int bsp_axpy_dev(bsp_handle_t h, int64_t n, double a, const double* x, double* y
  * array (about 32 KiB per GPU, held until exit): n is limited to 33,554,432
  * elements and larger n returns BSP_INVALID.  The first call on a device
  * resolves the scratch address (cudaGetSymbolAddress), so make it before any
- * stream capture.  Calls share the scratch: calls that overlap on the GPU
- * race, so serialise them (one stream, or events). */
+ * stream capture.  The resolved address is kept for the life of the
+ * process: after cudaDeviceReset (or anything else that destroys the
+ * device's primary context) it is stale, so do not call this function on a
+ * device again after resetting it.  Calls share the scratch: calls that
+ * overlap on the GPU race, so serialise them (one stream, or events). */
 int bsp_dot_noalloc(void* stream, int64_t n, const double* x, const double* y, double* out_dev);
 
 /* ---------------- preconditioners ----------------

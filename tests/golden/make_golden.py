@@ -12,11 +12,20 @@ converted to arrays) and the reference's infinity-norm errors on it, so the GPU
 can be checked against the reference's only known answer where the reference
 sources are not present.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Also stores the reference's solves of three full-size benchmark systems
+(``CONFIG_CASES``: the 64^2 bs4 IChol0-pCG system, the 64^3 bs8 ILU0-pGMRES(30)
+deflated-restart system and the 48^3 bs16 one): their residual histories,
+iteration counts, the norm of x and a fixed strided sample of x (the whole x
+for the 64^2 system), so the GPU solver is checked at full size.
+
+Run from the repository root:  python tests/golden/make_golden.py [--configs-only [NAME ...]]
+The reference sources are read from $BLOCKSP_REFERENCE (the LDG matrices under
+its test_mats/); the checker binary must have been built by oracle/Makefile.
 """
 from __future__ import annotations
 
 import json
+import os
 import subprocess
 import sys
 import tempfile
@@ -30,7 +39,19 @@ from blocksp_b200 import systems  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 EXE = ROOT / "oracle" / "_ref" / "ref_solve_hist"
-REF_MATS = Path("/root/reference/test_mats")
+REF_MATS = Path(os.environ.get("BLOCKSP_REFERENCE", "")) / "test_mats"
+
+# Full-size systems: name -> (system factory, B, D, solver, extra args, full x?)
+CONFIG_CASES = {
+    "cfg0_ichol0_pcg_2d64_bs4": ("config0", 2, 2, "ichol0_pcg", ["--tol", "1e-10", "--maxit", "2000"], True),
+    "cfg1_ilu0_pgmres_dr_3d64_bs8": ("config1", 4, 2, "ilu0_pgmres",
+                                     ["--tol", "1e-10", "--maxit", "5000", "--restart", "30", "--k", "10"],
+                                     False),
+    "cfg2b_ilu0_pgmres_dr_3d48_bs16": ("config2b", 8, 2, "ilu0_pgmres",
+                                       ["--tol", "1e-10", "--maxit", "5000", "--restart", "30", "--k", "10"],
+                                       False),
+}
+X_SAMPLE_STRIDE = 997  # a prime stride, so the sample visits every block-row position
 
 # name: (dims, bs, seed, skew, B, D, solver, extra args)
 CASES = {
@@ -60,10 +81,8 @@ def system_for(dims, bs, seed, skew, nrhs=1):
     return systems.grid_system(dims, bs, seed=seed, skew=skew, nrhs=nrhs)
 
 
-def run_case(name, spec, tmp: Path) -> dict:
-    dims, bs, seed, skew, B, D, solver, extra = spec
-    nrhs = D if solver == "bsmv_multi" else 1
-    s = system_for(dims, bs, seed, skew, nrhs)
+def run_ref(s, name, B, D, solver, extra, tmp: Path):
+    """Run the reference on system s; returns (x, residual history, iterations)."""
     f = tmp / f"{name}.bsps"
     systems.write_bsr(f, s)
     xo = tmp / f"{name}.x"
@@ -81,12 +100,44 @@ def run_case(name, spec, tmp: Path) -> dict:
             hist.append(float(p[2]))
         elif line.startswith("pCG iters") or line.startswith("pGMRES iters"):
             iters = int(p[2])
-    x = systems.read_vec(xo)
+    return systems.read_vec(xo), np.array(hist), iters
+
+
+def run_case(name, spec, tmp: Path) -> dict:
+    dims, bs, seed, skew, B, D, solver, extra = spec
+    nrhs = D if solver == "bsmv_multi" else 1
+    s = system_for(dims, bs, seed, skew, nrhs)
+    x, hist, iters = run_ref(s, name, B, D, solver, extra, tmp)
     meta = {"dims": list(dims), "bs": bs, "seed": seed, "skew": skew, "B": B, "D": D,
             "solver": solver, "args": extra}
-    np.savez_compressed(OUT / f"{name}.npz", x=x, hist=np.array(hist), iters=np.array(iters),
+    np.savez_compressed(OUT / f"{name}.npz", x=x, hist=hist, iters=np.array(iters),
                         meta=np.array(json.dumps(meta)))
     return {"name": name, "iters": iters, "hist_len": len(hist)}
+
+
+def run_config_case(name, spec, tmp: Path) -> dict:
+    factory, B, D, solver, extra, full_x = spec
+    s = getattr(systems, factory)()
+    x, hist, iters = run_ref(s, name, B, D, solver, extra, tmp)
+    sample_idx = np.arange(0, x.size, X_SAMPLE_STRIDE, dtype=np.int64)
+    out = {"hist": hist, "iters": np.array(iters), "x_norm": np.array(np.linalg.norm(x)),
+           "x_sample_idx": sample_idx, "x_sample": x[sample_idx],
+           "meta": np.array(json.dumps({"system": factory, "n": s.n, "bs": s.bs, "B": B, "D": D,
+                                        "solver": solver, "args": extra}))}
+    if full_x:
+        out["x"] = x
+    if solver == "ichol0_pcg":
+        # pCG's recursive residual is chaotic at rounding level: the oracle's
+        # per-step spread under 1e-15 relative perturbations (three trials) is
+        # stored with the history, since recomputing it takes minutes of numpy
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle.blocksp_oracle as O
+        from parity import cg_envelope
+        Ao = O.BSR.from_system(s)
+        tol, maxit = float(extra[extra.index("--tol") + 1]), int(extra[extra.index("--maxit") + 1])
+        out["hist_envelope"] = cg_envelope(Ao, s.b, tol, O.IChol0(Ao), maxit, hist)
+    np.savez_compressed(OUT / f"{name}.npz", **out)
+    return {"name": name, "iters": iters, "hist_len": len(hist), "x_norm": float(np.linalg.norm(x))}
 
 
 def ldg_fixture() -> None:
@@ -128,10 +179,17 @@ def ldg_fixture() -> None:
 def main():
     if not EXE.exists():
         sys.exit("build the reference checker first: make -C oracle")
+    configs_only = "--configs-only" in sys.argv
     with tempfile.TemporaryDirectory() as d:
-        for name, spec in CASES.items():
-            print(run_case(name, spec, Path(d)))
-    ldg_fixture()
+        if not configs_only:
+            for name, spec in CASES.items():
+                print(run_case(name, spec, Path(d)))
+        only = [a for a in sys.argv[1:] if not a.startswith("--")]
+        for name, spec in CONFIG_CASES.items():
+            if not only or name in only:
+                print(run_config_case(name, spec, Path(d)), flush=True)
+    if not configs_only:
+        ldg_fixture()
 
 
 if __name__ == "__main__":
