@@ -38,13 +38,22 @@ sys.path.insert(0, str(ROOT))
 METRIC = "time-to-1e-10 FP64 residual: learned/mixed vs plain GPU Krylov; bsmv HBM GB/s"
 FALLBACK_HBM_GBS = 6650.0
 TOL = 1e-10
-# The reference's own pGMRES iteration count on the default system (seed 1,
-# 64^3), measured by running the reference build to completion on it
-# (ILU0_pGMRES(A, 1e-10, 5000, 30, 10): 63 iterations, true residual 5.82e-11;
-# 4.0 s set-up + 50.0 s solve on one core of the build container).  The CPU
-# arms time a bounded sample (set-up + a few iterations) on the box and
-# extrapolate to this count.
-REF_ITERS = {64: 63}
+GOLDEN = ROOT / "tests" / "golden"
+# ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one ILU0
+# application at 64^3 with 8x8 FP64 blocks (its two streamed sweeps), from the
+# committed capture summarised in profiles/sweep_stream_ilu0_64cube_bs8.md
+ILU_APPLY_TRAFFIC_64 = None
+
+
+def reference_golden(side: int) -> dict | None:
+    """The reference's own solve of the default system (seed 1, side^3):
+    ILU0_pGMRES(A, 1e-10, 5000, 30, 10) run to completion by the reference
+    build, stored as a test fixture (iterations and residual history)."""
+    f = GOLDEN / "cfg1_ilu0_pgmres_dr_3d64_bs8.npz"
+    if side != 64 or not f.exists():
+        return None
+    d = np.load(f)
+    return {"iters": int(d["iters"]), "hist": d["hist"]}
 
 
 def read_peaks() -> tuple[float, str]:
@@ -164,9 +173,13 @@ def bsmv_bytes(n: int, bs: int, nnzb: int, nrhs: int = 1, val_bytes: int = 8, ve
 
 def ilu_apply_bytes(n: int, bs: int, nnzb: int, val_bytes: int = 8) -> int:
     """Algorithmic bytes of one ILU0 application (forward + backward sweep):
-    every factor block and inverted diagonal block once, the structure once,
-    the right-hand side read and the result written in each sweep."""
-    return (nnzb + n) * bs * bs * val_bytes + 2 * (nnzb * 4 + (n + 1) * 8) + 4 * n * bs * 8
+    the strictly-lower blocks (forward) and strictly-upper blocks plus the
+    inverted diagonal blocks (backward) once each (the diagonal U blocks are
+    not read: their inverses replace them), one column index per strict
+    block, a row pointer per row and sweep, and in each sweep the right-hand
+    side read and the result written."""
+    strict = nnzb - n
+    return (strict + n) * bs * bs * val_bytes + strict * 4 + 2 * (n + 1) * 4 + 4 * n * bs * 8
 
 
 # --------------------------------------------------------------------- GPU arm
@@ -208,6 +221,11 @@ def run_gpu(args, world, rank, local):
                 "refinements": info["n_outer"], "restarts": info["n_restarts"],
                 "true_rel_res": info["true_rel_res"], "status": info["status"]}
 
+    # parity run (untimed): the reference's method and stopping rule, whose
+    # residual history is compared with the reference's own solve of this system
+    pc = bsp.ILU0(A)
+    _, pinfo, phist = bsp.pGMRES(A, b, TOL, pc, 5000, 30, 10, return_info=True)
+    pc.close()
     variants = {k: v for k, v in {"plain_f64": _lib.PREC_F64, "mixed_f32": _lib.PREC_F32}.items()
                 if k in args.variants.split(",")}
     results = {}
@@ -260,34 +278,48 @@ def run_gpu(args, world, rank, local):
         h.close()
         return {"n": n, "bs": bs, "nnzb": nnzb, "results": results, "best": best, "e2e_s": float("nan"),
                 "bsmv_ms": bsmv_ms, "ilu_ms": ilu_ms, "levels": levels, "peak": peak,
-                "peak_kind": peak_kind, "clocks": clocks, "launches": launches, "x_norm": 0.0}
+                "peak_kind": peak_kind, "clocks": clocks, "launches": launches, "x_norm": 0.0,
+                "hist_f64": list(phist), "iters_f64": pinfo["iters"]}
     # Inputs in pinned host memory (numpy views of page-locked tensors); one
     # untimed call, then the mean over the timed calls.  Each call uploads the
     # matrix and right-hand side, builds ILU0, solves and reads x back.
     rp_h, ci_h, va_h, b_h = (
         pinned_copy(a) for a in (sysm.row_ptr.astype(np.int32), sysm.col_idx.astype(np.int32), sysm.vals, sysm.b))
 
+    parts = {"matrix_create_s": 0.0, "precond_create_s": 0.0, "solve_s": 0.0, "release_s": 0.0}
+
     def e2e_call():
+        t = [time.perf_counter()]
         A2 = bsp.Matrix(rp_h, ci_h, va_h, bs, handle=h)
+        t.append(time.perf_counter())
         pc2 = bsp.ILU0(A2)
+        t.append(time.perf_counter())
         out = bsp.pGMRES(A2, b_h, TOL, pc2, 5000, 30, 10, stop_rule=_lib.STOP_TRUE_RESIDUAL,
                          precision=variants[best])
+        t.append(time.perf_counter())
         pc2.close()
         A2.close()
+        t.append(time.perf_counter())
+        for k, key in enumerate(parts):
+            parts[key] += t[k + 1] - t[k]
         return out
 
     e2e_call()
+    for key in parts:
+        parts[key] = 0.0
     e2e_steps = max(1, args.steps)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         xh = e2e_call()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
+    e2e_parts = {k: v / e2e_steps for k, v in parts.items()}
     A.close()
     h.close()
     return {
         "n": n, "bs": bs, "nnzb": nnzb, "results": results, "best": best, "e2e_s": e2e_s,
         "bsmv_ms": bsmv_ms, "ilu_ms": ilu_ms, "levels": levels, "peak": peak, "peak_kind": peak_kind,
         "clocks": clocks, "launches": launches, "x_norm": float(np.linalg.norm(xh)),
+        "hist_f64": list(phist), "iters_f64": pinfo["iters"], "e2e_parts": e2e_parts,
     }
 
 
@@ -298,31 +330,45 @@ def ref_binary() -> Path | None:
     return p if p.exists() else None
 
 
-def cpu_reference_sample(side: int, sample_iters: int, budget_s: float = 25.0) -> dict | None:
-    """The reference's CPU ILU0_pGMRES on the same system, a bounded sample:
-    ILU0 set-up plus the first `sample_iters` pGMRES iterations, timed by the
-    reference build itself; returns set-up and per-iteration seconds."""
+def cpu_reference_full(side: int, runs: int = 1, budget_s: float = 150.0) -> dict | None:
+    """The reference's CPU ILU0_pGMRES(A, 1e-10, 5000, 30, 10) on the same
+    system, run to completion by the reference build (its own set-up and
+    solve timers): at least one full run, more while the budget lasts, up to
+    `runs`.  Returns the mean set-up, solve and total seconds, the iteration
+    count and the number of runs."""
     exe = ref_binary()
     if exe is None:
         return None
     from blocksp_b200 import systems
     s = systems.config1(seed=1, side=side)
+    done = []
     with tempfile.TemporaryDirectory() as d:
         f = Path(d) / "sys.bsps"
         systems.write_bsr(f, s)
         cmd = [str(exe), str(f), "--B", "4", "--D", "2", "--solver", "ilu0_pgmres", "--tol", "1e-10",
-               "--maxit", str(sample_iters), "--restart", "30", "--k", "10", "--time"]
+               "--maxit", "5000", "--restart", "30", "--k", "10", "--time", "--print-iters"]
         env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
-        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=budget_s * 20)
-    out = {}
-    for line in r.stdout.splitlines():
-        if line.startswith("TIME "):
-            k, v = line.split()[1:3]
-            out[k] = float(v)
-    if "setup_s" not in out or "solve_s" not in out:
+        t_start = time.time()
+        while len(done) < max(1, runs):
+            r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+            out = {}
+            for line in r.stdout.splitlines():
+                if line.startswith("TIME "):
+                    k, v = line.split()[1:3]
+                    out[k] = float(v)
+                elif line.startswith("pGMRES iters"):
+                    out["iters"] = int(line.split()[2])
+            if "setup_s" not in out or "solve_s" not in out:
+                break
+            done.append(out)
+            per = (time.time() - t_start) / len(done)
+            if time.time() - t_start + per > budget_s:
+                break
+    if not done:
         return None
-    out["per_iter_s"] = out["solve_s"] / max(1, sample_iters + 1)
-    return out
+    mean = lambda k: float(np.mean([o[k] for o in done]))  # noqa: E731
+    return {"setup_s": mean("setup_s"), "solve_s": mean("solve_s"), "total_s": mean("setup_s") + mean("solve_s"),
+            "iters": done[-1].get("iters"), "runs": len(done)}
 
 
 # ----------------------------------------------------------------- batch workload
@@ -625,7 +671,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--side", type=int, default=64)
     ap.add_argument("--bsmv-reps", type=int, default=50)
-    ap.add_argument("--cpu-sample-iters", type=int, default=8)
+    ap.add_argument("--cpu-budget", type=float, default=150.0,
+                    help="reference arm: seconds of full CPU solves to run (at least one)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="plain_f64,mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
@@ -649,31 +696,31 @@ def main():
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "
                 f"1e-10; 3D {args.side}^3 7-point block stencil, 8x8 FP64 blocks, skew c=0.3")
     cores = os.cpu_count() or 1
+    n_rows = args.side ** 3
+    nnzb = n_rows + 2 * 3 * (args.side - 1) * args.side ** 2
+    config = {"workload": workload, "n_block_rows": n_rows, "nnzb": nnzb, "bs": 8,
+              "l2": f"inputs larger than L2 ({nnzb * 64 * 8 / 1e6:.0f} MB of matrix blocks)",
+              "parallelism": "replicas"}
 
     if args.impl == "reference":
         if rank != 0:
             return
-        cb = cpu_reference_sample(args.side, args.cpu_sample_iters)
+        cb = cpu_reference_full(args.side, runs=args.steps, budget_s=args.cpu_budget)
         if cb is None:
             print(json.dumps({"impl": "reference", "unavailable":
                               "reference build oracle/_ref/ref_solve missing (run make -C oracle)"}))
             return
-        iters = REF_ITERS.get(args.side)
-        if iters is None:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              f"no measured reference iteration count for side {args.side}"}))
-            return
-        est = cb["setup_s"] + cb["per_iter_s"] * iters
-        line = {"metric": METRIC, "impl": "reference", "value": est, "unit": "s",
-                "higher_is_better": False, "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "config": {"workload": workload},
-                "cpu_baseline": {"value": est, "unit": "s", "cores": 1, "cores_available": cores,
-                                 "kind": "reference",
-                                 "sample": f"reference build: ILU0 set-up ({cb['setup_s']:.2f} s) + "
-                                           f"{args.cpu_sample_iters} pGMRES iterations "
-                                           f"({cb['per_iter_s']:.3f} s each), extrapolated to the "
-                                           f"reference's {iters} iterations on this system"},
-                "e2e": {"value": est, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        sample = (f"full run{'s' if cb['runs'] > 1 else ''}: {cb['runs']} complete reference ILU0_pGMRES(A, 1e-10, "
+                  f"5000, 30, 10) solve{'s' if cb['runs'] > 1 else ''} ({cb['iters']} iterations), mean set-up "
+                  f"{cb['setup_s']:.2f} s + solve {cb['solve_s']:.2f} s; single-threaded by construction, so one "
+                  "core; runs stop once the time budget is spent, so steps counts the runs made")
+        line = {"metric": METRIC, "impl": "reference", "value": cb["total_s"], "unit": "s",
+                "higher_is_better": False, "n_gpus": args.gpus, "steps": cb["runs"],
+                "warmup": 0, "ms_per_step": cb["total_s"] * 1e3, "config": config,
+                "iterations": cb["iters"],
+                "cpu_baseline": {"value": cb["total_s"], "unit": "s", "cores": 1, "cores_available": cores,
+                                 "kind": "reference", "sample": sample},
+                "e2e": {"value": cb["total_s"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
 
@@ -683,37 +730,47 @@ def main():
     best = r["results"][r["best"]]
     n, bs, nnzb = r["n"], r["bs"], r["nnzb"]
     bsmv_gbs = bsmv_bytes(n, bs, nnzb) / (r["bsmv_ms"] * 1e-3) / 1e9
-    ilu_gbs = ilu_apply_bytes(n, bs, nnzb) / (r["ilu_ms"] * 1e-3) / 1e9
+    ilu_b = ilu_apply_bytes(n, bs, nnzb)
+    ilu_gbs = ilu_b / (r["ilu_ms"] * 1e-3) / 1e9
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cb = cpu_reference_sample(args.side, args.cpu_sample_iters)
+        cb = cpu_reference_full(args.side, runs=1)
         if cb is not None:
-            iters = REF_ITERS.get(args.side, r["results"][r["best"]]["iters"])
-            cpu = {"value": cb["setup_s"] + cb["per_iter_s"] * iters, "unit": "s", "cores": 1,
-                   "cores_available": cores, "kind": "reference",
-                   "sample": f"reference ILU0 set-up ({cb['setup_s']:.2f} s) + {args.cpu_sample_iters} "
-                             f"pGMRES iterations ({cb['per_iter_s']:.3f} s each), extrapolated to the "
-                             f"{iters} iterations the same method takes"}
+            cpu = {"value": cb["total_s"], "unit": "s", "cores": 1, "cores_available": cores, "kind": "reference",
+                   "sample": f"full run: one complete reference ILU0_pGMRES(A, 1e-10, 5000, 30, 10) solve of "
+                             f"the same system ({cb['iters']} iterations), set-up {cb['setup_s']:.2f} s + solve "
+                             f"{cb['solve_s']:.2f} s; single-threaded by construction"}
+    gold = reference_golden(args.side)
+    parity = None
+    if gold is not None:
+        h = np.asarray(r["hist_f64"])
+        g = gold["hist"]
+        k = min(len(h), len(g))
+        parity = {"reference_iters": gold["iters"], "gpu_iters": r["iters_f64"],
+                  "history_max_abs_dev": float(np.abs(h[:k] / h[0] - g[:k] / g[0]).max())}
     xbytes = n * bs * 8
+    traffic = ILU_APPLY_TRAFFIC_64 if args.side == 64 else None
     line = {
         "metric": METRIC,
         "value": best["total_s"] / args.gpus if args.gpus > 1 else best["total_s"],
         "unit": "s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": best["total_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 64^3 7-point block stencil)",
-        "config": {"workload": workload, "n_block_rows": n, "nnzb": nnzb, "bs": bs,
-                   "best_variant": r["best"],
-                   "l2": "inputs larger than L2 (927 MB of matrix blocks)", "parallelism": "replicas"},
+        "vs_baseline": None, "dtype": "f64", "data": f"synthetic (seeded {args.side}^3 7-point block stencil)",
+        "config": {**config, "best_variant": r["best"]},
         "variants": r["results"],
-        "bsmv": {"ms": r["bsmv_ms"], "gbs": bsmv_gbs, "frac_of_peak": bsmv_gbs / r["peak"]},
-        "ilu0_apply": {"ms": r["ilu_ms"], "gbs_effective": ilu_gbs, "frac_of_peak": ilu_gbs / r["peak"],
+        "parity_vs_reference": parity,
+        "bsmv": {"kernel": "k_bsmv<8,double,double,1>", "ms": r["bsmv_ms"], "gbs": bsmv_gbs,
+                 "frac_of_peak": bsmv_gbs / r["peak"], "algorithmic_bytes": bsmv_bytes(n, bs, nnzb)},
+        "ilu0_apply": {"ms": r["ilu_ms"], "gbs": ilu_gbs, "frac_of_peak": ilu_gbs / r["peak"],
+                       "algorithmic_bytes": ilu_b,
                        "levels": [r["levels"]["levels_lower"], r["levels"]["levels_upper"]]},
-        "roofline": {"bound": "hbm", "kernel": "k_bsmv<8,double,double,1>", "achieved": bsmv_gbs,
-                     "peak": r["peak"], "unit": "GB/s", "frac": bsmv_gbs / r["peak"], "traffic": 960.9e6,
-                     "peak_source": r["peak_kind"]},
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_ssweep<8,double> x2 (one ILU0 application: forward + backward streamed sweeps)",
+                     "achieved": ilu_gbs, "peak": r["peak"], "unit": "GB/s", "frac": ilu_gbs / r["peak"],
+                     "traffic": traffic, "algorithmic_bytes": ilu_b, "peak_source": r["peak_kind"]},
         "e2e": {"value": r["e2e_s"], "unit": "s", "h2d_bytes_per_step": nnzb * bs * bs * 8 + nnzb * 4
-                + (n + 1) * 4 + xbytes, "d2h_bytes_per_step": xbytes},
+                + (n + 1) * 4 + xbytes, "d2h_bytes_per_step": xbytes, "parts": r.get("e2e_parts")},
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
         "cpu_baseline": cpu,

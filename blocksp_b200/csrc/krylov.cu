@@ -16,8 +16,10 @@
 //     invariant subspace, P_{k+1}, c_r, H_new) runs on one GPU warp in
 //     small_dense.h (working set in shared memory), and Qn <- Qn P_{k+1} is a tall-skinny in-place kernel.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 #include "reduce.cuh"
+#include "sentinel.cuh"
 #include "small_dense.h"
 
 struct bsp_precond_s;
@@ -254,6 +256,154 @@ struct MgsLastBody {
     st4(v, e, n, vv);
   }
 };
+
+// ---- modified Gram-Schmidt of one Arnoldi column in one persistent launch
+// (one_arnoldi, blocksp_solvers.hpp:109-136):
+//   for i = 0..j: H(i, j) = q_i . v;  v -= H(i, j) q_i
+//   H(j+1, j) = ||v||;  q_{j+1} = v / H(j+1, j) (unless below zero_thresh)
+// One CTA per SM, all co-resident (cooperative launch).  Each CTA keeps its
+// slice of v in registers for the whole column and the slice of the last
+// basis vector in shared memory, so a pass reads one basis vector from HBM
+// (the per-pass launch form reads v and q_{i-1}, q_i and writes v back).
+// Passes are separated by a bounded grid barrier; every CTA sums the per-CTA
+// partials in index order, so H is bit-reproducible.  The update and the dot
+// use the same fma sequence as the per-pass form, in MGS order.
+constexpr int kMgsThreads = 1024;
+
+struct MgsP {
+  int64_t len;
+  int64_t slice;           // elements per CTA
+  const double* v;         // M^-1 A q_j
+  double* const* Q;        // basis table
+  int j;                   // column
+  double* H;               // (m+1) x m, row-major, leading dimension ldh
+  int ldh;
+  const KHead* head;       // zero_thresh
+  double* partials;        // (j+2) x gridDim.x
+  unsigned* bar;           // barrier counter (0 at launch)
+  unsigned spin_limit;
+  DevStatus* st;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Sum over the CTA (every thread gets the result).
+__device__ __forceinline__ double cta_sum_1024(double a, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (lane == 0) red[warp] = a;
+  __syncthreads();
+  if (warp == 0) {
+    double t = red[lane];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) red[32] = t;
+  }
+  __syncthreads();
+  const double r = red[32];
+  __syncthreads();
+  return r;
+}
+
+// Grid barrier number `gen` (1, 2, ...): bounded spin, BSP_TIMEOUT on expiry.
+__device__ __forceinline__ void mgs_barrier(const MgsP& p, unsigned gen) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(p.bar, 1u);
+    const unsigned target = gen * gridDim.x;
+    unsigned spins = 0;
+    while (ld_acquire_u32(p.bar) < target) {
+      if (++spins > p.spin_limit) {
+        set_status(p.st, BSP_TIMEOUT, -1);
+        break;
+      }
+      poll_pause(spins);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Sum of the gridDim.x partials of one pass, in index order (same in every CTA).
+__device__ __forceinline__ double grid_total(const double* part, double* red) {
+  if (threadIdx.x < 32) {
+    double a = 0.0;
+    for (int c = threadIdx.x; c < (int)gridDim.x; c += 32) a += __ldcg(part + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) red[33] = a;
+  }
+  __syncthreads();
+  const double r = red[33];
+  __syncthreads();
+  return r;
+}
+
+template <int NPT>
+__global__ void __launch_bounds__(kMgsThreads, 1) k_mgs(const MgsP p) {
+  extern __shared__ double qs[];  // this CTA's slice of the last basis vector
+  __shared__ double red[34];
+  const int t = threadIdx.x;
+  const int64_t beg = (int64_t)blockIdx.x * p.slice;
+  const int nloc = (int)((beg + p.slice < p.len ? beg + p.slice : p.len) - beg);  // may be <= 0
+  double v[NPT];
+  {
+    const double* vb = p.v + beg;
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int o = t + k * kMgsThreads;
+      v[k] = o < nloc ? vb[o] : 0.0;
+    }
+  }
+  double h = 0.0;
+  unsigned gen = 0;
+  for (int i = 0; i <= p.j; ++i) {
+    const double* qb = p.Q[i] + beg;
+    double a = 0.0;
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int o = t + k * kMgsThreads;
+      if (o < nloc) {
+        if (i > 0) v[k] = fma(-h, qs[o], v[k]);
+        const double q = __ldcs(qb + o);
+        qs[o] = q;
+        a = fma(q, v[k], a);
+      }
+    }
+    a = cta_sum_1024(a, red);
+    if (t == 0) p.partials[(size_t)i * gridDim.x + blockIdx.x] = a;
+    mgs_barrier(p, ++gen);
+    h = grid_total(p.partials + (size_t)i * gridDim.x, red);
+    if (blockIdx.x == 0 && t == 0) p.H[(size_t)i * p.ldh + p.j] = h;
+  }
+  double a = 0.0;
+#pragma unroll
+  for (int k = 0; k < NPT; ++k) {
+    const int o = t + k * kMgsThreads;
+    if (o < nloc) {
+      v[k] = fma(-h, qs[o], v[k]);
+      a = fma(v[k], v[k], a);
+    }
+  }
+  a = cta_sum_1024(a, red);
+  if (t == 0) p.partials[(size_t)(p.j + 1) * gridDim.x + blockIdx.x] = a;
+  mgs_barrier(p, ++gen);
+  const double nrm = sqrt(fabs(grid_total(p.partials + (size_t)(p.j + 1) * gridDim.x, red)));
+  if (blockIdx.x == 0 && t == 0) p.H[(size_t)(p.j + 1) * p.ldh + p.j] = nrm;
+  if (fabs(nrm) < p.head->zero_thresh) return;  // breakdown: the basis is not extended
+  double* qn = p.Q[p.j + 1] + beg;
+#pragma unroll
+  for (int k = 0; k < NPT; ++k) {
+    const int o = t + k * kMgsThreads;
+    if (o < nloc) qn[o] = v[k] / nrm;
+  }
+}
 
 struct GPtrs {
   KHead* head;
@@ -499,6 +649,55 @@ __global__ void k_gm_pure_restart(GPtrs g) {
 }
 
 // ------------------------------------------------------------------ host helpers
+// One persistent MGS launch for column j when the slice of v fits the
+// registers of one CTA per SM (else returns 1: the per-pass form is used).
+template <int NPT>
+static int launch_mgs_t(bsp_handle_s* h, MgsP& p, int grid) {
+  const size_t smem = (size_t)NPT * kMgsThreads * sizeof(double);
+  static bool ok = false;
+  if (!ok) {
+    BSP_CUDA_TRY(cudaFuncSetAttribute(k_mgs<NPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    BSP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgs<NPT>, kMgsThreads, smem));
+    if (per_sm < 1) return 1;
+    ok = true;
+  }
+  void* args[] = {&p};
+  bsp::count_launch();
+  BSP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_mgs<NPT>, grid, kMgsThreads, args, smem, h->stream));
+  return BSP_OK;
+}
+
+static int launch_mgs(bsp_handle_s* h, int64_t len, const double* v, double* const* Q, int j, double* H, int ldh,
+                      const KHead* head, double* partials, unsigned* bar) {
+  const int grid = h->num_sms;
+  const int64_t per_thread = (len + (int64_t)grid * kMgsThreads - 1) / ((int64_t)grid * kMgsThreads);
+  MgsP p{};
+  p.len = len;
+  p.v = v;
+  p.Q = Q;
+  p.j = j;
+  p.H = H;
+  p.ldh = ldh;
+  p.head = head;
+  p.partials = partials;
+  p.bar = bar;
+  p.spin_limit = h->spin_limit;
+  p.st = h->ws.status.get();
+  BSP_CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(unsigned), h->stream));
+  auto run = [&](auto npt) -> int {
+    constexpr int N = decltype(npt)::value;
+    p.slice = (int64_t)N * kMgsThreads;
+    if (p.slice * grid < len) return 1;
+    return launch_mgs_t<N>(h, p, grid);
+  };
+  if (per_thread <= 4) return run(std::integral_constant<int, 4>{});
+  if (per_thread <= 8) return run(std::integral_constant<int, 8>{});
+  if (per_thread <= 16) return run(std::integral_constant<int, 16>{});
+  if (per_thread <= 24) return run(std::integral_constant<int, 24>{});
+  return 1;
+}
+
 static int read_head(bsp_handle_s* h, const KHead* d, KHead* out) {
   BSP_CUDA_TRY(cudaMemcpyAsync(out, d, sizeof(KHead), cudaMemcpyDeviceToHost, h->stream));
   BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -662,6 +861,10 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
   BSP_TRY(h->scratch("gmres.int", 1 + 2 * (size_t)m + 8, &dint.p));
   Span<KHead> dhead;
   BSP_TRY(h->scratch("gmres.head", 1, &dhead.p));
+  Span<double> mgs_part;
+  Span<unsigned> mgs_bar;
+  BSP_TRY(h->scratch("gmres.mgs_partials", (size_t)(m + 2) * h->num_sms, &mgs_part.p));
+  BSP_TRY(h->scratch("gmres.mgs_barrier", 1, &mgs_bar.p));
   BSP_CUDA_TRY(cudaMemsetAsync(dsm.get(), 0, total * sizeof(double), h->stream));
   BSP_CUDA_TRY(cudaMemsetAsync(dhead.get(), 0, sizeof(KHead), h->stream));
   GPtrs gp{};
@@ -718,15 +921,19 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     // v = M^-1 A q_j
     BSP_TRY(bsmv_launch(A, 1, 0, op_dtype, 1.0,qptr[j], 0.0, nullptr, vv.get(), h->stream));
     if (pc) BSP_TRY(precond_apply(pc, op_prec,vv.get(), vv.get()));
-    // MGS: j+2 fused passes
-    for (int i = 0; i <= j; ++i) {
-      MgsBody body{vv.get(), i > 0 ? qptr[i - 1] : nullptr, qptr[i],
-                   i > 0 ? gp.H + (size_t)(i - 1) * m + j : nullptr, 0.0, len};
-      BSP_TRY(launch_reduce<1>(h, 8 + (i & 1), chunks_of(len), body, StoreFin{gp.H + (size_t)i * m + j}));
+    // MGS: one persistent launch when v's slices fit, else j+2 fused passes
+    const int mg = launch_mgs(h, len, vv.get(), dq.get(), j, gp.H, m, hd, mgs_part.get(), mgs_bar.get());
+    if (mg > 1) return mg;
+    if (mg == 1) {
+      for (int i = 0; i <= j; ++i) {
+        MgsBody body{vv.get(), i > 0 ? qptr[i - 1] : nullptr, qptr[i],
+                     i > 0 ? gp.H + (size_t)(i - 1) * m + j : nullptr, 0.0, len};
+        BSP_TRY(launch_reduce<1>(h, 8 + (i & 1), chunks_of(len), body, StoreFin{gp.H + (size_t)i * m + j}));
+      }
+      BSP_TRY(launch_reduce<1>(h, 10, chunks_of(len), MgsLastBody{vv.get(), qptr[j], gp.H + (size_t)j * m + j, 0.0, len},
+                               NormFin{gp.H + (size_t)(j + 1) * m + j}));
+      bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vv.get(), gp.H + (size_t)(j + 1) * m + j, hd, qptr[j + 1]);
     }
-    BSP_TRY(launch_reduce<1>(h, 10, chunks_of(len), MgsLastBody{vv.get(), qptr[j], gp.H + (size_t)j * m + j, 0.0, len},
-                             NormFin{gp.H + (size_t)(j + 1) * m + j}));
-    bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, vv.get(), gp.H + (size_t)(j + 1) * m + j, hd, qptr[j + 1]);
     bsp::count_launch(), k_gm_ls<<<1, 1, 0, h->stream>>>(gp, o->max_iters);
     BSP_CUDA_TRY(cudaPeekAtLastError());
     BSP_TRY(read_head(h, hd, &st));

@@ -1048,11 +1048,23 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
   // streamed layouts of both sweeps (ILU0: unit L, then U with U_ii^-1;
   // IChol0: L with L_ii^-1, then L^T with L_ii^-T)
   const bool streamed = stream_supported(pc->bs);
-  std::vector<RowEntries> ent;
+  SweepEntries ent;
+  // strictly-lower (lower = true) or strictly-upper entries of the factor
+  auto tri_entries = [&](bool lower) {
+    ent.ptr.assign(n + 1, 0);
+    ent.col.clear();
+    ent.blk.clear();
+    for (int i = 0; i < n; ++i) {
+      const int a = lower ? ptr[i] : diag[i] + 1, b = lower ? diag[i] : ptr[i + 1];
+      for (int e = a; e < b; ++e) {
+        ent.col.push_back(col[e]);
+        ent.blk.push_back(e);
+      }
+      ent.ptr[i + 1] = (int)ent.col.size();
+    }
+  };
   if (streamed) {
-    ent.assign(n, RowEntries());
-    for (int i = 0; i < n; ++i)
-      for (int e = ptr[i]; e < diag[i]; ++e) ent[i].emplace_back(col[e], (int64_t)e);
+    tri_entries(true);
     pc->ss_lo = std::make_shared<StreamSym>();
     BSP_TRY(stream_build(n, true, stream_warps(pc->bs), ent, false, lower_only, false, *pc->ss_lo));
   }
@@ -1064,10 +1076,7 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
     BSP_TRY(upload(pc->order_up, order));
     BSP_TRY(make_tasks(pc, false, n, upper_deps));
     if (streamed) {
-      for (int i = 0; i < n; ++i) {
-        ent[i].clear();
-        for (int e = diag[i] + 1; e < ptr[i + 1]; ++e) ent[i].emplace_back(col[e], (int64_t)e);
-      }
+      tri_entries(false);
       pc->ss_up = std::make_shared<StreamSym>();
       BSP_TRY(stream_build(n, false, stream_warps(pc->bs), ent, false, true, false, *pc->ss_up));
     }
@@ -1094,10 +1103,9 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
     BSP_TRY(upload(pc->order_up, order));
     BSP_TRY(make_tasks(pc, false, n, trans_deps));
     if (streamed) {
-      for (int i = 0; i < n; ++i) {
-        ent[i].clear();
-        for (int t = tp[i]; t < tp[i + 1]; ++t) ent[i].emplace_back(trow[t], tblk[t]);
-      }
+      ent.ptr = tp;
+      ent.col = trow;
+      ent.blk = tblk;
       pc->ss_up = std::make_shared<StreamSym>();
       BSP_TRY(stream_build(n, false, stream_warps(pc->bs), ent, true, true, true, *pc->ss_up));
     }

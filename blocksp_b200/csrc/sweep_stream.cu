@@ -377,8 +377,8 @@ template <typename T> static int upload_vec(DevBuf<T>& d, const std::vector<T>& 
   return BSP_OK;
 }
 
-int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>& ent, bool trans_blocks,
-                 bool has_d, bool trans_d, StreamSym& S) {
+int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool trans_blocks, bool has_d,
+                 bool trans_d, StreamSym& S) {
   const int dir = ascending ? 1 : -1;
   S.n = n;
   S.W = warps;
@@ -394,7 +394,7 @@ int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>
     const int pr = r - dir;
     bool cont = false;
     if (idx > 0 && clen[chain_of[pr]] < kStreamCmax)
-      for (auto& e : ent[r]) cont |= (e.first == pr);
+      for (int t = E.ptr[r]; t < E.ptr[r + 1]; ++t) cont |= (E.col[t] == pr);
     if (cont) {
       const int c = chain_of[pr];
       chain_of[r] = c;
@@ -416,8 +416,8 @@ int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>
     for (int c = sp * warps; c < std::min(nc, (sp + 1) * warps); ++c)
       for (int k = 0; k < clen[c]; ++k) {
         const int r = first[c] + k * dir;
-        for (auto& e : ent[r]) {
-          const int so = chain_of[e.first] / warps;
+        for (int t = E.ptr[r]; t < E.ptr[r + 1]; ++t) {
+          const int so = chain_of[E.col[t]] / warps;
           if (so != sp) L = std::max(L, lvl[so] + 1);
         }
       }
@@ -432,8 +432,8 @@ int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>
   std::vector<int> super_beg(nsup + 1, 0), codes, q_row(n);
   std::vector<int4> chains, rec(n);
   std::vector<int64_t> src;
-  codes.reserve(n * 4);
-  src.reserve(n * 4);
+  codes.reserve(E.col.size());
+  src.reserve(E.col.size());
   chains.reserve(nc);
   int q = 0;
   std::vector<std::pair<int, int64_t>> ext, loc;
@@ -449,15 +449,15 @@ int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>
         ext.clear();
         loc.clear();
         bool has_in = false;
-        for (auto& e : ent[r]) {
-          const int j = e.first, cj = chain_of[j];
+        for (int tt = E.ptr[r]; tt < E.ptr[r + 1]; ++tt) {
+          const int j = E.col[tt], cj = chain_of[j];
           if (cj == c && pos[j] == k - 1) {
             has_in = true;
-            inchain = {-1, e.second};
+            inchain = {-1, E.blk[tt]};
           } else if (cj / warps == sp) {
-            loc.emplace_back(-2 - ((cj - sp * warps) * kStreamCmax + pos[j]), e.second);
+            loc.emplace_back(-2 - ((cj - sp * warps) * kStreamCmax + pos[j]), E.blk[tt]);
           } else {
-            ext.emplace_back(j, e.second);
+            ext.emplace_back(j, E.blk[tt]);
           }
         }
         const int e_first = (int)codes.size();

@@ -44,13 +44,17 @@ struct StreamSym {
   DevBuf<int> q_row;       // per stream row: its block row (D gather)
 };
 
-// Entries of row i of the sweep: calls f(j, factor_block_index) per entry.
-using RowEntries = std::vector<std::pair<int, int64_t>>;
+// The entries of a sweep in CSR form: row i reads rows col[t] through the
+// factor blocks blk[t], t in [ptr[i], ptr[i+1]).
+struct SweepEntries {
+  std::vector<int> ptr, col;
+  std::vector<int64_t> blk;
+};
 
-// Builds the streamed layout of a sweep over n rows.  ent[i] lists row i's
-// entries; ascending: forward sweep (dependencies j < i).
-int stream_build(int n, bool ascending, int warps, const std::vector<RowEntries>& ent, bool trans_blocks,
-                 bool has_d, bool trans_d, StreamSym& S);
+// Builds the streamed layout of a sweep over n rows; ascending: forward
+// sweep (dependencies j < i), else backward (j > i).
+int stream_build(int n, bool ascending, int warps, const SweepEntries& ent, bool trans_blocks, bool has_d,
+                 bool trans_d, StreamSym& S);
 
 // Block size, precision and warp count the streamed kernel supports.
 bool stream_supported(int bs);

@@ -343,6 +343,21 @@ int bsp_learned_smooth(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int K, 
 /* Builds the learned preconditioner of A (ILU0 + network correction). */
 int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int precision, bsp_precond_t* out);
 
+/* ---------------- MatrixMarket files ----------------
+ * mtxMatrix_to_BlockSp / mtxArray_to_solArray (blocksp_tests.hpp:582-699).
+ * Reading starts at 1-based line max(start_line, 1), the size line.
+ * Matrix: entries "i j value" (1-based unless base_zero, which the reference
+ * ignores); symmetric fills (j, i) too; blocks bs x bs in order of first
+ * appearance, a repeated entry overwrites.  Call once with row_ptr == NULL
+ * for n_rows, n_cols, nnzb, then with row_ptr[n_rows+1], col_idx[nnzb],
+ * vals[nnzb*bs*bs].  Vector: M x 1 values in solArray<T,B,D> order (value i
+ * at flat position i); B*D must divide M.  The reference misplaces values
+ * for D > 1 (in-block index i % B instead of i % (B*D), :679); this reader
+ * does not.  Call with out == NULL for the count. */
+int bsp_mtx_read_matrix(const char* path, int bs, int start_line, int symmetric, int base_zero, int* n_rows,
+                        int* n_cols, int64_t* nnzb, int* row_ptr, int* col_idx, double* vals);
+int bsp_mtx_read_vector(const char* path, int start_line, int B, int D, int64_t* n_values, double* out);
+
 #ifdef __cplusplus
 }
 #endif

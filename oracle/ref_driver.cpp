@@ -297,7 +297,8 @@ int main(int argc, char** argv) {
       case 1: return run_ldg<1>(o);
       case 2: return run_ldg<2>(o);
       case 4: return run_ldg<4>(o);
-      default: std::fprintf(stderr, "LDG: B must be 1, 2 or 4\n"); return 2;
+      case 8: return run_ldg<8>(o);
+      default: std::fprintf(stderr, "LDG: B must be 1, 2, 4 or 8\n"); return 2;
     }
   }
   if (!sys_path) {

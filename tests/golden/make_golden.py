@@ -18,7 +18,8 @@ deflated-restart system and the 48^3 bs16 one): their residual histories,
 iteration counts, the norm of x and a fixed strided sample of x (the whole x
 for the 64^2 system), so the GPU solver is checked at full size.
 
-Run from the repository root:  python tests/golden/make_golden.py [--configs-only [NAME ...]]
+Run from the repository root:
+    python tests/golden/make_golden.py [--configs-only [NAME ...] | --ldg-only]
 The reference sources are read from $BLOCKSP_REFERENCE (the LDG matrices under
 its test_mats/); the checker binary must have been built by oracle/Makefile.
 """
@@ -164,7 +165,7 @@ def ldg_fixture() -> None:
     b = read_vec(REF_MATS / "LDG_2D_vecLap_b.mtx")
     sol = read_vec(REF_MATS / "LDG_2D_vecLap_sol.mtx")
     errs = {}
-    for B in (1, 2, 4):
+    for B in (1, 2, 4, 8):
         r = subprocess.run([str(EXE), "--ldg", str(REF_MATS), "--B", str(B)], capture_output=True,
                            text=True, check=True)
         for line in r.stdout.splitlines():
@@ -179,6 +180,9 @@ def ldg_fixture() -> None:
 def main():
     if not EXE.exists():
         sys.exit("build the reference checker first: make -C oracle")
+    if "--ldg-only" in sys.argv:
+        ldg_fixture()
+        return
     configs_only = "--configs-only" in sys.argv
     with tempfile.TemporaryDirectory() as d:
         if not configs_only:
