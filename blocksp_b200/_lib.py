@@ -119,6 +119,11 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_learned_probes": (_I, [_P, _P, _P, _P, _I, _P]),
     "bsp_learned_precond": (_I, [_P, _P, _P, _I, C.POINTER(_P)]),
     "bsp_learned_smooth": (_I, [_P, _P, _P, _I, _I, _P]),
+    "bsp_bs_id": (_I, [_P, _I, _I, C.POINTER(_P)]),
+    "bsp_bs_tr": (_I, [_P, _P, C.POINTER(_P)]),
+    "bsp_bsmm": (_I, [_P, _P, _P, _I, C.POINTER(_P)]),
+    "bsp_matrix_add": (_I, [_P, _D, _P, _D, _P, C.POINTER(_P)]),
+    "bsp_matrix_export": (_I, [_P, _P, _P, _P]),
     "bsp_mtx_read_matrix": (_I, [C.c_char_p, _I, _I, _I, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I64),
                                  _P, _P, _P]),
     "bsp_mtx_read_vector": (_I, [C.c_char_p, _I, _I, _I, C.POINTER(_I64), _P]),

@@ -126,6 +126,32 @@ class Matrix:
     def from_system(cls, s, handle: Handle | None = None) -> "Matrix":
         return cls(s.row_ptr, s.col_idx, s.vals, s.bs, handle=handle)
 
+    @classmethod
+    def _wrap(cls, m: C.c_void_p, handle: Handle) -> "Matrix":
+        """A Matrix object owning the device matrix m made by the library."""
+        obj = cls.__new__(cls)
+        obj.handle = handle
+        n, nc, bs, nnzb = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        check(handle.lib.bsp_matrix_info(m, C.byref(n), C.byref(nc), C.byref(bs), C.byref(nnzb)), "bsp_matrix_info")
+        obj.n_rows, obj.n_cols, obj.bs, obj.nnzb = n.value, nc.value, bs.value, nnzb.value
+        obj.m = m
+        handle.adopt(obj)
+        return obj
+
+    def export(self):
+        """(row_ptr, col_idx, vals) of the matrix, copied to the host."""
+        rp = np.zeros(self.n_rows + 1, np.int32)
+        ci = np.zeros(max(self.nnzb, 1), np.int32)
+        va = np.zeros((max(self.nnzb, 1), self.bs, self.bs))
+        check(self.handle.lib.bsp_matrix_export(self.m, _ptr(rp), _ptr(ci), _ptr(va)), "bsp_matrix_export")
+        return rp, ci[:self.nnzb], va[:self.nnzb]
+
+    def __add__(self, other: "Matrix") -> "Matrix":
+        return matrix_add(1.0, self, 1.0, other)
+
+    def __sub__(self, other: "Matrix") -> "Matrix":
+        return matrix_add(1.0, self, -1.0, other)
+
     def make_lowp(self, dtype: int) -> None:
         check(self.handle.lib.bsp_matrix_make_lowp(self.m, dtype), "bsp_matrix_make_lowp",
               self.handle.h)
@@ -140,6 +166,39 @@ class Matrix:
             self.close()
         except Exception:
             pass
+
+
+def bs_id(size: int, bs: int, handle: Handle | None = None) -> Matrix:
+    """bs_id<T, M>(size) (blocksp_multiply.hpp:335-336): the block identity."""
+    h = handle or default_handle()
+    m = C.c_void_p()
+    check(h.lib.bsp_bs_id(h.h, int(size), int(bs), C.byref(m)), "bsp_bs_id", h.h)
+    return Matrix._wrap(m, h)
+
+
+def bs_tr(A: Matrix) -> Matrix:
+    """bs_tr(A) (blocksp_multiply.hpp:339-340): block (j, i) = A_ij^T."""
+    m = C.c_void_p()
+    check(A.handle.lib.bsp_bs_tr(A.handle.h, A.m, C.byref(m)), "bsp_bs_tr", A.handle.h)
+    return Matrix._wrap(m, A.handle)
+
+
+def bsmm(A: Matrix, B: Matrix, *more, Atran: bool = False) -> Matrix:
+    """bsmm(A, B[, C[, D]], Atran) (blocksp_multiply.hpp:343-362): op(A) B [C [D]]
+    with op(A) = A^T when Atran; longer products nest to the right (:137-159)."""
+    if more:
+        B = bsmm(B, *more)
+    m = C.c_void_p()
+    check(A.handle.lib.bsp_bsmm(A.handle.h, A.m, B.m, int(bool(Atran)), C.byref(m)), "bsp_bsmm", A.handle.h)
+    return Matrix._wrap(m, A.handle)
+
+
+def matrix_add(alpha: float, A: Matrix, beta: float, B: Matrix) -> Matrix:
+    """alpha A + beta B with the container's block order (A's blocks, then B's new ones)."""
+    m = C.c_void_p()
+    check(A.handle.lib.bsp_matrix_add(A.handle.h, float(alpha), A.m, float(beta), B.m, C.byref(m)),
+          "bsp_matrix_add", A.handle.h)
+    return Matrix._wrap(m, A.handle)
 
 
 def bsmv_dev(A: Matrix, x, y, nrhs: int = 1, transpose: bool = False, alpha: float = 1.0,

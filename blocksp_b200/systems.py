@@ -285,6 +285,30 @@ def convection_diffusion_system(dims: tuple[int, ...], bs: int, seed: int, sigma
                      name=f"convdiff{'x'.join(map(str, dims))}_bs{bs}_s{seed}")
 
 
+def random_blocksp(m: int, bs: int, n_col: int, seed: int, n: int | None = None) -> BSRSystem:
+    """A random block matrix in the manner of the reference's rand_BlockSp
+    (blocksp_utility.hpp:463-490): each block row draws n_col random block
+    columns (a repeated column overwrites its block, so rows keep the order of
+    first appearance and may hold fewer blocks) with block entries uniform in
+    [0, 1).  Seeded Philox draws replace the reference's rand() and
+    default_random_engine, whose sequences are implementation-defined."""
+    n = m if n is None else n
+    rng = rng_for(seed)
+    cols = np.minimum((rng.random(m * n_col) * n).astype(np.int64), n - 1).reshape(m, n_col)
+    vals = rng.random(m * n_col * bs * bs).reshape(m, n_col, bs, bs)
+    rp, ci, vs = [0], [], []
+    for i in range(m):
+        row = {}
+        for t in range(n_col):
+            row[int(cols[i, t])] = vals[i, t]
+        ci.extend(row.keys())
+        vs.extend(row.values())
+        rp.append(len(ci))
+    return BSRSystem(n=m, bs=bs, row_ptr=np.array(rp, dtype=np.int32), col_idx=np.array(ci, dtype=np.int32),
+                     vals=np.array(vs).reshape(-1, bs, bs), b=2.0 * rng.random(m * bs) - 1.0,
+                     name=f"rand{m}_bs{bs}_c{n_col}_s{seed}")
+
+
 # ---- the named workloads ----------------------------------------------------
 
 def config0(seed: int = 0, side: int = 64) -> BSRSystem:

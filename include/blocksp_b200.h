@@ -343,6 +343,26 @@ int bsp_learned_smooth(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int K, 
 /* Builds the learned preconditioner of A (ILU0 + network correction). */
 int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int precision, bsp_precond_t* out);
 
+/* ---------------- block sparse matrix algebra ----------------
+ * Results are new device matrices (destroy with bsp_matrix_destroy); their
+ * blocks are ordered within each row as the reference's containers create
+ * them (BlockSp::operator() appends a missing block at the row's end).
+ * bs_id (blocksp_multiply.hpp:335-336, blkSpIdent :21-28): n x n identity. */
+int bsp_bs_id(bsp_handle_t h, int n, int bs, bsp_matrix_t* out);
+/* bs_tr (:339-340, blkSpTranspose :31-42): block (j, i) = A_ij^T. */
+int bsp_bs_tr(bsp_handle_t h, bsp_matrix_t A, bsp_matrix_t* out);
+/* bsmm (:343-362, blkSpMatMat :51-133): C = A B, or A^T B when a_transpose;
+ * each C block sums its block products in the reference's order.  Triple and
+ * quadruple products nest to the right (:137-159). */
+int bsp_bsmm(bsp_handle_t h, bsp_matrix_t A, bsp_matrix_t B, int a_transpose, bsp_matrix_t* out);
+/* C = alpha A + beta B (CSR::operator+= / -= / *=, blocksp_containers.hpp:
+ * 302-318, 340-347): A's blocks, then B's blocks missing from A per row. */
+int bsp_matrix_add(bsp_handle_t h, double alpha, bsp_matrix_t A, double beta, bsp_matrix_t B,
+                   bsp_matrix_t* out);
+/* Structure and FP64 values back to host buffers (row_ptr[n_rows+1],
+ * col_idx[nnzb], vals[nnzb*bs*bs]). */
+int bsp_matrix_export(bsp_matrix_t A, int* row_ptr, int* col_idx, double* vals);
+
 /* ---------------- MatrixMarket files ----------------
  * mtxMatrix_to_BlockSp / mtxArray_to_solArray (blocksp_tests.hpp:582-699).
  * Reading starts at 1-based line max(start_line, 1), the size line.

@@ -94,6 +94,89 @@ class BSR:
                    np.array(vs).reshape(-1, self.bs, self.bs), self.n_cols)
 
 
+# ---------------------------------------------------------------- block algebra
+
+class _Rows:
+    """Row lists of (col, block) in creation order: the reference container's
+    operator() appends a missing block at the end of its row
+    (containers.hpp:147-164)."""
+
+    def __init__(self, m: int, bs: int):
+        self.bs = bs
+        self.rows = [dict() for _ in range(m)]  # dicts keep insertion order
+
+    def at(self, i: int, j: int) -> np.ndarray:
+        r = self.rows[i]
+        if j not in r:
+            r[j] = np.zeros((self.bs, self.bs))
+        return r[j]
+
+    def to_bsr(self, n_cols: int) -> BSR:
+        rp, ci, vs = [0], [], []
+        for r in self.rows:
+            for j, v in r.items():
+                ci.append(j)
+                vs.append(v)
+            rp.append(len(ci))
+        return BSR(len(self.rows), self.bs, np.array(rp, dtype=np.int32), np.array(ci, dtype=np.int32),
+                   np.array(vs).reshape(-1, self.bs, self.bs), n_cols)
+
+
+def bs_id(n: int, bs: int) -> BSR:
+    """blkSpIdent (multiply.hpp:21-28)."""
+    return BSR(n, bs, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32),
+               np.repeat(np.eye(bs)[None], n, axis=0))
+
+
+def bs_tr(A: BSR) -> BSR:
+    """blkSpTranspose (multiply.hpp:31-42): tran(colInd, im) = A(im, colInd)^T,
+    rows scanned in increasing order."""
+    R = _Rows(A.n_cols, A.bs)
+    for i in range(A.n):
+        for t in range(A.row_ptr[i], A.row_ptr[i + 1]):
+            R.at(int(A.col_idx[t]), i)[...] = A.vals[t].T
+    return R.to_bsr(A.n)
+
+
+def _mat_mat(a: np.ndarray, b: np.ndarray, a_trans: bool = False) -> np.ndarray:
+    """dense::matMat (dense_multiply.hpp:130-190): loops im, ik, in with the
+    inner index ascending (the nested-loop form the reference uses up to 8x8)."""
+    if a_trans:
+        a = a.T
+    out = np.zeros((a.shape[0], b.shape[1]))
+    for k in range(a.shape[1]):
+        out += np.outer(a[:, k], b[k, :])
+    return out
+
+
+def bsmm(A: BSR, B: BSR, a_trans: bool = False) -> BSR:
+    """blkSpMatMat (multiply.hpp:51-133): C(imA, colIndB) += A(imA, colIndA) B(colIndA, colIndB)
+    or, transposed, C(colIndA, colIndB) += A(imA, colIndA)^T B(imA, colIndB)."""
+    R = _Rows(A.n_cols if a_trans else A.n, A.bs)
+    for i in range(A.n):
+        for a in range(A.row_ptr[i], A.row_ptr[i + 1]):
+            k = int(A.col_idx[a])
+            src = i if a_trans else k
+            for b in range(B.row_ptr[src], B.row_ptr[src + 1]):
+                j = int(B.col_idx[b])
+                row = k if a_trans else i
+                blk = R.at(row, j)
+                blk += _mat_mat(A.vals[a], B.vals[b], a_trans)
+    return R.to_bsr(B.n_cols)
+
+
+def matrix_add(alpha: float, A: BSR, beta: float, B: BSR) -> BSR:
+    """alpha A + beta B as the container computes A1 += A2 after scaling
+    (containers.hpp:302-318, 340-347): A's blocks, then B's new blocks."""
+    R = _Rows(A.n, A.bs)
+    for i in range(A.n):
+        for t in range(A.row_ptr[i], A.row_ptr[i + 1]):
+            R.at(i, int(A.col_idx[t]))[...] = alpha * A.vals[t] if alpha != 1.0 else A.vals[t]
+        for t in range(B.row_ptr[i], B.row_ptr[i + 1]):
+            R.at(i, int(B.col_idx[t]))[...] += beta * B.vals[t]
+    return R.to_bsr(A.n_cols)
+
+
 # ---------------------------------------------------------------- bsmv / vectors
 
 def bsmv(A: BSR, x: np.ndarray, nrhs: int = 1, transpose: bool = False) -> np.ndarray:

@@ -9,7 +9,8 @@
 // usage: ref_solve <system.bsps> --B b --D d --solver NAME [options]
 //   solvers: bsmv | bsmv_multi | ilu0_pgmres | sor_pgmres | nopre_pgmres |
 //            ichol0_pcg | sor_pcg | diag_pcg | nopre_pcg |
-//            ilu0_apply | ichol0_apply | sor_apply | diag_apply
+//            ilu0_apply | ichol0_apply | sor_apply | diag_apply |
+//            bsmm (--atran 0/1) | bs_tr | pseudo_heat (--delta d): result matrix to --x
 //   options: --tol t --maxit m --restart r --k k --w w --nu nu --sortype t
 //            --reps n (bsmv) --x out.vec --time --print-iters
 //   LDG known answer: ref_solve --ldg <dir with LDG_2D_vecLap*.mtx> --B b
@@ -67,9 +68,41 @@ void write_vec(const std::string& path, const double* v, long long m) {
   f.write((const char*)v, 8 * m);
 }
 
+// A BlockSp (and right-hand side b) in the exchange format read_sys reads.
+template <int N>
+void write_blocksp(const std::string& path, const BlockSp::BlockSp<double, N>& A, const std::vector<double>& b) {
+  std::vector<int> rp{0}, ci;
+  std::vector<double> v;
+  for (int i = 0; i < A.m(); ++i) {
+    const auto& blocks = A.get_data(i);
+    const auto& cols = A.get_colIndex(i);
+    for (size_t t = 0; t < blocks.size(); ++t) {
+      ci.push_back(cols[t]);
+      v.insert(v.end(), blocks[t].data(), blocks[t].data() + N * N);
+    }
+    rp.push_back((int)ci.size());
+  }
+  std::ofstream f(path, std::ios::binary);
+  const int ver = 1, n = A.m(), bs = N, nrhs = 1;
+  const long long nnzb = (long long)ci.size();
+  f.write("BSPS", 4);
+  f.write((const char*)&ver, 4);
+  f.write((const char*)&n, 4);
+  f.write((const char*)&bs, 4);
+  f.write((const char*)&nnzb, 8);
+  f.write((const char*)&nrhs, 4);
+  f.write((const char*)rp.data(), 4 * rp.size());
+  f.write((const char*)ci.data(), 4 * ci.size());
+  f.write((const char*)v.data(), 8 * v.size());
+  std::vector<double> bb(b);
+  bb.resize((size_t)n * N, 0.0);
+  f.write((const char*)bb.data(), 8 * bb.size());
+}
+
 struct Opts {
   std::string solver = "ilu0_pgmres", xout, ldg;
-  double tol = 1e-10, w = 1.6;
+  double tol = 1e-10, w = 1.6, delta = 2e-4;
+  int atran = 0;
   int maxit = 5000, restart = -1, k = -1, nu = 3, sortype = 0, reps = 1, B = 0, D = 1;
   bool time = false, print_iters = false;
 };
@@ -140,6 +173,14 @@ int run(const Sys& s, const Opts& o) {
     solArray<double, B, D> x;
     double t0 = now(), t1 = t0, t2 = t0;
     const std::string& sv = o.solver;
+    if (sv == "bsmm" || sv == "bs_tr" || sv == "pseudo_heat") {
+      // block algebra: the result matrix is written to --x in the exchange format
+      if (sv == "bsmm") write_blocksp<N>(o.xout, bsmm<double, N>(A, A, o.atran != 0), s.b);
+      else if (sv == "bs_tr") write_blocksp<N>(o.xout, bs_tr<double, N>(A), s.b);
+      else  // block_pseudo_heat's operator (blocksp_tests.hpp:282-285)
+        write_blocksp<N>(o.xout, bs_id<double, N>(s.n) - o.delta * bsmm(A, A, true), s.b);
+      return 0;
+    }
     if (sv == "bsmv") {
       t1 = now();
       for (int r = 0; r < o.reps; ++r) {
@@ -286,6 +327,8 @@ int main(int argc, char** argv) {
     else if (a == "--nu") o.nu = std::stoi(next());
     else if (a == "--sortype") o.sortype = std::stoi(next());
     else if (a == "--reps") o.reps = std::stoi(next());
+    else if (a == "--atran") o.atran = std::stoi(next());
+    else if (a == "--delta") o.delta = std::stod(next());
     else if (a == "--x") o.xout = next();
     else if (a == "--ldg") o.ldg = next();
     else if (a == "--time") o.time = true;
@@ -309,7 +352,7 @@ int main(int argc, char** argv) {
 #define BSP_CASE(BB, DD) \
   if (o.B == BB && o.D == DD) return run<BB, DD>(s, o);
   BSP_CASE(1, 1) BSP_CASE(2, 1) BSP_CASE(3, 1) BSP_CASE(4, 1) BSP_CASE(8, 1) BSP_CASE(16, 1)
-  BSP_CASE(1, 2) BSP_CASE(2, 2) BSP_CASE(4, 2) BSP_CASE(8, 2)
+  BSP_CASE(1, 2) BSP_CASE(2, 2) BSP_CASE(4, 2) BSP_CASE(8, 2) BSP_CASE(16, 2)
 #undef BSP_CASE
   std::fprintf(stderr, "unsupported (B, D) = (%d, %d)\n", o.B, o.D);
   return 2;

@@ -19,7 +19,7 @@ iteration counts, the norm of x and a fixed strided sample of x (the whole x
 for the 64^2 system), so the GPU solver is checked at full size.
 
 Run from the repository root:
-    python tests/golden/make_golden.py [--configs-only [NAME ...] | --ldg-only]
+    python tests/golden/make_golden.py [--configs-only [NAME ...] | --ldg-only | --algebra-only]
 The reference sources are read from $BLOCKSP_REFERENCE (the LDG matrices under
 its test_mats/); the checker binary must have been built by oracle/Makefile.
 """
@@ -53,6 +53,18 @@ CONFIG_CASES = {
                                        False),
 }
 X_SAMPLE_STRIDE = 997  # a prime stride, so the sample visits every block-row position
+
+# Block algebra on seeded random block matrices (systems.random_blocksp):
+# name -> (m, bs, n_col, seed, B, D, driver mode, extra args)
+ALGEBRA_CASES = {
+    "bsmm_rand_bs4": (24, 4, 4, 31, 4, 1, "bsmm", ["--atran", "0"]),
+    "bsmm_t_rand_bs4": (24, 4, 4, 31, 4, 1, "bsmm", ["--atran", "1"]),
+    "bs_tr_rand_bs4": (24, 4, 4, 31, 4, 1, "bs_tr", []),
+    "bsmm_t_rand_bs8": (16, 8, 3, 33, 8, 1, "bsmm", ["--atran", "1"]),
+}
+# block_pseudo_heat (blocksp_tests.hpp:269-300): ASym = I - delta A^T A with
+# A random, 32x32 blocks (B = 16, D = 2), then the reference's solvers on it
+PSEUDO_HEAT = {"m": 64, "bs": 32, "n_col": 4, "seed": 32, "delta": 2e-4, "B": 16, "D": 2}
 
 # name: (dims, bs, seed, skew, B, D, solver, extra args)
 CASES = {
@@ -141,6 +153,40 @@ def run_config_case(name, spec, tmp: Path) -> dict:
     return {"name": name, "iters": iters, "hist_len": len(hist), "x_norm": float(np.linalg.norm(x))}
 
 
+def run_algebra(A, name, B, D, mode, extra, tmp: Path):
+    """The reference's block algebra on A (the driver writes the result matrix)."""
+    f = tmp / f"{name}.bsps"
+    systems.write_bsr(f, A)
+    out = tmp / f"{name}.out.bsps"
+    subprocess.run([str(EXE), str(f), "--B", str(B), "--D", str(D), "--solver", mode, "--x", str(out), *extra],
+                   capture_output=True, text=True, check=True)
+    return systems.read_bsr(out)
+
+
+def algebra_fixtures(tmp: Path) -> None:
+    for name, (m, bs, nc, seed, B, D, mode, extra) in ALGEBRA_CASES.items():
+        C = run_algebra(systems.random_blocksp(m, bs, nc, seed), name, B, D, mode, extra, tmp)
+        meta = {"m": m, "bs": bs, "n_col": nc, "seed": seed, "mode": mode, "args": extra}
+        np.savez_compressed(OUT / f"{name}.npz", row_ptr=C.row_ptr, col_idx=C.col_idx, vals=C.vals,
+                            meta=np.array(json.dumps(meta)))
+        print({"name": name, "nnzb": C.nnzb})
+    ph = PSEUDO_HEAT
+    A = systems.random_blocksp(ph["m"], ph["bs"], ph["n_col"], ph["seed"])
+    S = run_algebra(A, "pseudo_heat", ph["B"], ph["D"], "pseudo_heat", ["--delta", repr(ph["delta"])], tmp)
+    S.b = A.b
+    flat = S.vals.reshape(-1)
+    idx = np.arange(0, flat.size, X_SAMPLE_STRIDE, dtype=np.int64)
+    out = {"row_ptr": S.row_ptr, "col_idx": S.col_idx, "vals_norm": np.array(np.linalg.norm(flat)),
+           "vals_sample_idx": idx, "vals_sample": flat[idx], "meta": np.array(json.dumps(ph))}
+    for tag, solver, args in (("pcg", "ichol0_pcg", ["--tol", "1e-10", "--maxit", "2000"]),
+                              ("gmres", "ilu0_pgmres",
+                               ["--tol", "1e-10", "--maxit", "5000", "--restart", "30", "--k", "10"])):
+        x, hist, iters = run_ref(S, f"pseudo_heat_{tag}", ph["B"], ph["D"], solver, args, tmp)
+        out[f"{tag}_x"], out[f"{tag}_hist"], out[f"{tag}_iters"] = x, hist, np.array(iters)
+        print({"name": f"pseudo_heat_{tag}", "iters": iters})
+    np.savez_compressed(OUT / "pseudo_heat_bs32.npz", **out)
+
+
 def ldg_fixture() -> None:
     """The reference's LDG fixture as arrays plus its known-answer errors."""
     if not REF_MATS.exists():
@@ -183,11 +229,16 @@ def main():
     if "--ldg-only" in sys.argv:
         ldg_fixture()
         return
+    if "--algebra-only" in sys.argv:
+        with tempfile.TemporaryDirectory() as d:
+            algebra_fixtures(Path(d))
+        return
     configs_only = "--configs-only" in sys.argv
     with tempfile.TemporaryDirectory() as d:
         if not configs_only:
             for name, spec in CASES.items():
                 print(run_case(name, spec, Path(d)))
+            algebra_fixtures(Path(d))
         only = [a for a in sys.argv[1:] if not a.startswith("--")]
         for name, spec in CONFIG_CASES.items():
             if not only or name in only:

@@ -1,0 +1,67 @@
+"""Block algebra of the oracle against the reference (CPU).
+
+The fixtures are the reference's own bsmm (A B and A^T B), bs_tr and
+block_pseudo_heat operator I - delta A^T A (blocksp_multiply.hpp:21-159,
+blocksp_tests.hpp:269-300) on seeded random block matrices, written by the
+reference build (tests/golden/make_golden.py).  Structure (block order within
+each row) must be identical; values within 1e-13 relative.
+"""
+import json
+
+import numpy as np
+import pytest
+
+import oracle.blocksp_oracle as O
+from blocksp_b200 import systems
+from parity import GOLDEN
+
+CASES = ["bsmm_rand_bs4", "bsmm_t_rand_bs4", "bs_tr_rand_bs4", "bsmm_t_rand_bs8"]
+
+
+def load_case(name):
+    d = np.load(GOLDEN / f"{name}.npz")
+    meta = json.loads(str(d["meta"]))
+    A = systems.random_blocksp(meta["m"], meta["bs"], meta["n_col"], meta["seed"])
+    return d, meta, A
+
+
+def oracle_result(meta, A):
+    Ao = O.BSR.from_system(A)
+    if meta["mode"] == "bs_tr":
+        return O.bs_tr(Ao)
+    return O.bsmm(Ao, Ao, meta["args"][1] == "1")
+
+
+def check_same(got_rp, got_ci, got_vals, d, tol=1e-13):
+    assert np.array_equal(got_rp, d["row_ptr"]) and np.array_equal(got_ci, d["col_idx"])
+    ref = d["vals"]
+    assert np.abs(np.asarray(got_vals) - ref).max() <= tol * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_block_algebra_vs_reference(name):
+    d, meta, A = load_case(name)
+    C = oracle_result(meta, A)
+    check_same(C.row_ptr, C.col_idx, C.vals, d)
+
+
+def pseudo_heat_oracle():
+    d = np.load(GOLDEN / "pseudo_heat_bs32.npz")
+    ph = json.loads(str(d["meta"]))
+    A = systems.random_blocksp(ph["m"], ph["bs"], ph["n_col"], ph["seed"])
+    Ao = O.BSR.from_system(A)
+    S = O.matrix_add(1.0, O.bs_id(ph["m"], ph["bs"]), -ph["delta"], O.bsmm(Ao, Ao, True))
+    return d, ph, A, S
+
+
+def check_pseudo_heat(rp, ci, vals, d, tol=1e-13):
+    assert np.array_equal(rp, d["row_ptr"]) and np.array_equal(ci, d["col_idx"])
+    flat = np.asarray(vals).reshape(-1)
+    sample = d["vals_sample"]
+    assert np.abs(flat[d["vals_sample_idx"]] - sample).max() <= tol * np.abs(sample).max()
+    assert abs(np.linalg.norm(flat) - float(d["vals_norm"])) <= tol * float(d["vals_norm"])
+
+
+def test_oracle_pseudo_heat_operator_vs_reference():
+    d, ph, A, S = pseudo_heat_oracle()
+    check_pseudo_heat(S.row_ptr, S.col_idx, S.vals, d)
