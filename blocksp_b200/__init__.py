@@ -9,9 +9,9 @@ function does.
 from . import _lib
 from ._lib import BspError
 from .api import (Batch, IChol0, IChol0_pCG, ILU0, ILU0_pGMRES, SOR, SOR_pCG, SOR_pGMRES, Diag, Handle, Matrix,
-                  NoPre, Precond, bs_id, bs_tr, bsmm, bsmv, bsmv_dev, default_handle, dot_dev, ez, matrix_add, pCG,
+                  NoPre, Precond, Eigenvalues, arnoldi_eigenvalues, bs_id, bs_tr, bsmm, bsmv, bsmv_dev, default_handle, dot_dev, ez, matrix_add, pCG,
                   pGMRES)
 
-__all__ = ["Batch", "BspError", "Handle", "Matrix", "bs_id", "bs_tr", "bsmm", "matrix_add", "bsmv", "bsmv_dev", "default_handle", "dot_dev", "_lib",
+__all__ = ["Batch", "BspError", "Handle", "Matrix", "Eigenvalues", "arnoldi_eigenvalues", "bs_id", "bs_tr", "bsmm", "matrix_add", "bsmv", "bsmv_dev", "default_handle", "dot_dev", "_lib",
            "Precond", "NoPre", "Diag", "SOR", "ILU0", "IChol0", "pCG", "pGMRES", "SOR_pGMRES",
            "SOR_pCG", "ILU0_pGMRES", "IChol0_pCG", "ez"]

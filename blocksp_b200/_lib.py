@@ -38,7 +38,7 @@ class PrecondParams(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iters", C.c_int), ("restart", C.c_int), ("k", C.c_int),
                 ("print_iters", C.c_int), ("stop_rule", C.c_int), ("precision", C.c_int),
-                ("inner_tol", C.c_double), ("max_outer", C.c_int)]
+                ("inner_tol", C.c_double), ("max_outer", C.c_int), ("print_eig_info", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -119,6 +119,7 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_learned_probes": (_I, [_P, _P, _P, _P, _I, _P]),
     "bsp_learned_precond": (_I, [_P, _P, _P, _I, C.POINTER(_P)]),
     "bsp_learned_smooth": (_I, [_P, _P, _P, _I, _I, _P]),
+    "bsp_arnoldi_eigenvalues": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _P, C.POINTER(_I)]),
     "bsp_bs_id": (_I, [_P, _I, _I, C.POINTER(_P)]),
     "bsp_bs_tr": (_I, [_P, _P, C.POINTER(_P)]),
     "bsp_bsmm": (_I, [_P, _P, _P, _I, C.POINTER(_P)]),

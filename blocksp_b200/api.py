@@ -336,9 +336,9 @@ def IChol0(A: Matrix, precision: int = _lib.PREC_F64) -> Precond:
 # ---------------------------------------------------------------- solvers
 
 def _opts(tol, max_iters, restart=-1, k=-1, print_iters=False, stop_rule=_lib.STOP_REFERENCE,
-          precision=_lib.PREC_F64, inner_tol=1e-4, max_outer=50) -> SolveOpts:
+          precision=_lib.PREC_F64, inner_tol=1e-4, max_outer=50, print_eig_info=False) -> SolveOpts:
     return SolveOpts(float(tol), int(max_iters), int(restart), int(k), int(bool(print_iters)),
-                     int(stop_rule), int(precision), float(inner_tol), int(max_outer))
+                     int(stop_rule), int(precision), float(inner_tol), int(max_outer), int(bool(print_eig_info)))
 
 
 def _info_dict(info: SolveInfo) -> dict:
@@ -384,13 +384,72 @@ def pCG(A: Matrix, b, tol: float, preCond: Precond | None = None, maxIters: int 
 def pGMRES(A: Matrix, b, tol: float, preCond: Precond | None = None, maxIters: int = 500,
            restart: int = -1, k: int = -1, printIters: bool = False, return_info: bool = False,
            stop_rule: int = _lib.STOP_REFERENCE, precision: int = _lib.PREC_F64,
-           inner_tol: float = 1e-6, max_outer: int = 50):
+           inner_tol: float = 1e-6, max_outer: int = 50, printEigInfo: bool = False):
     """Left-preconditioned GMRES with optional deflated restart (blocksp_solvers.hpp:156-295).
 
-    stop_rule / precision as for pCG."""
+    stop_rule / precision as for pCG.  printEigInfo prints the (harmonic, once
+    restarted) Ritz value summary of the final Hessenberg matrix (:272-288)."""
     return _solve("bsp_pgmres_dev", "bsp_pgmres", A, b, preCond,
                   _opts(tol, maxIters, restart, k, printIters, stop_rule=stop_rule,
-                        precision=precision, inner_tol=inner_tol, max_outer=max_outer), return_info)
+                        precision=precision, inner_tol=inner_tol, max_outer=max_outer,
+                        print_eig_info=printEigInfo), return_info)
+
+
+class Eigenvalues:
+    """Eigenvalues_Arr (blocksp_dense_solvers.hpp:909-1000): real and imaginary
+    parts, magnitudes and their statistics."""
+
+    def __init__(self, wr: np.ndarray, wi: np.ndarray, harmonic_Ritz: bool = False):
+        self.WR, self.WI = np.asarray(wr, float), np.asarray(wi, float)
+        self.WM = np.sqrt(self.WR ** 2 + self.WI ** 2)
+        self.harmonic_Ritz = harmonic_Ritz
+        self.N = len(self.WR)
+
+    def real(self): return self.WR
+    def imag(self): return self.WI
+    def mag(self): return self.WM
+    def min_real(self): return float(self.WR.min())
+    def max_real(self): return float(self.WR.max())
+    def min_abs_real(self): return float(np.abs(self.WR).min())
+    def max_abs_real(self): return float(np.abs(self.WR).max())
+    def min_imag(self): return float(self.WI.min())
+    def max_imag(self): return float(self.WI.max())
+    def min_abs_imag(self): return float(np.abs(self.WI).min())
+    def max_abs_imag(self): return float(np.abs(self.WI).max())
+    def min_mag(self): return float(self.WM.min())
+    def max_mag(self): return float(self.WM.max())
+    def arg_min_mag(self): return int(np.argmin(self.WM))
+    def arg_max_mag(self): return int(np.argmax(self.WM))
+    def cond_number(self): return self.max_mag() / self.min_mag()
+
+    def printEigInfo(self) -> None:
+        print("Harmonic Ritz info" if self.harmonic_Ritz else "Eigenvalue info")
+        print(f"min/max real eig {self.min_real():g} {self.max_real():g}")
+        print(f"min/max img  eig {self.min_imag():g} {self.max_imag():g}")
+        print(f"smallest magn eig {self.min_mag():g}")
+        print(f"largest magn eig  {self.max_mag():g}")
+        print(f"ratio/cond {self.cond_number():g}")
+
+    def printEigVals(self) -> None:
+        if self.harmonic_Ritz:
+            print("Harmonic Ritz values")
+        for title, v in (("real component", self.WR), ("imaginary component", self.WI), ("magnitude", self.WM)):
+            print(f"Eigenvalues - {title}")
+            print(" ".join(f"{x:g}" for x in v))
+
+
+def arnoldi_eigenvalues(A: Matrix, iters: int = 30, preCond: Precond | None = None, printEigInfo: bool = False,
+                        printEigVals: bool = False, harmonic_Ritz: bool = False) -> Eigenvalues:
+    """arnoldi_eigenvalues (blocksp_solvers.hpp:306-334): Ritz (or harmonic Ritz)
+    values of M^-1 A after `iters` Arnoldi steps from q_0 = e_0, on the GPU."""
+    lib = A.handle.lib
+    wr = np.zeros(max(1, iters))
+    wi = np.zeros(max(1, iters))
+    n = C.c_int()
+    check(lib.bsp_arnoldi_eigenvalues(A.handle.h, A.m, preCond.p if preCond is not None else None, int(iters),
+                                      int(bool(harmonic_Ritz)), int(bool(printEigInfo)), int(bool(printEigVals)),
+                                      _ptr(wr), _ptr(wi), C.byref(n)), "bsp_arnoldi_eigenvalues", A.handle.h)
+    return Eigenvalues(wr[:n.value], wi[:n.value], harmonic_Ritz)
 
 
 class SOR_pGMRES:

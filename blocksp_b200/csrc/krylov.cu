@@ -16,6 +16,8 @@
 //     invariant subspace, P_{k+1}, c_r, H_new) runs on one GPU warp in
 //     small_dense.h (working set in shared memory), and Qn <- Qn P_{k+1} is a tall-skinny in-place kernel.
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
 #include <type_traits>
 #include <vector>
 #include "reduce.cuh"
@@ -648,6 +650,88 @@ __global__ void k_gm_pure_restart(GPtrs g) {
   if (!(r > h->tolerance)) h->done = DONE_CONVERGED;
 }
 
+// Eigenvalues of the square part H_s (n x n) of H ((n+1) x n, leading
+// dimension ldh), or harmonic Ritz values when harmonic (Eigenvalues_Arr,
+// blocksp_dense_solvers.hpp:916-961): one warp, scratch in global memory.
+__global__ void __launch_bounds__(32) k_ritz(const double* __restrict__ H, int ldh, int n, int harmonic,
+                                             double* work, int* iwork, double* wr, double* wi, int* ok) {
+  const sd::WarpTeam tm;
+  const int r0 = tm.rank(), ns = tm.size();
+  double* Hn = work;
+  double* Z = Hn + (size_t)n * n;
+  double* scr = Z + (size_t)n * n;
+  double* w = scr + (size_t)n * n + 4 * (size_t)n + 32;
+  for (int e = r0; e < n * n; e += ns) Hn[e] = H[(size_t)(e / n) * ldh + e % n];
+  tm.sync();
+  if (harmonic) {
+    // H_tilde = H_n + h_mn^2 H_n^-T e_n e_n^T (only the last column changes)
+    const double hmn = H[(size_t)n * ldh + n - 1];
+    for (int i = r0; i < n; i += ns) w[i] = (i == n - 1) ? 1.0 : 0.0;
+    tm.sync();
+    sd::solve_transposed(tm, Hn, n, n, w, scr, iwork);
+    for (int i = r0; i < n; i += ns) Hn[(size_t)i * n + n - 1] += hmn * hmn * w[i];
+    tm.sync();
+  }
+  sd::hessenberg(tm, Hn, n, n, Z, n, scr);
+  const bool conv = sd::francis_qr(tm, Hn, n, n, Z, n);
+  if (r0 == 0) {
+    sd::schur_eigs(Hn, n, n, wr, wi);
+    *ok = conv ? 1 : 0;
+  }
+}
+
+// printEigInfo / printEigVals text of Eigenvalues_Arr (dense_solvers.hpp:973-990).
+static void print_eigs(const double* wr, const double* wi, int n, bool harmonic, bool info, bool vals) {
+  if (n < 1) return;
+  std::vector<double> wm(n);
+  for (int i = 0; i < n; ++i) wm[i] = std::sqrt(wr[i] * wr[i] + wi[i] * wi[i]);
+  auto mn = [&](const double* a) { return *std::min_element(a, a + n); };
+  auto mx = [&](const double* a) { return *std::max_element(a, a + n); };
+  if (vals) {
+    if (harmonic) printf("Harmonic Ritz values\n");
+    printf("Eigenvalues - real component\n");
+    for (int i = 0; i < n; ++i) printf("%g%c", wr[i], i + 1 < n ? ' ' : '\n');
+    printf("Eigenvalues - imaginary component\n");
+    for (int i = 0; i < n; ++i) printf("%g%c", wi[i], i + 1 < n ? ' ' : '\n');
+    printf("Eigenvalues - magnitude\n");
+    for (int i = 0; i < n; ++i) printf("%g%c", wm[i], i + 1 < n ? ' ' : '\n');
+  }
+  if (info) {
+    printf(harmonic ? "Harmonic Ritz info\n" : "Eigenvalue info\n");
+    printf("min/max real eig %g %g\n", mn(wr), mx(wr));
+    printf("min/max img  eig %g %g\n", mn(wi), mx(wi));
+    printf("smallest magn eig %g\n", mn(wm.data()));
+    printf("largest magn eig  %g\n", mx(wm.data()));
+    printf("ratio/cond %g\n", mx(wm.data()) / mn(wm.data()));
+  }
+  fflush(stdout);
+}
+
+// Ritz values of the n-column H (device, leading dimension ldh) to the host.
+static int ritz_values(bsp_handle_s* h, const double* H, int ldh, int n, bool harmonic, double* wr, double* wi) {
+  if (n < 1) return BSP_OK;
+  double* work = nullptr;
+  int* iwork = nullptr;
+  BSP_TRY(h->scratch("ritz.work", (size_t)3 * n * n + 7 * (size_t)n + 64, &work));
+  BSP_TRY(h->scratch("ritz.iwork", (size_t)n + 1, &iwork));
+  double* wdev = work + (size_t)3 * n * n + 5 * (size_t)n + 32;  // 2n values
+  bsp::count_launch(), k_ritz<<<1, 32, 0, h->stream>>>(H, ldh, n, harmonic ? 1 : 0, work, iwork + 1, wdev,
+                                                       wdev + n, iwork);
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  std::vector<double> wv(2 * (size_t)n);
+  int ok = 0;
+  BSP_CUDA_TRY(cudaMemcpyAsync(wv.data(), wdev, 2 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaMemcpyAsync(&ok, iwork, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (!ok) {
+    record_error("eigenvalues: the QR iteration did not converge");
+    return BSP_BREAKDOWN;
+  }
+  std::copy(wv.begin(), wv.begin() + n, wr);
+  std::copy(wv.begin() + n, wv.end(), wi);
+  return BSP_OK;
+}
+
 // ------------------------------------------------------------------ host helpers
 // One persistent MGS launch for column j when the slice of v fits the
 // registers of one CTA per SM (else returns 1: the per-pass form is used).
@@ -990,6 +1074,14 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
     printf("pGMRES iters %d\n", st.tot);  // solvers.hpp:266-270
     if (st.tot > o->max_iters) printf("maximum pGMRES iterations reached\n");
   }
+  if (o->print_eig_info && st.j > 0) {
+    // eigenvalues of the final H's square part; harmonic Ritz values after a
+    // restart (solvers.hpp:272-288)
+    std::vector<double> wr(st.j), wi(st.j);
+    const bool harm = n_restarts > 0;
+    BSP_TRY(ritz_values(h, gp.H, m, st.j, harm, wr.data(), wi.data()));
+    print_eigs(wr.data(), wi.data(), st.j, harm, true, false);
+  }
   return status_of(st.done);
 }
 
@@ -1137,6 +1229,67 @@ int bsp_pgmres(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const double* b
                const bsp_solve_opts* opts, double* hist, int hist_cap, bsp_solve_info* info) {
   return solve_host(true, h, A, pc, b, x, opts, hist, hist_cap, info);
 }
+int bsp_arnoldi_eigenvalues(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int iters, int harmonic_ritz,
+                            int print_info, int print_vals, double* wr, double* wi, int* n_out) {
+  if (!h || !A || !wr || !wi || !n_out || iters < 1) return BSP_INVALID;
+  if (A->n_rows != A->n_cols) return BSP_INVALID;
+  BSP_CUDA_TRY(cudaSetDevice(h->device));
+  const int64_t len = (int64_t)A->n_rows * A->bs;
+  iters = (int)std::min<int64_t>(iters, len);  // solvers.hpp:323
+  const int m = iters;
+  double *basis = nullptr, *v = nullptr, *H = nullptr, *part = nullptr;
+  double** qtab = nullptr;
+  KHead* head = nullptr;
+  unsigned* bar = nullptr;
+  BSP_TRY(h->scratch("arnoldi.basis", (size_t)(m + 1) * len, &basis));
+  BSP_TRY(h->scratch("arnoldi.v", len, &v));
+  BSP_TRY(h->scratch("arnoldi.H", (size_t)(m + 1) * m, &H));
+  BSP_TRY(h->scratch("arnoldi.qtab", m + 1, &qtab));
+  BSP_TRY(h->scratch("arnoldi.head", 1, &head));
+  BSP_TRY(h->scratch("arnoldi.partials", (size_t)(m + 2) * h->num_sms, &part));
+  BSP_TRY(h->scratch("arnoldi.barrier", 1, &bar));
+  std::vector<double*> qp(m + 1);
+  for (int i = 0; i <= m; ++i) qp[i] = basis + (size_t)i * len;
+  BSP_CUDA_TRY(cudaMemcpyAsync(qtab, qp.data(), (m + 1) * sizeof(double*), cudaMemcpyHostToDevice, h->stream));
+  // zero_thresh = 10 M^2 eps (solvers.hpp:320) in the head the MGS kernels read
+  KHead hd{};
+  hd.zero_thresh = 10.0 * A->bs * A->bs * kEps;
+  BSP_CUDA_TRY(cudaMemcpyAsync(head, &hd, sizeof(KHead), cudaMemcpyHostToDevice, h->stream));
+  BSP_CUDA_TRY(cudaMemsetAsync(H, 0, (size_t)(m + 1) * m * sizeof(double), h->stream));
+  // q_0 = e_0
+  BSP_CUDA_TRY(cudaMemsetAsync(qp[0], 0, len * sizeof(double), h->stream));
+  const double one = 1.0;
+  BSP_CUDA_TRY(cudaMemcpyAsync(qp[0], &one, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const int g = grid_for(h, len, 256);
+  int n = 0;
+  for (int it = 0; it < m; ++it) {
+    BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, 1.0, qp[it], 0.0, nullptr, v, h->stream));
+    if (pc) BSP_TRY(precond_apply(pc, BSP_PREC_F64, v, v));
+    const int mg = launch_mgs(h, len, v, qtab, it, H, m, head, part, bar);
+    if (mg > 1) return mg;
+    if (mg == 1) {
+      for (int i = 0; i <= it; ++i) {
+        MgsBody body{v, i > 0 ? qp[i - 1] : nullptr, qp[i], i > 0 ? H + (size_t)(i - 1) * m + it : nullptr, 0.0, len};
+        BSP_TRY(launch_reduce<1>(h, 8 + (i & 1), chunks_of(len), body, StoreFin{H + (size_t)i * m + it}));
+      }
+      BSP_TRY(launch_reduce<1>(h, 10, chunks_of(len), MgsLastBody{v, qp[it], H + (size_t)it * m + it, 0.0, len},
+                               NormFin{H + (size_t)(it + 1) * m + it}));
+      bsp::count_launch(), k_div<<<g, 256, 0, h->stream>>>(len, v, H + (size_t)(it + 1) * m + it, head, qp[it + 1]);
+    }
+    n = it + 1;
+    double hsub = 0.0;
+    BSP_CUDA_TRY(cudaMemcpyAsync(&hsub, H + (size_t)(it + 1) * m + it, sizeof(double), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    BSP_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (std::fabs(hsub) < hd.zero_thresh) break;  // the Krylov space is exhausted
+  }
+  if (pc) BSP_TRY(precond_check_status(pc));
+  BSP_TRY(ritz_values(h, H, m, n, harmonic_ritz != 0, wr, wi));
+  *n_out = n;
+  print_eigs(wr, wi, n, harmonic_ritz != 0, print_info != 0, print_vals != 0);
+  return BSP_OK;
+}
+
 int bsp_true_residual_dev(bsp_handle_t h, bsp_matrix_t A, const double* b, const double* x,
                           double* rel_res_host) {
   if (!h || !A || !b || !x || !rel_res_host) return BSP_INVALID;

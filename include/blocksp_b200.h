@@ -112,6 +112,8 @@ typedef struct {
   int precision;       /* bsp_precision of the inner work                       */
   double inner_tol;    /* mixed precision: relative tolerance of each inner solve */
   int max_outer;       /* mixed precision: max refinement steps                 */
+  int print_eig_info;  /* pGMRES: print the Ritz (harmonic Ritz if restarted)
+                          value summary of the final H (solvers.hpp:272-288)    */
 } bsp_solve_opts;
 
 typedef struct {
@@ -342,6 +344,18 @@ int bsp_learned_probes(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, const d
 int bsp_learned_smooth(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int K, int steps, double* vecs);
 /* Builds the learned preconditioner of A (ILU0 + network correction). */
 int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int precision, bsp_precond_t* out);
+
+/* ---------------- eigenvalue diagnostics ----------------
+ * arnoldi_eigenvalues (blocksp_solvers.hpp:306-334) with Eigenvalues_Arr
+ * (blocksp_dense_solvers.hpp:909-1000): `iters` Arnoldi steps of M^-1 A (pc
+ * may be NULL) from q_0 = e_0 on the GPU, then the eigenvalues of the square
+ * part of H (harmonic Ritz values H_n + h_mn^2 H_n^-T e_n e_n^T when
+ * harmonic_ritz).  wr, wi: host arrays of iters values; *n_out = the number
+ * of values (fewer than iters when the Krylov space is exhausted: where the
+ * reference would read past its basis, this stops).  print_info / print_vals
+ * print the reference's printEigInfo / printEigVals text. */
+int bsp_arnoldi_eigenvalues(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int iters, int harmonic_ritz,
+                            int print_info, int print_vals, double* wr, double* wi, int* n_out);
 
 /* ---------------- block sparse matrix algebra ----------------
  * Results are new device matrices (destroy with bsp_matrix_destroy); their

@@ -20,6 +20,8 @@
 // Only the C ABI (blocksp_b200.h) is used underneath; link with
 // -lblocksp_b200.
 #pragma once
+#include <algorithm>
+#include <cmath>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -199,10 +201,10 @@ BlockSp::solArray<T, B, D> pGMRES(const BlockSp::BlockSp<T, B * D>& A, const Blo
                                   int k = -1, bool printIters = false, bool printEigInfo = false,
                                   bsp_solve_info* info = nullptr) {
   (void)A;
-  (void)printEigInfo;
   const std::vector<double> bv = flat(b);
   std::vector<double> xv(bv.size());
-  bsp_solve_opts o{tol, maxIters, restart, k, printIters ? 1 : 0, BSP_STOP_REFERENCE, BSP_PREC_F64, 1e-6, 50};
+  bsp_solve_opts o{tol,  maxIters, restart, k, printIters ? 1 : 0, BSP_STOP_REFERENCE, BSP_PREC_F64, 1e-6, 50,
+                   printEigInfo ? 1 : 0};
   bsp_solve_info local{};
   const int st = bsp_pgmres(preCond.matrix()->handle(), preCond.matrix()->get(), preCond.get(), bv.data(),
                             xv.data(), &o, nullptr, 0, info ? info : &local);
@@ -306,5 +308,135 @@ BlockSp::solArray<T, B, D> ichol0_pCG(const BlockSp::BlockSp<T, B * D>& A, const
   return IChol0_pCG<T, B, D>(A, 1.0e-8, 5000, printIters).solve(A, b);
 }
 }  // namespace ez
+
+// ---------------------------------------------------------------- block algebra
+// bs_id, bs_tr, bsmm (blocksp_multiply.hpp:335-362) on the reference's
+// container: computed on the GPU, returned as a host BlockSp<T,M> whose rows
+// list their blocks in the order the reference's loops create them.
+namespace detail {
+// Owns a device matrix made by the library.
+struct OwnedMatrix {
+  bsp_matrix_t m = nullptr;
+  ~OwnedMatrix() { bsp_matrix_destroy(m); }
+};
+template <typename T, int M> BlockSp::BlockSp<T, M> to_blocksp(bsp_matrix_t C) {
+  int n = 0, nc = 0, bs = 0;
+  int64_t nnzb = 0;
+  check(bsp_matrix_info(C, &n, &nc, &bs, &nnzb), "bsp_matrix_info");
+  std::vector<int> rp(n + 1), ci(nnzb > 0 ? nnzb : 1);
+  std::vector<double> v((size_t)(nnzb > 0 ? nnzb : 1) * M * M);
+  check(bsp_matrix_export(C, rp.data(), ci.data(), v.data()), "bsp_matrix_export");
+  BlockSp::BlockSp<T, M> out(n, nc);
+  for (int i = 0; i < n; ++i)
+    for (int t = rp[i]; t < rp[i + 1]; ++t) {
+      blitz::TinyMatrix<T, M, M> blk;
+      for (int e = 0; e < M * M; ++e) blk.data()[e] = v[(size_t)t * M * M + e];
+      out(i, ci[t]) = blk;
+    }
+  return out;
+}
+}  // namespace detail
+
+template <typename T, int M> BlockSp::BlockSp<T, M> bs_id(int size) {
+  auto h = Handle::shared();
+  detail::OwnedMatrix C;
+  check(bsp_bs_id(h->get(), size, M, &C.m), "bsp_bs_id", h->get());
+  return detail::to_blocksp<T, M>(C.m);
+}
+
+template <typename T, int M> BlockSp::BlockSp<T, M> bs_tr(const BlockSp::BlockSp<T, M>& A) {
+  DeviceMatrix dA(A, M);
+  detail::OwnedMatrix C;
+  check(bsp_bs_tr(dA.handle(), dA.get(), &C.m), "bsp_bs_tr", dA.handle());
+  return detail::to_blocksp<T, M>(C.m);
+}
+
+template <typename T, int M>
+BlockSp::BlockSp<T, M> bsmm(const BlockSp::BlockSp<T, M>& A, const BlockSp::BlockSp<T, M>& B, bool Atran = false) {
+  DeviceMatrix dA(A, M), dB(B, M);
+  detail::OwnedMatrix C;
+  check(bsp_bsmm(dA.handle(), dA.get(), dB.get(), Atran ? 1 : 0, &C.m), "bsp_bsmm", dA.handle());
+  return detail::to_blocksp<T, M>(C.m);
+}
+// triple and quadruple products nest to the right (blocksp_multiply.hpp:137-159)
+template <typename T, int M>
+BlockSp::BlockSp<T, M> bsmm(const BlockSp::BlockSp<T, M>& A, const BlockSp::BlockSp<T, M>& B,
+                            const BlockSp::BlockSp<T, M>& C, bool Atran = false) {
+  return bsmm<T, M>(A, bsmm<T, M>(B, C), Atran);
+}
+template <typename T, int M>
+BlockSp::BlockSp<T, M> bsmm(const BlockSp::BlockSp<T, M>& A, const BlockSp::BlockSp<T, M>& B,
+                            const BlockSp::BlockSp<T, M>& C, const BlockSp::BlockSp<T, M>& D, bool Atran = false) {
+  return bsmm<T, M>(A, bsmm<T, M>(B, C, D), Atran);
+}
+
+// ---------------------------------------------------------------- MatrixMarket files
+// mtxMatrix_to_BlockSp / mtxArray_to_solArray (blocksp_tests.hpp:582-699)
+// through the library's readers (D > 1 vectors are placed correctly).
+template <typename T, int B>
+BlockSp::BlockSp<T, B> mtxMatrix_to_BlockSp(const std::string& path, unsigned start_line = 0, bool symmetric = false,
+                                            bool base_zero = false) {
+  int n = 0, nc = 0;
+  int64_t nnzb = 0;
+  check(bsp_mtx_read_matrix(path.c_str(), B, (int)start_line, symmetric, base_zero, &n, &nc, &nnzb, nullptr,
+                            nullptr, nullptr),
+        "bsp_mtx_read_matrix");
+  std::vector<int> rp(n + 1), ci(nnzb > 0 ? nnzb : 1);
+  std::vector<double> v((size_t)(nnzb > 0 ? nnzb : 1) * B * B);
+  check(bsp_mtx_read_matrix(path.c_str(), B, (int)start_line, symmetric, base_zero, &n, &nc, &nnzb, rp.data(),
+                            ci.data(), v.data()),
+        "bsp_mtx_read_matrix");
+  BlockSp::BlockSp<T, B> A(n, nc);
+  for (int i = 0; i < n; ++i)
+    for (int t = rp[i]; t < rp[i + 1]; ++t) {
+      blitz::TinyMatrix<T, B, B> blk;
+      for (int e = 0; e < B * B; ++e) blk.data()[e] = v[(size_t)t * B * B + e];
+      A(i, ci[t]) = blk;
+    }
+  return A;
+}
+template <typename T, int B, int D = 1>
+BlockSp::solArray<T, B, D> mtxArray_to_solArray(const std::string& path, unsigned start_line = 0) {
+  int64_t m = 0;
+  check(bsp_mtx_read_vector(path.c_str(), (int)start_line, B, D, &m, nullptr), "bsp_mtx_read_vector");
+  std::vector<double> v(m);
+  check(bsp_mtx_read_vector(path.c_str(), (int)start_line, B, D, &m, v.data()), "bsp_mtx_read_vector");
+  return unflat<T, B, D>(v, (int)(m / (B * D)));
+}
+
+// ---------------------------------------------------------------- eigenvalues
+// Eigenvalues_Arr (blocksp_dense_solvers.hpp:909-1000) of arnoldi_eigenvalues
+// (blocksp_solvers.hpp:306-334), computed on the GPU.
+struct Eigenvalues {
+  std::vector<double> WR, WI, WM;
+  bool harmonic_Ritz = false;
+  double min_real() const { return *std::min_element(WR.begin(), WR.end()); }
+  double max_real() const { return *std::max_element(WR.begin(), WR.end()); }
+  double min_imag() const { return *std::min_element(WI.begin(), WI.end()); }
+  double max_imag() const { return *std::max_element(WI.begin(), WI.end()); }
+  double min_mag() const { return *std::min_element(WM.begin(), WM.end()); }
+  double max_mag() const { return *std::max_element(WM.begin(), WM.end()); }
+  double cond_number() const { return max_mag() / min_mag(); }
+};
+template <typename T, int M, typename PreCond = DevicePrecond<T, M, 1>>
+Eigenvalues arnoldi_eigenvalues(const BlockSp::BlockSp<T, M>& A, int iters = 30, const PreCond* preCond = nullptr,
+                                bool printEigInfo = false, bool printEigVals = false, bool harmonic_Ritz = false) {
+  DeviceMatrix dA(A, M);
+  // a preconditioner carries its own device copy of A; the Arnoldi runs on it
+  const bsp_matrix_t mat = preCond ? preCond->matrix()->get() : dA.get();
+  const bsp_handle_t h = preCond ? preCond->matrix()->handle() : dA.handle();
+  Eigenvalues e;
+  e.harmonic_Ritz = harmonic_Ritz;
+  e.WR.resize(iters);
+  e.WI.resize(iters);
+  int n = 0;
+  check(bsp_arnoldi_eigenvalues(h, mat, preCond ? preCond->get() : nullptr, iters, harmonic_Ritz, printEigInfo,
+                                printEigVals, e.WR.data(), e.WI.data(), &n),
+        "bsp_arnoldi_eigenvalues", h);
+  e.WR.resize(n);
+  e.WI.resize(n);
+  for (int i = 0; i < n; ++i) e.WM.push_back(std::sqrt(e.WR[i] * e.WR[i] + e.WI[i] * e.WI[i]));
+  return e;
+}
 
 }  // namespace blocksp_b200

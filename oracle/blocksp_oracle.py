@@ -495,6 +495,36 @@ def _one_arnoldi(it, H, Qn, A, pre, zero_thresh):
     return Hn
 
 
+def ritz_values(H: np.ndarray, harmonic: bool = False) -> np.ndarray:
+    """Eigenvalues_Arr (dense_solvers.hpp:916-961) of H's square part H_s;
+    harmonic: of H_s + h_mn^2 H_s^-T e_n e_n^T.  LAPACK gees stands for the
+    reference's call through numpy."""
+    n = H.shape[1]
+    Hs = H[:n, :n].copy()
+    if harmonic:
+        e = np.zeros(n)
+        e[-1] = 1.0
+        Hs[:, -1] += H[n, n - 1] ** 2 * np.linalg.solve(Hs.T, e)
+    return np.linalg.eigvals(Hs)
+
+
+def arnoldi_eigenvalues(A: BSR, iters: int = 30, pre=no_pre, harmonic: bool = False) -> np.ndarray:
+    """arnoldi_eigenvalues (solvers.hpp:306-334): iters Arnoldi steps of M^-1 A
+    from q_0 = e_0 (stopping where the Krylov space is exhausted), then the
+    (harmonic) Ritz values."""
+    nv = A.n * A.bs
+    q0 = np.zeros(nv)
+    q0[0] = 1.0
+    Qn = [q0]
+    H = np.zeros((1, 0))
+    zero_thresh = 10 * A.bs * A.bs * np.finfo(float).eps
+    for it in range(min(iters, nv)):
+        H = _one_arnoldi(it, H, Qn, A, pre, zero_thresh)
+        if len(Qn) < it + 2:
+            break
+    return ritz_values(H, harmonic)
+
+
 def deflated_restart(H, Qn, res_vec, res_mag, k):
     """Morgan's GMRES-DR restart (deflated_restart.hpp:38-269), real case.
 

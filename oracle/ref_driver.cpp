@@ -10,7 +10,8 @@
 //   solvers: bsmv | bsmv_multi | ilu0_pgmres | sor_pgmres | nopre_pgmres |
 //            ichol0_pcg | sor_pcg | diag_pcg | nopre_pcg |
 //            ilu0_apply | ichol0_apply | sor_apply | diag_apply |
-//            bsmm (--atran 0/1) | bs_tr | pseudo_heat (--delta d): result matrix to --x
+//            bsmm (--atran 0/1) | bs_tr | pseudo_heat (--delta d): result matrix to --x |
+//            arnoldi_eig | arnoldi_eig_ilu0 (--maxit = iters, --k 1: harmonic Ritz)
 //   options: --tol t --maxit m --restart r --k k --w w --nu nu --sortype t
 //            --reps n (bsmv) --x out.vec --time --print-iters
 //   LDG known answer: ref_solve --ldg <dir with LDG_2D_vecLap*.mtx> --B b
@@ -173,6 +174,20 @@ int run(const Sys& s, const Opts& o) {
     solArray<double, B, D> x;
     double t0 = now(), t1 = t0, t2 = t0;
     const std::string& sv = o.solver;
+    if (sv == "arnoldi_eig" || sv == "arnoldi_eig_ilu0") {
+      // arnoldi_eigenvalues (blocksp_solvers.hpp:306-334): one EIG line per value
+      auto print = [](const dense::Eigenvalues_Arr<double>& e) {
+        for (int i = 0; i < e.N; ++i) std::cout << "EIG " << e.WR(i) << " " << e.WI(i) << "\n";
+      };
+      if (sv == "arnoldi_eig") {
+        const preConditioners::NoPre<double, N, 1>* none = nullptr;
+        print(arnoldi_eigenvalues<double, N>(A, o.maxit, none, false, false, o.k > 0));
+      } else {
+        preConditioners::ILU0<double, N, 1> pre(A);
+        print(arnoldi_eigenvalues<double, N>(A, o.maxit, &pre, false, false, o.k > 0));
+      }
+      return 0;
+    }
     if (sv == "bsmm" || sv == "bs_tr" || sv == "pseudo_heat") {
       // block algebra: the result matrix is written to --x in the exchange format
       if (sv == "bsmm") write_blocksp<N>(o.xout, bsmm<double, N>(A, A, o.atran != 0), s.b);

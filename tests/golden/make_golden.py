@@ -62,6 +62,14 @@ ALGEBRA_CASES = {
     "bs_tr_rand_bs4": (24, 4, 4, 31, 4, 1, "bs_tr", []),
     "bsmm_t_rand_bs8": (16, 8, 3, 33, 8, 1, "bsmm", ["--atran", "1"]),
 }
+# arnoldi_eigenvalues: name -> (dims, bs, seed, skew, B, D, mode, iters, harmonic).
+# Without a preconditioner only: the reference build's arnoldi_eigenvalues
+# with an ILU0 preconditioner pointer ends in SIGSEGV (the driver's
+# arnoldi_eig_ilu0 mode), so that case is checked against the oracle only.
+EIG_CASES = {
+    "arnoldi_eig_3d_bs8": ((5, 5, 5), 8, 71, 0.3, 8, 1, "arnoldi_eig", 30, 0),
+    "arnoldi_eig_harm_3d_bs8": ((5, 5, 5), 8, 72, 0.3, 8, 1, "arnoldi_eig", 20, 1),
+}
 # block_pseudo_heat (blocksp_tests.hpp:269-300): ASym = I - delta A^T A with
 # A random, 32x32 blocks (B = 16, D = 2), then the reference's solvers on it
 PSEUDO_HEAT = {"m": 64, "bs": 32, "n_col": 4, "seed": 32, "delta": 2e-4, "B": 16, "D": 2}
@@ -163,6 +171,20 @@ def run_algebra(A, name, B, D, mode, extra, tmp: Path):
     return systems.read_bsr(out)
 
 
+def eig_fixtures(tmp: Path) -> None:
+    for name, (dims, bs, seed, skew, B, D, mode, iters, harm) in EIG_CASES.items():
+        s = system_for(dims, bs, seed, skew)
+        f = tmp / f"{name}.bsps"
+        systems.write_bsr(f, s)
+        r = subprocess.run([str(EXE), str(f), "--B", str(B), "--D", str(D), "--solver", mode, "--maxit", str(iters),
+                            "--k", str(harm)], capture_output=True, text=True, check=True)
+        ev = np.array([[float(v) for v in ln.split()[1:3]] for ln in r.stdout.splitlines() if ln.startswith("EIG ")])
+        meta = {"dims": list(dims), "bs": bs, "seed": seed, "skew": skew, "mode": mode, "iters": iters,
+                "harmonic": harm}
+        np.savez_compressed(OUT / f"{name}.npz", wr=ev[:, 0], wi=ev[:, 1], meta=np.array(json.dumps(meta)))
+        print({"name": name, "n": len(ev)})
+
+
 def algebra_fixtures(tmp: Path) -> None:
     for name, (m, bs, nc, seed, B, D, mode, extra) in ALGEBRA_CASES.items():
         C = run_algebra(systems.random_blocksp(m, bs, nc, seed), name, B, D, mode, extra, tmp)
@@ -232,6 +254,7 @@ def main():
     if "--algebra-only" in sys.argv:
         with tempfile.TemporaryDirectory() as d:
             algebra_fixtures(Path(d))
+            eig_fixtures(Path(d))
         return
     configs_only = "--configs-only" in sys.argv
     with tempfile.TemporaryDirectory() as d:

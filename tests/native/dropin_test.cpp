@@ -6,6 +6,7 @@
 //
 // usage: dropin_test <system.bsps> B D
 // output: "CHECK <solver> <rel max-norm x difference> <ref iters> <gpu iters>"
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -95,6 +96,38 @@ int run(const Sys& s) {
     auto y_ref = BlockSp::bsmv(A, b);
     auto y_gpu = blocksp_b200::bsmv<double, B, D>(A, b);
     std::printf("CHECK bsmv %.3e 0 0\n", rel_diff(y_gpu, y_ref));
+  }
+  // block algebra: identical structure (block order per row) and values
+  {
+    auto same = [](const BlockSp::BlockSp<double, N>& X, const BlockSp::BlockSp<double, N>& Y) {
+      double num = 0.0, den = 0.0;
+      bool structure = X.m() == Y.m();
+      for (int i = 0; structure && i < X.m(); ++i) {
+        const auto& cx = X.get_colIndex(i);
+        const auto& cy = Y.get_colIndex(i);
+        structure = cx.size() == cy.size() && std::equal(cx.begin(), cx.end(), cy.begin());
+        for (size_t t = 0; structure && t < cx.size(); ++t)
+          for (int e = 0; e < N * N; ++e) {
+            num = std::fmax(num, std::fabs(X.get_data(i)[t].data()[e] - Y.get_data(i)[t].data()[e]));
+            den = std::fmax(den, std::fabs(Y.get_data(i)[t].data()[e]));
+          }
+      }
+      return structure ? num / den : 1.0;
+    };
+    std::printf("CHECK bsmm %.3e 0 0\n", same(blocksp_b200::bsmm<double, N>(A, A), BlockSp::bsmm<double, N>(A, A)));
+    std::printf("CHECK bsmm_t %.3e 0 0\n",
+                same(blocksp_b200::bsmm<double, N>(A, A, true), BlockSp::bsmm<double, N>(A, A, true)));
+    std::printf("CHECK bs_tr %.3e 0 0\n", same(blocksp_b200::bs_tr<double, N>(A), BlockSp::bs_tr<double, N>(A)));
+    std::printf("CHECK bs_id %.3e 0 0\n",
+                same(blocksp_b200::bs_id<double, N>(s.n), BlockSp::bs_id<double, N>(s.n)));
+    // Ritz values of A from 12 Arnoldi steps: largest magnitude and the real range
+    BlockSp::preConditioners::NoPre<double, N, 1>* none = nullptr;
+    auto er = BlockSp::arnoldi_eigenvalues<double, N>(A, 12, none);
+    auto eg = blocksp_b200::arnoldi_eigenvalues<double, N>(A, 12);
+    const double d = std::fmax(std::fabs(eg.max_mag() - er.max_mag()) / er.max_mag(),
+                               std::fmax(std::fabs(eg.max_real() - er.max_real()) / er.max_mag(),
+                                         std::fabs(eg.min_real() - er.min_real()) / er.max_mag()));
+    std::printf("CHECK arnoldi_eig %.3e %d %d\n", d, (int)er.WR.size(), (int)eg.WR.size());
   }
   const double tol = 1e-10;
   {

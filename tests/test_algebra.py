@@ -65,3 +65,31 @@ def check_pseudo_heat(rp, ci, vals, d, tol=1e-13):
 def test_oracle_pseudo_heat_operator_vs_reference():
     d, ph, A, S = pseudo_heat_oracle()
     check_pseudo_heat(S.row_ptr, S.col_idx, S.vals, d)
+
+
+# ---- arnoldi_eigenvalues (blocksp_solvers.hpp:306-334) ----
+EIG_CASES = ["arnoldi_eig_3d_bs8", "arnoldi_eig_harm_3d_bs8"]
+
+
+def load_eig(name):
+    d = np.load(GOLDEN / f"{name}.npz")
+    meta = json.loads(str(d["meta"]))
+    s = systems.grid_system(tuple(meta["dims"]), meta["bs"], seed=meta["seed"], skew=meta["skew"])
+    return d["wr"] + 1j * d["wi"], meta, s
+
+
+def match_eigs(got, ref, tol):
+    """Every reference value has a computed value within tol * max |lambda| (and vice versa)."""
+    got, ref = np.asarray(got), np.asarray(ref)
+    assert len(got) == len(ref)
+    scale = np.abs(ref).max()
+    d1 = np.abs(got[:, None] - ref[None, :]).min(axis=0)
+    d2 = np.abs(got[:, None] - ref[None, :]).min(axis=1)
+    assert max(d1.max(), d2.max()) <= tol * scale, (d1.max(), d2.max())
+
+
+@pytest.mark.parametrize("name", EIG_CASES)
+def test_oracle_arnoldi_eigenvalues_vs_reference(name):
+    ref, meta, s = load_eig(name)
+    got = O.arnoldi_eigenvalues(O.BSR.from_system(s), meta["iters"], harmonic=bool(meta["harmonic"]))
+    match_eigs(got, ref, 1e-9)

@@ -60,3 +60,43 @@ def test_gpu_pseudo_heat_operator_and_solves(handle):
     assert abs(info["iters"] - int(d["gmres_iters"])) <= 2
     check_history(hist, list(d["gmres_hist"]))
     assert rel(x, d["gmres_x"]) <= 1e-8
+
+
+# ---- arnoldi_eigenvalues on the GPU (blocksp_solvers.hpp:306-334) ----
+from test_algebra import EIG_CASES, load_eig, match_eigs  # noqa: E402
+
+
+@pytest.mark.parametrize("name", EIG_CASES)
+def test_gpu_arnoldi_eigenvalues_vs_reference(handle, name):
+    import blocksp_b200 as bsp
+    ref, meta, s = load_eig(name)
+    A = bsp.Matrix.from_system(s, handle)
+    e = bsp.arnoldi_eigenvalues(A, meta["iters"], harmonic_Ritz=bool(meta["harmonic"]))
+    match_eigs(e.real() + 1j * e.imag(), ref, 1e-9)
+    assert abs(e.cond_number() - np.abs(ref).max() / np.abs(ref).min()) <= 1e-6 * e.cond_number()
+
+
+def test_gpu_arnoldi_eigenvalues_preconditioned_vs_oracle(handle):
+    """With block ILU0 (the reference build's preconditioned form ends in a
+    segmentation fault, so the oracle is the check): harmonic Ritz values of
+    M^-1 A after 20 steps."""
+    import blocksp_b200 as bsp
+    import oracle.blocksp_oracle as O
+    from blocksp_b200 import systems
+    s = systems.grid_system((5, 5, 5), 8, seed=72, skew=0.3)
+    A = bsp.Matrix.from_system(s, handle)
+    e = bsp.arnoldi_eigenvalues(A, 20, bsp.ILU0(A), harmonic_Ritz=True)
+    Ao = O.BSR.from_system(s)
+    ref = O.arnoldi_eigenvalues(Ao, 20, O.ILU0(Ao), harmonic=True)
+    match_eigs(e.real() + 1j * e.imag(), ref, 1e-8)
+
+
+def test_gpu_pgmres_print_eig_info(handle, capfd):
+    """pGMRES(printEigInfo) prints the harmonic Ritz summary after a restart."""
+    import blocksp_b200 as bsp
+    from blocksp_b200 import systems
+    s = systems.grid_system((6, 6, 6), 8, seed=13, skew=0.3)
+    A = bsp.Matrix.from_system(s, handle)
+    bsp.pGMRES(A, s.b, 1e-10, bsp.ILU0(A), 5000, 10, 4, printIters=True, printEigInfo=True)
+    out = capfd.readouterr().out
+    assert "pGMRES iters" in out and "Harmonic Ritz info" in out and "ratio/cond" in out

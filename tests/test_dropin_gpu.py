@@ -41,9 +41,19 @@ def test_dropin_binary_is_built():
     assert EXE.exists(), "build with __graft_entry__.build() (oracle/Makefile target _ref/dropin_test)"
 
 
+def check_algebra(out):
+    """bsmm / bs_tr / bs_id: same block order per row and values within 1e-13;
+    Arnoldi Ritz values (12 steps) within 1e-8 of the reference's."""
+    for name in ("bsmm", "bsmm_t", "bs_tr", "bs_id"):
+        assert out[name][0] <= 1e-13, (name, out[name])
+    d, n_ref, n_gpu = out["arnoldi_eig"]
+    assert d <= 1e-8 and n_ref == n_gpu, out["arnoldi_eig"]
+
+
 def test_dropin_spd_2d(tmp_path):
     out = run(tmp_path, systems.grid_system((12, 12), 4, seed=61), 2, 2, True)
     assert out["bsmv"][0] <= 1e-14
+    check_algebra(out)
     for name in ("ilu0_pgmres_dr", "sor_pgmres", "ichol0_pcg", "sor_pcg"):
         d, ir, ig = out[name]
         assert d <= 1e-8 and abs(ir - ig) <= 2, (name, out[name])
@@ -52,6 +62,7 @@ def test_dropin_spd_2d(tmp_path):
 def test_dropin_nonsymmetric_3d(tmp_path):
     out = run(tmp_path, systems.grid_system((6, 6, 6), 8, seed=62, skew=0.3), 4, 2, False)
     assert out["bsmv"][0] <= 1e-14
+    check_algebra(out)
     for name in ("ilu0_pgmres_dr", "sor_pgmres"):
         d, ir, ig = out[name]
         assert d <= 1e-8 and abs(ir - ig) <= 2, (name, out[name])
