@@ -21,6 +21,7 @@ PC_NONE, PC_DIAG_LU, PC_DIAG_CHOL, PC_SOR_LU, PC_SOR_CHOL, PC_ILU0, PC_ICHOL0 = 
 PC_LEARNED_LLT, PC_LEARNED_LU = 7, 8
 PREC_F64, PREC_F32, PREC_BF16 = 0, 1, 2
 STOP_REFERENCE, STOP_TRUE_RESIDUAL = 0, 1
+LEARNED_LU, LEARNED_LLT = 0, 1
 
 
 class BspError(RuntimeError):
@@ -108,6 +109,7 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_batch_results": (_I, [_P, _I, _P, _P, _P, _P, _I]),
     "bsp_learned_create": (_I, [_P, _I, _I, C.POINTER(_P)]),
     "bsp_learned_destroy": (_I, [_P]),
+    "bsp_learned_set_form": (_I, [_P, _I]),
     "bsp_learned_param_count": (_I, [_P, C.POINTER(_I64)]),
     "bsp_learned_set_params": (_I, [_P, _P, _I64]),
     "bsp_learned_get_params": (_I, [_P, _P, _I64]),

@@ -1,6 +1,7 @@
-// learned.cu — learned block-LU preconditioner: a message-passing network over
+// learned.cu — learned block preconditioner: a message-passing network over
 // the block graph of A, with hand-written forward and backward kernels, trained
-// on the GPU, whose output corrects the block-ILU0 factors.
+// on the GPU, whose output corrects the block-ILU0 factors (LU form, for
+// pGMRES) or the block-IChol0 factor (L L^T form, for pCG on SPD systems).
 //
 // No reference counterpart: the reference's preconditioners end at IChol0
 // (blocksp_preconditioners.hpp:364-538).  The factors keep A's sparsity and
@@ -66,12 +67,22 @@ struct Graph {
 
 template <typename T> __device__ __forceinline__ T relu(T v) { return v > T(0) ? v : T(0); }
 
-// Output scale of the correction of block (i, j): the scale of U_ij for j > i,
-// of L_ij = A_ij U_jj^-1 for j < i.
-template <typename T> __device__ __forceinline__ T edge_scale(const T* s, int i, int j) {
+// Output scale of the correction of block (i, j).  LU form: the scale of U_ij
+// for j > i, of L_ij = A_ij U_jj^-1 for j < i.  L L^T form (llt): the scale of
+// L_ij = A_ij L_jj^-T, sqrt(s_i), for j < i; upper blocks are not part of L
+// (scale 0, so they get neither an output nor a gradient).
+template <typename T> __device__ __forceinline__ T edge_scale(const T* s, int i, int j, int llt) {
   const T si = s[i], sj = s[j];
+  if (llt) return j < i ? T(kAlpha) * sqrt(si) : T(0);
   return T(kAlpha) * (j < i ? sqrt(si / sj) : sqrt(si * sj));
 }
+// Diagonal-block scale: s_i (U_ii ~ A_ii) or sqrt(s_i) (L_ii ~ A_ii^1/2).
+template <typename T> __device__ __forceinline__ T diag_scale(const T* s, int i, int llt) {
+  return T(kAlpha) * (llt ? sqrt(s[i]) : s[i]);
+}
+// L L^T form: the diagonal correction is lower triangular (L_ii stays a
+// triangular factor), entry o = r * 8 + c of the row-major block.
+__device__ __forceinline__ bool diag_kept(int o, int llt) { return !llt || (o % 8) <= (o / 8); }
 
 // ------------------------------------------------------------------ row kernels
 // out(r, o) = sum_t W[o][t] in_r[t] + b[o], o < NOUT: one warp per row.
@@ -295,16 +306,18 @@ template <typename T> struct DecEdgeOut {          // dF[blk] = edge_scale v
   const int* col;
   const int* blk;
   double* dF;
+  int llt;
   __device__ void store(int k, int o, T v) const {
-    dF[(int64_t)blk[k] * kB2 + o] = double(edge_scale(s, row[k], col[k]) * v);
+    dF[(int64_t)blk[k] * kB2 + o] = double(edge_scale(s, row[k], col[k], llt) * v);
   }
 };
 template <typename T> struct DecDiagOut {
   const T* s;
   const int* diag;
   double* dF;
+  int llt;
   __device__ void store(int i, int o, T v) const {
-    dF[(int64_t)diag[i] * kB2 + o] = double(T(kAlpha) * s[i] * v);
+    dF[(int64_t)diag[i] * kB2 + o] = diag_kept(o, llt) ? double(diag_scale(s, i, llt) * v) : 0.0;
   }
 };
 
@@ -315,8 +328,9 @@ template <typename T> struct GEdgeDec {            // edge_scale gdF[blk[k]]
   const int* col;
   const int* blk;
   const T* gdF;
+  int llt;
   __device__ void load(int k, T* dst, int lane) const {
-    const T sc = edge_scale(s, row[k], col[k]);
+    const T sc = edge_scale(s, row[k], col[k], llt);
     for (int o = lane; o < kB2; o += 32) dst[o] = sc * gdF[(int64_t)blk[k] * kB2 + o];
   }
 };
@@ -324,9 +338,11 @@ template <typename T> struct GDiagDec {
   const T* s;
   const int* diag;
   const T* gdF;
+  int llt;
   __device__ void load(int i, T* dst, int lane) const {
-    const T sc = T(kAlpha) * s[i];
-    for (int o = lane; o < kB2; o += 32) dst[o] = sc * gdF[(int64_t)diag[i] * kB2 + o];
+    const T sc = diag_scale(s, i, llt);
+    for (int o = lane; o < kB2; o += 32)
+      dst[o] = diag_kept(o, llt) ? sc * gdF[(int64_t)diag[i] * kB2 + o] : T(0);
   }
 };
 template <typename T> struct GMask {               // g[r] * (act[r] > 0)
@@ -448,6 +464,56 @@ __global__ void k_factor_grad(int n, int bs, int K, int64_t N, const int* __rest
         double acc = 0.0;
         for (int k = 0; k < K; ++k)
           acc = fma(left[(int64_t)k * N + (int64_t)i * bs + r], right[(int64_t)k * N + (int64_t)j * bs + c], acc);
+        gdF[perm[b] * b2 + e] = T(-acc);
+      }
+    }
+  }
+}
+
+// L L^T form.  loss = (1/K) sum_k ||M^-1 A q_k - q_k||^2 with M = L L^T: with
+// z = M^-1 A q, g = (2/K)(z - q), w = M^-1 g (M is symmetric), y = L^T z and
+// u = L^T w,
+//   d loss / d L_ij = -sum_k (w_k[i] y_k[j]^T + z_k[i] u_k[j]^T)   (j <= i)
+// y = L^T z over the transposed strictly-lower structure plus the diagonal.
+__global__ void k_lower_t_prod(int n, int bs, const int* __restrict__ tptr, const int* __restrict__ trow,
+                               const int64_t* __restrict__ tblk, const int* __restrict__ fdiag,
+                               const double* __restrict__ f, const double* __restrict__ z, double* __restrict__ y) {
+  const int64_t N = (int64_t)n * bs;
+  const int b2 = bs * bs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / bs), c = (int)(e % bs);
+    double acc = 0.0;
+    const double* d = f + (int64_t)fdiag[i] * b2;
+    for (int r = 0; r < bs; ++r) acc = fma(d[r * bs + c], z[(int64_t)i * bs + r], acc);
+    for (int t = tptr[i]; t < tptr[i + 1]; ++t) {
+      const double* blk = f + tblk[t] * b2;  // L_{trow[t], i}
+      const int j = trow[t];
+      for (int r = 0; r < bs; ++r) acc = fma(blk[r * bs + c], z[(int64_t)j * bs + r], acc);
+    }
+    y[e] = acc;
+  }
+}
+template <typename T>
+__global__ void k_factor_grad_llt(int n, int bs, int K, int64_t N, const int* __restrict__ fptr,
+                                  const int* __restrict__ fcol, const int* __restrict__ fdiag,
+                                  const int64_t* __restrict__ perm, const double* __restrict__ w,
+                                  const double* __restrict__ y, const double* __restrict__ z,
+                                  const double* __restrict__ u, T* __restrict__ gdF) {
+  const int lane = threadIdx.x & 31;
+  const int b2 = bs * bs;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
+    for (int b = fptr[i]; b < fptr[i + 1]; ++b) {
+      const int j = fcol[b];
+      const bool diag = b == fdiag[i];
+      for (int e = lane; e < b2; e += 32) {
+        const int r = e / bs, c = e % bs;
+        double acc = 0.0;
+        if (!diag || c <= r)
+          for (int k = 0; k < K; ++k) {
+            const int64_t oi = (int64_t)k * N + (int64_t)i * bs + r, oj = (int64_t)k * N + (int64_t)j * bs + c;
+            acc = fma(w[oi], y[oj], acc);
+            acc = fma(z[oi], u[oj], acc);
+          }
         gdF[perm[b] * b2 + e] = T(-acc);
       }
     }
@@ -599,6 +665,7 @@ struct bsp_learned_s {
   bsp_handle_t h = nullptr;
   int device = 0;
   int bs = 0, dtype = 0;
+  int form = BSP_LEARNED_LU;  // factor form the network emits
   int64_t n_params = 0;
   std::vector<ParamSlot> slots;
   std::unique_ptr<ModelBase> impl;
@@ -739,10 +806,13 @@ template <typename T> struct Model : ModelBase {
     const T* hL = hs.get() + (size_t)kLayers * n * H;
     const int so = 2 + 2 * kLayers;
     double* dst = out ? out : dF.get();
+    const int llt = M->form == BSP_LEARNED_LLT;
+    if (llt) BSP_CUDA_TRY(cudaMemsetAsync(dst, 0, (size_t)A->nnzb * kB2 * sizeof(double), h->stream));
     BSP_TRY((run_dense<T, 3 * H, kB2>(h, E, W(so), B(so), DecIn<T>{hL, e.get(), G.e_row.get(), G.e_col.get()},
-                                      DecEdgeOut<T>{s.get(), G.e_row.get(), G.e_col.get(), G.e_blk.get(), dst})));
+                                      DecEdgeOut<T>{s.get(), G.e_row.get(), G.e_col.get(), G.e_blk.get(), dst,
+                                                    llt})));
     BSP_TRY((run_dense<T, H, kB2>(h, n, W(so + 1), B(so + 1), RowIn<T, H>{hL},
-                                  DecDiagOut<T>{s.get(), G.diag_pos.get(), dst})));
+                                  DecDiagOut<T>{s.get(), G.diag_pos.get(), dst, llt})));
     return BSP_OK;
   }
 
@@ -753,12 +823,14 @@ template <typename T> struct Model : ModelBase {
     BSP_TRY(run_forward(h, A, nullptr));
     const int n = G.n, E = G.E, Es = std::max(E, 1), bs = 8;
     const int64_t N = (int64_t)n * bs;
-    if (!work || work->A != A || work->n != n || work->f_nnzb != ilu->f_nnzb) {
+    const int llt = M->form == BSP_LEARNED_LLT;
+    const int wkind = llt ? BSP_PC_LEARNED_LLT : BSP_PC_LEARNED_LU;
+    if (!work || work->A != A || work->n != n || work->f_nnzb != ilu->f_nnzb || work->kind != wkind) {
       work = std::make_unique<bsp_precond_s>();
       work->h = h;
       work->device = h->device;
       work->A = const_cast<bsp_matrix_s*>(A);
-      work->kind = BSP_PC_LEARNED_LU;
+      work->kind = wkind;
       work->n = n;
       work->bs = bs;
       work->precision = BSP_PREC_F64;
@@ -782,22 +854,42 @@ template <typename T> struct Model : ModelBase {
       bsp::count_launch(), k_diff<<<eg, 256, 0, h->stream>>>(N, z, q, le.get());
       BSP_TRY(bsp_dot_dev(h, N, le.get(), le.get(), lsc.get() + k));
       bsp::count_launch(), k_scale<<<eg, 256, 0, h->stream>>>(N, 2.0 / K, le.get());
-      BSP_TRY(precond_apply_transposed(work.get(), le.get(), lw.get() + (int64_t)k * N, llam.get() + (int64_t)k * N));
-      bsp::count_launch(), k_upper_prod<<<eg, 256, 0, h->stream>>>(n, bs, work->f_ptr.get(), work->f_col.get(),
-                                                                   work->f_diag.get(), work->f_vals.get(), z,
-                                                                   ly.get() + (int64_t)k * N);
+      if (llt) {
+        // w = M^-1 g (M = L L^T is symmetric); y = L^T z, u = L^T w (u in llam)
+        double* wk = lw.get() + (int64_t)k * N;
+        BSP_TRY(precond_apply(work.get(), BSP_PREC_F64, le.get(), wk));
+        bsp::count_launch(), k_lower_t_prod<<<eg, 256, 0, h->stream>>>(
+            n, bs, work->t_ptr.get(), work->t_row.get(), work->t_blk.get(), work->f_diag.get(), work->f_vals.get(), z,
+            ly.get() + (int64_t)k * N);
+        bsp::count_launch(), k_lower_t_prod<<<eg, 256, 0, h->stream>>>(
+            n, bs, work->t_ptr.get(), work->t_row.get(), work->t_blk.get(), work->f_diag.get(), work->f_vals.get(), wk,
+            llam.get() + (int64_t)k * N);
+      } else {
+        BSP_TRY(precond_apply_transposed(work.get(), le.get(), lw.get() + (int64_t)k * N, llam.get() + (int64_t)k * N));
+        bsp::count_launch(), k_upper_prod<<<eg, 256, 0, h->stream>>>(n, bs, work->f_ptr.get(), work->f_col.get(),
+                                                                     work->f_diag.get(), work->f_vals.get(), z,
+                                                                     ly.get() + (int64_t)k * N);
+      }
     }
     const int ng = (int)std::min<int64_t>(ceil_div((int64_t)n * 32, 256), (int64_t)h->num_sms * 16);
-    bsp::count_launch(), k_factor_grad<T><<<ng, 256, 0, h->stream>>>(n, bs, K, N, work->f_ptr.get(), work->f_col.get(),
-                                                                    work->f_diag.get(), work->d_perm.get(), llam.get(),
-                                                                    ly.get(), lw.get(), lz.get(), gdF.get());
+    if (llt) {
+      // upper blocks of A are not in L: their gradient is zero
+      BSP_CUDA_TRY(cudaMemsetAsync(gdF.get(), 0, (size_t)A->nnzb * kB2 * sizeof(T), h->stream));
+      bsp::count_launch(), k_factor_grad_llt<T><<<ng, 256, 0, h->stream>>>(
+          n, bs, K, N, work->f_ptr.get(), work->f_col.get(), work->f_diag.get(), work->d_perm.get(), lw.get(),
+          ly.get(), lz.get(), llam.get(), gdF.get());
+    } else {
+      bsp::count_launch(), k_factor_grad<T><<<ng, 256, 0, h->stream>>>(n, bs, K, N, work->f_ptr.get(), work->f_col.get(),
+                                                                      work->f_diag.get(), work->d_perm.get(), llam.get(),
+                                                                      ly.get(), lw.get(), lz.get(), gdF.get());
+    }
     BSP_CUDA_TRY(cudaPeekAtLastError());
     const Graph gr = G.view();
     // network backward: decoders
     const T* hL = hs.get() + (size_t)kLayers * n * H;
     const int so = 2 + 2 * kLayers;
-    GEdgeDec<T> ge{s.get(), G.e_row.get(), G.e_col.get(), G.e_blk.get(), gdF.get()};
-    GDiagDec<T> gd{s.get(), G.diag_pos.get(), gdF.get()};
+    GEdgeDec<T> ge{s.get(), G.e_row.get(), G.e_col.get(), G.e_blk.get(), gdF.get(), llt};
+    GDiagDec<T> gd{s.get(), G.diag_pos.get(), gdF.get(), llt};
     if (E > 0) {
       BSP_TRY((run_wgrad<T, 3 * H, kB2>(h, E, ge, DecIn<T>{hL, e.get(), G.e_row.get(), G.e_col.get()}, part.get(),
                                         Gp(so))));
@@ -902,6 +994,12 @@ int bsp_learned_create(bsp_handle_t h, int bs, int dtype, bsp_learned_t* out) {
   return BSP_OK;
 }
 
+int bsp_learned_set_form(bsp_learned_t M, int form) {
+  if (!M || (form != BSP_LEARNED_LU && form != BSP_LEARNED_LLT)) return BSP_INVALID;
+  M->form = form;
+  return BSP_OK;
+}
+
 int bsp_learned_destroy(bsp_learned_t M) {
   if (!M) return BSP_OK;
   cudaSetDevice(M->device);
@@ -942,9 +1040,11 @@ int bsp_learned_forward(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, double*
 }
 
 int bsp_learned_ilu_factors(bsp_handle_t h, bsp_precond_t ilu, double* F0) {
-  if (!h || !ilu || !F0 || ilu->kind != BSP_PC_ILU0) return BSP_INVALID;
+  if (!h || !ilu || !F0 || (ilu->kind != BSP_PC_ILU0 && ilu->kind != BSP_PC_ICHOL0)) return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
   const int b2 = ilu->bs * ilu->bs;
+  // IChol0 covers A's lower blocks only: the others are zero
+  BSP_CUDA_TRY(cudaMemsetAsync(F0, 0, (size_t)ilu->A->nnzb * b2 * sizeof(double), h->stream));
   bsp::count_launch(), k_scatter_f0<<<grid_for(h, ilu->f_nnzb * b2, 256), 256, 0, h->stream>>>(
       ilu->f_nnzb, b2, ilu->d_perm.get(), ilu->f_vals.get(), F0);
   BSP_CUDA_TRY(cudaPeekAtLastError());
@@ -955,7 +1055,7 @@ int bsp_learned_ilu_factors(bsp_handle_t h, bsp_precond_t ilu, double* F0) {
 int bsp_learned_loss_grad(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, bsp_precond_t ilu, int n_probes,
                           const double* probes, double* loss) {
   if (!h || !M || !A || !ilu || !probes || !loss || n_probes < 1 || A->bs != M->bs || ilu->A != A ||
-      ilu->kind != BSP_PC_ILU0)
+      ilu->kind != (M->form == BSP_LEARNED_LLT ? BSP_PC_ICHOL0 : BSP_PC_ILU0))
     return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
   return M->impl->loss_grad(h, A, ilu, n_probes, probes, loss);
@@ -1034,7 +1134,7 @@ int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int pre
   pc->h = h;
   pc->device = h->device;
   pc->A = A;
-  pc->kind = BSP_PC_LEARNED_LU;
+  pc->kind = M->form == BSP_LEARNED_LLT ? BSP_PC_LEARNED_LLT : BSP_PC_LEARNED_LU;
   pc->n = A->n_rows;
   pc->bs = A->bs;
   pc->precision = precision;

@@ -1251,8 +1251,9 @@ __global__ void k_add_perm(int64_t nblk, int b2, const int64_t* __restrict__ per
     f[e] += dF[perm[e / b2] * b2 + e % b2];
 }
 
-// Learned LU: the block-ILU0 factors plus a correction dF given in A's block
-// order; the diagonal inverses are recomputed from the corrected U_ii.
+// Learned factors: the block-ILU0 factors (LU form) or the block-IChol0 factor
+// (L L^T form) plus a correction dF given in A's block order; the diagonal
+// inverses are recomputed from the corrected U_ii / L_ii (general inverses).
 int precond_build_learned(bsp_precond_s* pc, const double* dF) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
   stream_invalidate(pc);
@@ -1260,9 +1261,11 @@ int precond_build_learned(bsp_precond_s* pc, const double* dF) {
   BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
   BSP_TRY(take(pc->A, pc->ticket, 1));
   BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
-  BSP_TRY(build_factor_structure(pc, false));
-  BSP_TRY(run_factor(pc, FACT_ILU0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(), pc->f_diag.get(),
-                     pc->f_vals.get(), n));
+  // LU form on the ILU0 factors; L L^T form on the IChol0 factor (A.lowTri())
+  const bool llt = pc->kind == BSP_PC_LEARNED_LLT;
+  BSP_TRY(build_factor_structure(pc, llt));
+  BSP_TRY(run_factor(pc, llt ? FACT_ICHOL0 : FACT_ILU0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(),
+                     pc->f_diag.get(), pc->f_vals.get(), n));
   const int64_t tot = pc->f_nnzb * b2;
   if (tot > 0)
     bsp::count_launch(), k_add_perm<<<grid_for(pc->h, tot, 256), 256, 0, pc->h->stream>>>(
@@ -1565,7 +1568,7 @@ int precond_learned_init(bsp_precond_s* pc) {
   BSP_TRY(take(pc->A, pc->flags, std::max(n, 1)));
   BSP_TRY(take(pc->A, pc->ticket, 1));
   BSP_CUDA_TRY(cudaMemset(pc->flags.get(), 0, std::max(n, 1) * sizeof(int)));
-  return build_factor_structure(pc, false);
+  return build_factor_structure(pc, pc->kind == BSP_PC_LEARNED_LLT);
 }
 
 // work's factors = ilu's factors + dF (A order); work shares ilu's structure
@@ -1737,14 +1740,15 @@ int bsp_precond_export(bsp_precond_t pc, double* vals_host, int64_t capacity) {
   BSP_CUDA_TRY(cudaSetDevice(pc->device));
   const int b2 = pc->bs * pc->bs;
   bsp_handle_s* h = pc->h;
-  if (pc->kind == BSP_PC_ILU0 || pc->kind == BSP_PC_ICHOL0 || pc->kind == BSP_PC_LEARNED_LU) {
+  if (pc->kind == BSP_PC_ILU0 || pc->kind == BSP_PC_ICHOL0 || pc->kind == BSP_PC_LEARNED_LU ||
+      pc->kind == BSP_PC_LEARNED_LLT) {
     // blocks in the caller's layout: ILU0 / learned LU in A's block order; IChol0 in the
     // order of A.lowTri() (A's rows, blocks with col <= row in stored order)
     const int64_t nf = pc->f_nnzb;
     if (capacity < nf * b2) return BSP_INVALID;
     std::vector<double> f(nf * b2);
     BSP_CUDA_TRY(cudaMemcpy(f.data(), pc->f_vals.get(), f.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    if (pc->kind != BSP_PC_ICHOL0) {
+    if (pc->kind != BSP_PC_ICHOL0 && pc->kind != BSP_PC_LEARNED_LLT) {
       for (int64_t e = 0; e < nf; ++e)
         std::copy(f.begin() + e * b2, f.begin() + (e + 1) * b2, vals_host + pc->h_perm[e] * b2);
     } else {

@@ -1,11 +1,15 @@
-"""Learned block-LU preconditioner: host side of the network in learned.cu.
+"""Learned block preconditioner: host side of the network in learned.cu.
 
 The network (a 3-layer message-passing network, hidden width 32, over the block
 graph of A) is trained on the GPU by the library's own forward and backward
 kernels; this module drives it: parameter I/O, probe generation, the training
-loop, and ``LearnedLU(A, model)`` which builds the preconditioner, falling back
-to block ILU0 when the model did not beat ILU0's iteration count on its
-held-out validation systems.
+loop, and the preconditioners it builds, in two factor forms:
+
+* LU form (``LearnedLU``, pGMRES): corrects the block-ILU0 factors; falls back
+  to block ILU0 when the model did not beat ILU0's iteration count on its
+  held-out validation systems;
+* L L^T form (``LearnedLLT``, pCG on SPD systems): corrects the block-IChol0
+  factor; falls back to block IChol0 the same way.
 
 No reference counterpart (the reference's preconditioners end at IChol0,
 blocksp_preconditioners.hpp:364-538); the produced factors keep A's sparsity
@@ -27,6 +31,8 @@ from .api import Handle, Matrix, Precond, _ptr, default_handle
 LAYERS = 3
 HIDDEN = 32
 WEIGHTS = Path(__file__).resolve().parent / "weights" / "learned_convdiff_bs8.npz"
+WEIGHTS_LLT = Path(__file__).resolve().parent / "weights" / "learned_diffusion_llt_bs8.npz"
+FORMS = {"lu": _lib.LEARNED_LU, "llt": _lib.LEARNED_LLT}
 
 
 def param_shapes(bs: int = 8, H: int = HIDDEN, layers: int = LAYERS) -> dict[str, tuple]:
@@ -68,15 +74,17 @@ class LearnedModel:
     """Device-resident network parameters with their Adam state."""
 
     def __init__(self, handle: Handle | None = None, bs: int = 8, dtype: int = _lib.BSP_F32,
-                 params=None, meta: dict | None = None):
+                 params=None, meta: dict | None = None, form: str = "lu"):
         self.handle = handle or default_handle()
         self.bs = bs
         self.dtype = dtype
+        self.form = form
         m = C.c_void_p()
         check(self.handle.lib.bsp_learned_create(self.handle.h, bs, dtype, C.byref(m)), "bsp_learned_create",
               self.handle.h)
         self.m = m
         self.handle.adopt(self)
+        check(self.handle.lib.bsp_learned_set_form(self.m, FORMS[form]), "bsp_learned_set_form")
         cnt = C.c_int64()
         check(self.handle.lib.bsp_learned_param_count(self.m, C.byref(cnt)), "bsp_learned_param_count")
         self.n_params = cnt.value
@@ -110,7 +118,8 @@ class LearnedModel:
     def load(cls, path: str | Path = WEIGHTS, handle: Handle | None = None, dtype: int = _lib.BSP_F32):
         d = np.load(path)
         meta = json.loads(str(d["meta"]))
-        return cls(handle, int(meta.get("bs", 8)), dtype, params=d["params"], meta=meta)
+        return cls(handle, int(meta.get("bs", 8)), dtype, params=d["params"], meta=meta,
+                   form=meta.get("form", "lu"))
 
     # -------------------------------------------------------------- kernels
     def forward(self, A: Matrix):
@@ -138,7 +147,7 @@ class LearnedModel:
         p = C.c_void_p()
         check(self.handle.lib.bsp_learned_precond(self.handle.h, self.m, A.m, precision, C.byref(p)),
               "bsp_learned_precond", self.handle.h)
-        return Precond.wrap(A, p, _lib.PC_LEARNED_LU)
+        return Precond.wrap(A, p, _lib.PC_LEARNED_LLT if self.form == "llt" else _lib.PC_LEARNED_LU)
 
     def close(self) -> None:
         if getattr(self, "m", None):
@@ -199,38 +208,61 @@ def LearnedLU(A: Matrix, model: LearnedModel | None, precision: int = _lib.PREC_
     """The learned preconditioner, or block ILU0 when the model is absent or its
     validation showed no gain over ILU0's iteration count (the fallback)."""
     from .api import ILU0
-    if model is None or not model.meta.get("beats_ilu0", False):
+    if model is None or model.form != "lu" or not model.meta.get("beats_ilu0", False):
         return ILU0(A, precision)
+    return model.precond(A, precision)
+
+
+def LearnedLLT(A: Matrix, model: LearnedModel | None, precision: int = _lib.PREC_F64) -> Precond:
+    """The learned L L^T preconditioner for pCG on SPD systems, or block IChol0
+    when the model is absent or its validation showed no gain over IChol0's
+    iteration count (the fallback)."""
+    from .api import IChol0
+    if model is None or model.form != "llt" or not model.meta.get("beats_baseline", False):
+        return IChol0(A, precision)
     return model.precond(A, precision)
 
 
 # ------------------------------------------------------------------ training
 
-def solve_iters(A: Matrix, b, pc, tol: float = 1e-10, restart: int = 30, k: int = 10) -> tuple[int, float]:
-    """pGMRES(restart, k) iterations to the FP64 true residual tol, and that residual."""
-    from .api import pGMRES
-    _, info, _ = pGMRES(A, b, tol, pc, 5000, restart, k, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL)
+def solve_iters(A: Matrix, b, pc, tol: float = 1e-10, restart: int = 30, k: int = 10,
+                form: str = "lu") -> tuple[int, float]:
+    """Iterations to the FP64 true residual tol, and that residual: pGMRES(restart,
+    k) for the LU form, pCG for the L L^T form."""
+    from .api import pCG, pGMRES
+    if form == "llt":
+        _, info, _ = pCG(A, b, tol, pc, 20000, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL)
+    else:
+        _, info, _ = pGMRES(A, b, tol, pc, 5000, restart, k, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL)
     return int(info["iters"]), float(info["true_rel_res"])
+
+
+def training_system(dims, seed: int, form: str = "lu"):
+    """A training / validation system: 3D convection-diffusion (LU form) or the
+    same heterogeneous diffusion without convection, which is SPD (L L^T form)."""
+    from . import systems
+    return systems.convection_diffusion_system(dims, 8, int(seed), speed=0.0 if form == "llt" else 0.5)
 
 
 def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, epochs: int = 1,
           n_probes: int = 16, lr: float = 1e-4, handle: Handle | None = None, seed: int = 0,
-          n_smooth: int = 8, smooth_steps: int = 20, log=print) -> LearnedModel:
-    """Train on convection-diffusion systems (systems.convection_diffusion_system)
-    with the GPU kernels; then validate against ILU0 on held-out seeds and
-    record whether the model beats ILU0's iteration count (the fallback gate)."""
+          n_smooth: int = 8, smooth_steps: int = 20, log=print, form: str = "lu") -> LearnedModel:
+    """Train on convection-diffusion systems (LU form; SPD diffusion for the L L^T
+    form) with the GPU kernels; then validate against the baseline (ILU0 /
+    IChol0) on held-out seeds and record whether the model beats its iteration
+    count (the fallback gate)."""
     import torch
-    from . import systems
-    from .api import ILU0
+    from .api import IChol0, ILU0
     h = handle or default_handle()
-    model = LearnedModel(h, 8, _lib.BSP_F32, params=init_params(8, seed))
+    base = IChol0 if form == "llt" else ILU0
+    model = LearnedModel(h, 8, _lib.BSP_F32, params=init_params(8, seed), form=form)
     t0 = time.time()
     history = []
     for ep in range(epochs):
         for si, s in enumerate(train_seeds):
-            sysm = systems.convection_diffusion_system(dims, 8, int(s))
+            sysm = training_system(dims, s, form)
             A = Matrix.from_system(sysm, h)
-            ilu = ILU0(A)
+            ilu = base(A)
             Q = training_probes(A, ilu, torch.tensor(sysm.b, device="cuda"), n_probes - n_smooth, n_smooth,
                                 smooth_steps, int(s))
             for _ in range(steps_per_system):
@@ -243,26 +275,27 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
                 log(f"epoch {ep} system {si} loss {history[-1]:.6e} ({time.time() - t0:.0f}s)")
     val = []
     for s in val_seeds:
-        sysm = systems.convection_diffusion_system(dims, 8, int(s))
+        sysm = training_system(dims, s, form)
         A = Matrix.from_system(sysm, h)
-        ilu = ILU0(A)
-        it0, r0 = solve_iters(A, sysm.b, ilu)
+        ilu = base(A)
+        it0, r0 = solve_iters(A, sysm.b, ilu, form=form)
         lp = model.precond(A)
-        it1, r1 = solve_iters(A, sysm.b, lp)
+        it1, r1 = solve_iters(A, sysm.b, lp, form=form)
         val.append({"seed": int(s), "ilu0_iters": it0, "learned_iters": it1, "ilu0_res": r0, "learned_res": r1})
         lp.close()
         ilu.close()
         A.close()
-        log(f"validation seed {s}: ILU0 {it0} iterations, learned {it1}")
+        log(f"validation seed {s}: {base.__name__} {it0} iterations, learned {it1}")
     beats = bool(val) and sum(v["learned_iters"] for v in val) < sum(v["ilu0_iters"] for v in val) and \
         all(v["learned_res"] <= 1e-10 for v in val)
-    model.meta = {"bs": 8, "hidden": HIDDEN, "layers": LAYERS, "dims": list(dims),
+    model.meta = {"bs": 8, "hidden": HIDDEN, "layers": LAYERS, "dims": list(dims), "form": form,
+                  "baseline": base.__name__, "beats_baseline": beats,
                   "train_seeds": [int(s) for s in train_seeds], "val_seeds": [int(s) for s in val_seeds],
                   "steps_per_system": steps_per_system, "epochs": epochs, "n_probes": n_probes, "lr": lr,
                   "n_smooth": n_smooth, "smooth_steps": smooth_steps,
                   "loss_first": history[0] if history else None, "loss_last": history[-1] if history else None,
                   "loss_history": history[:: max(1, len(history) // 200)], "validation": val,
-                  "beats_ilu0": beats, "train_seconds": time.time() - t0}
+                  "beats_ilu0": beats and form == "lu", "train_seconds": time.time() - t0}
     return model
 
 
@@ -278,11 +311,13 @@ if __name__ == "__main__":  # pragma: no cover - the training run itself
     ap.add_argument("--lr", type=float, default=1e-4)
     ap.add_argument("--smooth", type=int, default=8)
     ap.add_argument("--smooth-steps", type=int, default=20)
-    ap.add_argument("--out", default=str(WEIGHTS))
+    ap.add_argument("--form", default="lu", choices=["lu", "llt"])
+    ap.add_argument("--out", default=None)
     a = ap.parse_args()
     tr = [10_000 + i for i in range(a.train)]
     va = [20_000 + i for i in range(a.val)]
     m = train(tr, va, (a.side,) * 3, a.steps, a.epochs, a.probes, a.lr, n_smooth=a.smooth,
-              smooth_steps=a.smooth_steps)
+              smooth_steps=a.smooth_steps, form=a.form)
+    a.out = a.out or str(WEIGHTS_LLT if a.form == "llt" else WEIGHTS)
     m.save(a.out)
     print(json.dumps({k: v for k, v in m.meta.items() if k != "loss_history"}))

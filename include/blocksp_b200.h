@@ -320,6 +320,14 @@ int bsp_batch_results(bsp_batch_t B, int nrhs, int* iters, int* state, double* f
 typedef struct bsp_learned_s* bsp_learned_t;
 
 int bsp_learned_create(bsp_handle_t h, int bs, int dtype, bsp_learned_t* out);
+/* Factor form the network emits (default BSP_LEARNED_LU): BSP_LEARNED_LU
+ * corrects the block-ILU0 factors (M = L U, pGMRES, BSP_PC_LEARNED_LU);
+ * BSP_LEARNED_LLT corrects the block-IChol0 factor (M = L L^T, SPD, pCG,
+ * BSP_PC_LEARNED_LLT; lower blocks only, diagonal corrections kept lower
+ * triangular).  loss_grad then takes an IChol0 preconditioner in place of
+ * ILU0.  No counterpart in the reference. */
+enum bsp_learned_form { BSP_LEARNED_LU = 0, BSP_LEARNED_LLT = 1 };
+int bsp_learned_set_form(bsp_learned_t M, int form);
 int bsp_learned_destroy(bsp_learned_t M);
 int bsp_learned_param_count(bsp_learned_t M, int64_t* count);
 int bsp_learned_set_params(bsp_learned_t M, const double* params, int64_t count);

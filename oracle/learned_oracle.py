@@ -103,8 +103,13 @@ def features(g: Graph, vals: np.ndarray):
     return s, x, a
 
 
-def forward(p: dict, g: Graph, vals: np.ndarray, L: int = 3):
-    """Returns dF (nnzb, bs, bs) in A's block order and the cache for backward."""
+def forward(p: dict, g: Graph, vals: np.ndarray, L: int = 3, form: str = "lu"):
+    """Returns dF (nnzb, bs, bs) in A's block order and the cache for backward.
+
+    form "llt" (the L L^T variant for SPD systems): the output scales are
+    alpha sqrt(s_i) for lower blocks (the scale of L_ij = A_ij L_jj^-T) and for
+    the diagonal (L_ii ~ A_ii^1/2), upper blocks get no correction, and the
+    diagonal correction is kept lower triangular."""
     bs = vals.shape[1]
     s, x, a = features(g, vals)
     h = relu(x @ p["Wn"].T + p["bn"])
@@ -121,12 +126,19 @@ def forward(p: dict, g: Graph, vals: np.ndarray, L: int = 3):
         us.append(u)
         hs.append(h)
     si, sj = s[g.e_row], s[g.e_col]
-    se = ALPHA * np.where(g.e_col < g.e_row, np.sqrt(si / sj), np.sqrt(si * sj))
+    if form == "llt":
+        se = ALPHA * np.where(g.e_col < g.e_row, np.sqrt(si), 0.0)
+        sd = ALPHA * np.sqrt(s)
+        dmask = np.tril(np.ones((bs, bs))).reshape(-1)
+    else:
+        se = ALPHA * np.where(g.e_col < g.e_row, np.sqrt(si / sj), np.sqrt(si * sj))
+        sd = ALPHA * s
+        dmask = np.ones(bs * bs)
     din = np.concatenate([h[g.e_row], h[g.e_col], e], axis=1)
     dF = np.zeros((len(g.col_idx), bs * bs))
     dF[g.e_blk] = se[:, None] * (din @ p["Wo"].T + p["bo"])
-    dF[g.diag_pos] = (ALPHA * s)[:, None] * (h @ p["Wd"].T + p["bd"])
-    cache = dict(s=s, x=x, a=a, e=e, hs=hs, msgs=msgs, ms=ms, us=us, se=se, din=din)
+    dF[g.diag_pos] = sd[:, None] * (h @ p["Wd"].T + p["bd"]) * dmask
+    cache = dict(s=s, x=x, a=a, e=e, hs=hs, msgs=msgs, ms=ms, us=us, se=se, sd=sd, dmask=dmask, din=din)
     return dF.reshape(-1, bs, bs), cache
 
 
@@ -173,6 +185,42 @@ def loss_and_factor_grad(g: Graph, vals: np.ndarray, F: np.ndarray, Q: np.ndarra
     return loss, gF
 
 
+def llt_dense(g: Graph, F: np.ndarray) -> np.ndarray:
+    """L: the lower blocks of F (diagonal blocks lower triangular), dense."""
+    n, bs = g.n, F.shape[1]
+    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
+    diag = g.col_idx == rows
+    lower = g.col_idx < rows
+    Fl = np.where(lower[:, None, None], F, 0.0) + np.where(diag[:, None, None], np.tril(F), 0.0)
+    return dense_of(g, Fl)
+
+
+def loss_and_factor_grad_llt(g: Graph, vals: np.ndarray, F: np.ndarray, Q: np.ndarray):
+    """L L^T form: loss = (1/K) sum ||M^-1 A q - q||^2, M = L L^T, and d loss / d F
+    (nnzb, bs, bs): with z = M^-1 A q, g = (2/K)(z - q), w = M^-1 g, y = L^T z,
+    u = L^T w,  d loss / d L_ij = -(w_i y_j^T + z_i u_j^T) for j <= i (lower
+    triangle of the diagonal blocks), zero for upper blocks."""
+    n, bs = g.n, vals.shape[1]
+    rows = np.repeat(np.arange(n), np.diff(g.row_ptr))
+    K = Q.shape[0]
+    A = dense_of(g, vals)
+    Ld = llt_dense(g, F)
+    M = Ld @ Ld.T
+    Z = np.linalg.solve(M, A @ Q.T)
+    E = Z - Q.T
+    loss = float(np.sum(E * E)) / K
+    W = np.linalg.solve(M, 2.0 * E / K)
+    Y, U = Ld.T @ Z, Ld.T @ W
+    gF = np.zeros_like(F)
+    for b, (i, j) in enumerate(zip(rows, g.col_idx)):
+        if j > i:
+            continue
+        si, sj = slice(i * bs, (i + 1) * bs), slice(j * bs, (j + 1) * bs)
+        gb = -(W[si] @ Y[sj].T + Z[si] @ U[sj].T)
+        gF[b] = np.tril(gb) if i == j else gb
+    return loss, gF
+
+
 def backward(p: dict, g: Graph, cache: dict, gdF: np.ndarray, L: int = 3) -> dict:
     """Parameter gradients given d loss / d dF (nnzb, bs, bs)."""
     B2 = gdF.shape[1] * gdF.shape[2]
@@ -185,7 +233,7 @@ def backward(p: dict, g: Graph, cache: dict, gdF: np.ndarray, L: int = 3) -> dic
     grads["Wo"] = go.T @ cache["din"]
     grads["bo"] = go.sum(0)
     gdin = go @ p["Wo"]                                      # (E, 3H)
-    gd = (ALPHA * s)[:, None] * gdF[g.diag_pos]              # (n, B2)
+    gd = cache["sd"][:, None] * gdF[g.diag_pos] * cache["dmask"]  # (n, B2)
     grads["Wd"] = gd.T @ hs[-1]
     grads["bd"] = gd.sum(0)
     dh = gd @ p["Wd"]
@@ -217,23 +265,29 @@ def backward(p: dict, g: Graph, cache: dict, gdF: np.ndarray, L: int = 3) -> dic
     return grads
 
 
-def loss_fn(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3) -> float:
-    dF, _ = forward(p, g, vals, L)
-    return loss_and_factor_grad(g, vals, F0 + dF, Q)[0]
+def _factor_loss(form: str):
+    return loss_and_factor_grad_llt if form == "llt" else loss_and_factor_grad
 
 
-def loss_and_grads(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3):
-    dF, cache = forward(p, g, vals, L)
-    loss, gF = loss_and_factor_grad(g, vals, F0 + dF, Q)
+def loss_fn(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3,
+            form: str = "lu") -> float:
+    dF, _ = forward(p, g, vals, L, form)
+    return _factor_loss(form)(g, vals, F0 + dF, Q)[0]
+
+
+def loss_and_grads(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3,
+                   form: str = "lu"):
+    dF, cache = forward(p, g, vals, L, form)
+    loss, gF = _factor_loss(form)(g, vals, F0 + dF, Q)
     return loss, backward(p, g, cache, gF, L)
 
 
 def finite_difference(p: dict, g: Graph, vals, F0, Q, name: str, idx: tuple, h: float = 1e-6,
-                      L: int = 3) -> float:
+                      L: int = 3, form: str = "lu") -> float:
     """Central difference of the loss in one parameter entry."""
     q = {k: v.copy() for k, v in p.items()}
     q[name][idx] += h
-    lp = loss_fn(q, g, vals, F0, Q, L)
+    lp = loss_fn(q, g, vals, F0, Q, L, form)
     q[name][idx] -= 2 * h
-    lm = loss_fn(q, g, vals, F0, Q, L)
+    lm = loss_fn(q, g, vals, F0, Q, L, form)
     return (lp - lm) / (2 * h)

@@ -89,3 +89,54 @@ def test_gaussian_field_statistics():
     # correlation at lag 8 along x near exp(-1/2)
     a = (f * np.roll(f, 8, axis=2)).mean() / f.var()
     assert 0.3 < a < 0.9
+
+
+# ---- the L L^T form (SPD systems, pCG) ----
+def ichol0_in_a_order(s):
+    """The block-IChol0 factor of s in A's block order (upper blocks zero)."""
+    L = O.IChol0(O.BSR.from_system(s)).L
+    F = np.zeros_like(s.vals)
+    for i in range(s.n):
+        lo = [t for t in range(s.row_ptr[i], s.row_ptr[i + 1]) if s.col_idx[t] <= i]
+        F[lo] = L.vals[L.row_ptr[i]:L.row_ptr[i + 1]]
+    return F
+
+
+def small_spd_case(seed=9, dims=(4, 3, 3)):
+    s = systems.convection_diffusion_system(dims, 8, seed, speed=0.0)
+    return s, LO.graph_of(s.row_ptr, s.col_idx), ichol0_in_a_order(s)
+
+
+def test_llt_oracle_gradients_match_finite_differences():
+    s, g, F0 = small_spd_case()
+    rng = np.random.default_rng(5)
+    p = LO.init_params(8, seed=6)
+    for k in p:
+        p[k] = p[k] + (0.005 if k in ("Wo", "bo", "Wd", "bd") else 0.05) * rng.standard_normal(p[k].shape)
+    Q = np.linalg.qr(rng.standard_normal((s.n * 8, 3)))[0].T
+    _, gr = LO.loss_and_grads(p, g, s.vals, F0, Q, form="llt")
+    worst = 0.0
+    for name in p:
+        for _ in range(2):
+            idx = tuple(int(rng.integers(0, d)) for d in p[name].shape)
+            fd = LO.finite_difference(p, g, s.vals, F0, Q, name, idx, h=1e-5, form="llt")
+            an = gr[name][idx]
+            worst = max(worst, abs(fd - an) / max(1e-8, abs(fd) + abs(an)))
+    assert worst <= 1e-5, worst
+
+
+def test_llt_form_keeps_the_factor_lower_and_spd():
+    s, g, F0 = small_spd_case()
+    rng = np.random.default_rng(8)
+    p = LO.init_params(8, seed=2)
+    p["Wd"] += 0.01 * rng.standard_normal(p["Wd"].shape)
+    p["Wo"] += 0.01 * rng.standard_normal(p["Wo"].shape)
+    dF, _ = LO.forward(p, g, s.vals, form="llt")
+    rows = np.repeat(np.arange(s.n), np.diff(s.row_ptr))
+    assert not np.any(dF[s.col_idx > rows])                        # no upper corrections
+    assert not np.any(np.triu(dF[s.col_idx == rows], 1))           # triangular diagonal corrections
+    Ld = LO.llt_dense(g, F0 + dF)
+    assert np.all(np.linalg.eigvalsh(Ld @ Ld.T) > 0)
+    # with zero decoders the factor is IChol0's: L L^T = the reference's IC(0)
+    dF0, _ = LO.forward(LO.init_params(8, seed=2), g, s.vals, form="llt")
+    assert not np.any(dF0)
