@@ -78,6 +78,8 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_handle_sync": (_I, [_P]),
     "bsp_handle_stream": (_P, [_P]),
     "bsp_handle_set_spin_limit": (_I, [_P, C.c_uint]),
+    "bsp_release_cached_memory": (_I, [_I]),
+    "bsp_cached_memory": (_I, [_I, C.POINTER(_I64)]),
     "bsp_matrix_create": (_I, [_P, _I, _I, _I, _I64, _P, _P, _P, C.POINTER(_P)]),
     "bsp_matrix_create_dev": (_I, [_P, _I, _I, _I, _I64, _P, _P, _P, C.POINTER(_P)]),
     "bsp_matrix_destroy": (_I, [_P]),

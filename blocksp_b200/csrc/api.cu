@@ -2,12 +2,91 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include "reduce.cuh"
 
 namespace bsp {
 
 static thread_local std::string g_last_error;
 void record_error(const std::string& msg) { g_last_error = msg; }
+
+// ---- device memory cache (see pool_alloc in internal.hpp) ----
+namespace {
+struct Pool {
+  std::mutex mu;
+  std::map<int, std::multimap<size_t, void*>> free_blocks;  // device -> (capacity, block)
+  std::map<int, size_t> cached;                             // device -> bytes held
+};
+// Never destroyed: buffers released during static destruction still find it.
+Pool& pool() {
+  static Pool* p = new Pool;
+  return *p;
+}
+void pool_trim_locked(Pool& P, int device) {
+  for (auto& kv : P.free_blocks) {
+    if (device >= 0 && kv.first != device) continue;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != kv.first) cudaSetDevice(kv.first);
+    for (auto& b : kv.second) cudaFree(b.second);
+    kv.second.clear();
+    P.cached[kv.first] = 0;
+    if (cur >= 0 && cur != kv.first) cudaSetDevice(cur);
+  }
+}
+}  // namespace
+
+cudaError_t pool_alloc(void** p, size_t bytes, size_t* cap, int* device) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  *device = dev;
+  Pool& P = pool();
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto& fl = P.free_blocks[dev];
+    auto it = fl.lower_bound(bytes);
+    // a cached block at most 1/8 (plus 1 MiB) larger than the request
+    if (it != fl.end() && it->first <= bytes + bytes / 8 + (size_t(1) << 20)) {
+      *p = it->second;
+      *cap = it->first;
+      P.cached[dev] -= it->first;
+      fl.erase(it);
+      return cudaSuccess;
+    }
+  }
+  e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(P.mu);
+      pool_trim_locked(P, dev);
+    }
+    e = cudaMalloc(p, bytes);
+  }
+  *cap = bytes;
+  return e;
+}
+
+void pool_free(void* p, size_t cap, int device) {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (device >= 0 && cur != device) cudaSetDevice(device);
+  // queued work may still use the block: wait as cudaFree does
+  const bool idle = cudaDeviceSynchronize() == cudaSuccess;
+  Pool& P = pool();
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    if (idle && P.cached[device] + cap <= kPoolMaxBytes) {
+      P.free_blocks[device].emplace(cap, p);
+      P.cached[device] += cap;
+      p = nullptr;
+    }
+  }
+  if (p) cudaFree(p);
+  if (cur >= 0 && device >= 0 && cur != device) cudaSetDevice(cur);
+}
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -57,26 +136,27 @@ static int validate_structure(int n_rows, int n_cols, int bs, int64_t nnzb, cons
     record_error("matrix: more than 2^31-1 blocks");
     return BSP_INVALID;
   }
-  std::vector<unsigned char> seen;
+  // One O(nnzb) pass: range checks, and duplicate columns within a row (not
+  // representable in the reference container: operator() finds the existing
+  // entry, containers.hpp:156-157) found with a per-column stamp of the last
+  // row that used it, so no row is copied or sorted.
+  std::vector<int> stamp(n_cols, -1);
   for (int i = 0; i < n_rows; ++i) {
     if (row_ptr[i + 1] < row_ptr[i]) {
       record_error("matrix: row_ptr not monotone");
       return BSP_INVALID;
     }
-    for (int t = row_ptr[i]; t < row_ptr[i + 1]; ++t)
-      if (col_idx[t] < 0 || col_idx[t] >= n_cols) {
+    for (int t = row_ptr[i]; t < row_ptr[i + 1]; ++t) {
+      const int c = col_idx[t];
+      if (c < 0 || c >= n_cols) {
         record_error("matrix: column index out of range in row " + std::to_string(i));
         return BSP_INVALID;
       }
-    // duplicate columns within a row are not representable in the reference
-    // container (operator() finds the existing entry, containers.hpp:156-157)
-    if (row_ptr[i + 1] - row_ptr[i] > 1) {
-      std::vector<int> c(col_idx + row_ptr[i], col_idx + row_ptr[i + 1]);
-      std::sort(c.begin(), c.end());
-      if (std::adjacent_find(c.begin(), c.end()) != c.end()) {
+      if (stamp[c] == i) {
         record_error("matrix: duplicate column in row " + std::to_string(i));
         return BSP_INVALID;
       }
+      stamp[c] = i;
     }
   }
   return BSP_OK;
@@ -152,6 +232,21 @@ int bsp_handle_create(int device, void* stream, bsp_handle_t* out) {
   BSP_CUDA_TRY(cudaMemset(h->ws.scalars.get(), 0, 256 * sizeof(double)));
   BSP_CUDA_TRY(cudaMemset(h->ws.status.get(), 0, sizeof(DevStatus)));
   *out = h.release();
+  return BSP_OK;
+}
+
+int bsp_release_cached_memory(int device) {
+  Pool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  pool_trim_locked(P, device);
+  return BSP_OK;
+}
+
+int bsp_cached_memory(int device, int64_t* bytes) {
+  if (!bytes) return BSP_INVALID;
+  Pool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  *bytes = (int64_t)P.cached[device];
   return BSP_OK;
 }
 

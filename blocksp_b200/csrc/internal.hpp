@@ -11,34 +11,55 @@
 
 namespace bsp {
 
-// Owning device buffer (cudaMallocAsync-free: plain cudaMalloc so that the
-// pointers stay valid across streams and graph captures).
+// Process-wide cache of device allocations, per device.  A freed block is
+// kept (after the device has finished all queued work, as cudaFree would
+// wait) and handed to a later allocation of nearly the same size, so building
+// matrices and preconditioners repeatedly does not pay cudaMalloc / cudaFree
+// for gigabytes each time.  At most kPoolMaxBytes are kept per device; an
+// allocation that fails frees the cache and retries; bsp_release_cached_memory
+// returns it to the driver.
+constexpr size_t kPoolMaxBytes = size_t(32) << 30;
+cudaError_t pool_alloc(void** p, size_t bytes, size_t* cap, int* device);
+void pool_free(void* p, size_t cap, int device);
+
+// Owning device buffer: plain device memory (no stream-ordered allocator), so
+// the pointers stay valid across streams and graph captures.  cap is the
+// size of the underlying block in bytes (at least n * sizeof(T)).
 template <typename T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t cap = 0;
+  int dev = -1;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), cap(o.cap), dev(o.dev) { o.p = nullptr; o.n = o.cap = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; cap = o.cap; dev = o.dev;
+      o.p = nullptr; o.n = o.cap = 0;
+    }
     return *this;
   }
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) pool_free(p, cap, dev);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   int alloc(size_t count) {
     release();
     if (count == 0) return BSP_OK;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    void* q = nullptr;
+    cudaError_t e = pool_alloc(&q, count * sizeof(T), &cap, &dev);
     if (e != cudaSuccess) {
       p = nullptr;
+      cap = 0;
       record_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
       return e == cudaErrorMemoryAllocation ? BSP_OUT_OF_MEMORY : BSP_CUDA_ERROR;
     }
+    p = static_cast<T*>(q);
     n = count;
     return BSP_OK;
   }
@@ -177,8 +198,10 @@ template <typename T> int take(bsp_matrix_s* A, DevBuf<T>& d, size_t count) {
   d.release();
   d.p = reinterpret_cast<T*>(A->bin[best].p);
   d.n = count;
+  d.cap = A->bin[best].cap;
+  d.dev = A->bin[best].dev;
   A->bin[best].p = nullptr;
-  A->bin[best].n = 0;
+  A->bin[best].n = A->bin[best].cap = 0;
   A->bin.erase(A->bin.begin() + best);
   return BSP_OK;
 }
@@ -188,8 +211,10 @@ template <typename T> void give(bsp_matrix_s* A, DevBuf<T>& d) {
   DevBuf<unsigned char> r;
   r.p = reinterpret_cast<unsigned char*>(d.p);
   r.n = d.n * sizeof(T);
+  r.cap = d.cap;
+  r.dev = d.dev;
   d.p = nullptr;
-  d.n = 0;
+  d.n = d.cap = 0;
   A->bin.push_back(std::move(r));
   if (A->bin.size() > kBinMax) A->bin.erase(A->bin.begin());
 }

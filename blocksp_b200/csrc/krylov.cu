@@ -1145,10 +1145,13 @@ int refine_solve(bool gmres, bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc
     n_hist += std::min(ii.n_hist, cap);
     n_restarts += ii.n_restarts;
     ++outer;
-    if (s != BSP_OK && s != BSP_MAXIT) {
-      status = s;
+    if (s != BSP_OK && s != BSP_MAXIT && s != BSP_BREAKDOWN) {
+      status = s;  // NaN or a device failure: the correction is not usable
       break;
     }
+    // x += d.  A Krylov breakdown still leaves the minimiser over the space
+    // built so far in d, so it is applied and the true residual recomputed;
+    // the solve then stops with BREAKDOWN unless that residual meets tol.
     bsp::count_launch(), k_add<<<g, 256, 0, h->stream>>>(len, d.get(), x);
     // r = b - A x in FP64; rel = ||r|| / ||b||
     BSP_TRY(bsmv_launch(A, 1, 0, BSP_F64, -1.0, x, 1.0, b, r.get(), h->stream));
@@ -1159,6 +1162,7 @@ int refine_solve(bool gmres, bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc
     rel = sqrt(rr) / bnorm;
     if (!std::isfinite(rel)) status = BSP_NAN;
     else if (rel <= o->tol) status = BSP_OK;
+    else if (s == BSP_BREAKDOWN) status = BSP_BREAKDOWN;
     else if (total_iters >= o->max_iters) break;
   }
   const double ms = tm.stop_ms();

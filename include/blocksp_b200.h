@@ -138,6 +138,15 @@ int bsp_handle_create(int device, void* stream, bsp_handle_t* out);
 int bsp_handle_destroy(bsp_handle_t h);
 int bsp_handle_sync(bsp_handle_t h);
 void* bsp_handle_stream(bsp_handle_t h);
+/* Device memory the library caches (no counterpart in the reference, which
+ * allocates on the host).  Buffers the library frees (matrices,
+ * preconditioners, handle scratch) are kept per device, up to 32 GiB, and
+ * reused by later allocations of nearly the same size, so repeated set-up
+ * avoids cudaMalloc / cudaFree.  Release returns the cache of `device` (-1:
+ * every device) to the driver; the allocator also does so by itself before
+ * it reports an allocation failure. */
+int bsp_release_cached_memory(int device);
+int bsp_cached_memory(int device, int64_t* bytes);
 /* Failure detection (no counterpart in the reference, which never waits on
  * another thread): every device-side wait of the sync-free sweeps and
  * factorisations polls at most `polls` times (default 2^22, with a nanosleep

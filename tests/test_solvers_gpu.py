@@ -200,3 +200,20 @@ def test_true_residual_refinement_pcg(handle, precision):
                             precision=precision)
     assert info["status"] == 0 and info["true_rel_res"] <= 1e-10
     assert O.true_rel_residual(Ao, s.b, x) <= 1.5e-10
+
+
+def test_refinement_applies_the_correction_after_a_breakdown(handle):
+    """An inner pGMRES that breaks down (here the Krylov space of M^-1 A b is
+    one-dimensional: A = 2I in 8x8 blocks, ILU0 exact) still holds the
+    minimiser; the FP64 refinement applies it, recomputes the true residual
+    and reports convergence instead of returning the previous iterate."""
+    import blocksp_b200 as bsp
+    from blocksp_b200 import _lib, systems
+    n, bs = 10, 8
+    s = systems.BSRSystem(n=n, bs=bs, row_ptr=np.arange(n + 1, dtype=np.int32), col_idx=np.arange(n, dtype=np.int32),
+                          vals=np.repeat(2.0 * np.eye(bs)[None], n, 0), b=np.random.default_rng(3).random(n * bs))
+    A = bsp.Matrix.from_system(s, handle)
+    x, info, _ = bsp.pGMRES(A, s.b, 1e-10, bsp.ILU0(A), 100, 30, 10, return_info=True,
+                           stop_rule=_lib.STOP_TRUE_RESIDUAL)
+    assert info["status"] == 0 and info["true_rel_res"] <= 1e-14
+    assert np.abs(x - s.b / 2).max() <= 1e-15
