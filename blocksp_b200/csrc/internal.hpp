@@ -78,6 +78,7 @@ struct Workspace {
 };
 
 struct StreamSym;
+struct FactorPlan;
 
 // Structure-only analysis behind a preconditioner (sorted factor pattern,
 // permutation, dependency levels, chain tasks).  It depends on the matrix
@@ -93,6 +94,8 @@ struct SymbolicCache {
   DevBuf<int64_t> d_perm, t_blk;
   // streamed layouts of the two sweeps (block sizes the streamed kernel takes)
   std::shared_ptr<StreamSym> ss_lo, ss_up;
+  // elimination plan of the row-resident factorisation kernel
+  std::shared_ptr<FactorPlan> plan;
 };
 
 // Non-owning view of a scratch buffer (handle scratch; see bsp_handle_s).

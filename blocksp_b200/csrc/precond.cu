@@ -643,6 +643,7 @@ struct FactorP {
 };
 
 constexpr int kFactorWarps = 4;
+constexpr size_t kFactorRowsSmem = 96 * 1024;  // staging of the row-resident kernel per CTA
 
 __global__ void __launch_bounds__(kFactorWarps * 32) k_factor(const FactorP p) {
   extern __shared__ double smem[];
@@ -710,6 +711,138 @@ __global__ void __launch_bounds__(kFactorWarps * 32) k_factor(const FactorP p) {
     __threadfence();
     __syncwarp();
     if (lane == 0 && p.flags) st_release(p.flags + k, p.epoch);
+    __syncwarp();
+  }
+}
+
+// Row-resident factorisation (ILU0 / IChol0, bs <= 16): one warp per block
+// row k, rows claimed in level order.  The row's blocks are copied to shared
+// memory before the warp waits for the rows it depends on, every dependency
+// block (inverse diagonals U_ii^-1 / L_ii^-1 and the update sources of the
+// elimination plan) is then fetched in one batch, and the whole elimination
+// runs in shared memory: per lower entry (increasing i) L_ki = A_ki U_ii^-1
+// (ILU0) or A_ki L_ii^-T (IChol0), then the planned updates of the later
+// blocks; finally the diagonal block is inverted (ILU0) or factored and its
+// triangular inverse formed (IChol0), and the row is written back.  The same
+// operations in the same order as k_factor (bit-identical factors); only the
+// memory traffic on the dependency path changes.
+__device__ inline void warp_gemm_sub_smem(double* T, const double* A, const double* B, int bs, bool trB) {
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < bs * bs; e += 32) {
+    const int r = e / bs, c = e % bs;
+    double acc = 0.0;
+    if (trB)
+      for (int t = 0; t < bs; ++t) acc = fma(A[r * bs + t], B[c * bs + t], acc);
+    else
+      for (int t = 0; t < bs; ++t) acc = fma(A[r * bs + t], B[t * bs + c], acc);
+    T[e] = T[e] - acc;
+  }
+  __syncwarp();
+}
+
+struct FactorRowsP {
+  int n, bs, mode;
+  const int* order;
+  const int* ptr;
+  const int* col;
+  const int* diag;
+  const int* pp;
+  const int2* pairs;
+  double* vals;
+  double* dinv;
+  int* flags;
+  int epoch;
+  unsigned* ticket;
+  DevStatus* st;
+  unsigned spin_limit;
+  int nbmax, depmax;  // row blocks and dependency blocks staged per warp
+};
+
+__global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
+  extern __shared__ double fr_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bs = p.bs, b2 = bs * bs;
+  double* rowb = fr_smem + (size_t)warp * (p.nbmax + p.depmax + 3) * b2;
+  double* dep = rowb + (size_t)p.nbmax * b2;
+  double* Lb = dep + (size_t)p.depmax * b2;
+  double* aug = Lb + b2;
+  const bool chol = p.mode == FACT_ICHOL0;
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = (int)atomicAdd(p.ticket, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= p.n) break;
+    const int k = __ldg(p.order + t);
+    const int beg = __ldg(p.ptr + k), dg = __ldg(p.diag + k), end = __ldg(p.ptr + k + 1);
+    // the row's own blocks, in flight while the warp waits for its dependencies
+    for (int x = lane; x < (end - beg) * b2; x += 32)
+      cp_async_small<8>(rowb + x, p.vals + (int64_t)beg * b2 + x);
+    cp_async_commit();
+    for (int e = beg; e < dg; ++e) wait_flag(p.flags + __ldg(p.col + e), p.epoch, p.st, k, p.spin_limit);
+    int e = beg;
+    while (e < dg) {
+      // a batch of consecutive lower entries whose dependency blocks fit
+      int used = 0, eb = e;
+      while (eb < dg) {
+        int need = 1;
+        for (int q = __ldg(p.pp + eb); q < __ldg(p.pp + eb + 1); ++q) need += __ldg(&p.pairs[q].y) >= 0;
+        if (eb > e && used + need > p.depmax) break;
+        used += need;
+        ++eb;
+      }
+      int slot = 0;
+      for (int x = e; x < eb; ++x) {
+        const double* src = p.dinv + (int64_t)__ldg(p.col + x) * b2;
+        for (int y = lane; y < b2; y += 32) cp_async_small<8>(dep + (size_t)slot * b2 + y, src + y);
+        ++slot;
+        for (int q = __ldg(p.pp + x); q < __ldg(p.pp + x + 1); ++q) {
+          const int s = __ldg(&p.pairs[q].y);
+          if (s < 0) continue;
+          for (int y = lane; y < b2; y += 32) cp_async_small<8>(dep + (size_t)slot * b2 + y, p.vals + (int64_t)s * b2 + y);
+          ++slot;
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncwarp();
+      slot = 0;
+      for (int x = e; x < eb; ++x) {
+        double* Ak = rowb + (size_t)(x - beg) * b2;
+        // ILU0: L_ki = A_ki U_ii^{-1};  IChol0: L_ki = A_ki L_ii^{-T}
+        warp_gemm(Lb, Ak, dep + (size_t)slot * b2, bs, chol);
+        ++slot;
+        for (int y = lane; y < b2; y += 32) Ak[y] = Lb[y];
+        __syncwarp();
+        for (int q = __ldg(p.pp + x); q < __ldg(p.pp + x + 1); ++q) {
+          const int2 pr = p.pairs[q];
+          const double* S;
+          if (pr.y >= 0) {
+            S = dep + (size_t)slot * b2;
+            ++slot;
+          } else {
+            S = rowb + (size_t)(-1 - pr.y - beg) * b2;
+          }
+          warp_gemm_sub_smem(rowb + (size_t)(pr.x - beg) * b2, Lb, S, bs, chol);
+        }
+      }
+      e = eb;
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+    double* Dk = rowb + (size_t)(dg - beg) * b2;
+    if (chol) {
+      const bool ok = warp_cholesky(Dk, bs);
+      if (!ok && lane == 0) set_status(p.st, BSP_NOT_SPD, k);
+      warp_lower_inverse(Lb, Dk, bs);
+    } else {
+      const bool ok = warp_inverse(Lb, Dk, aug, bs);  // aug: bs x 2bs scratch
+      if (!ok && lane == 0) set_status(p.st, BSP_ZERO_PIVOT, k);
+    }
+    for (int x = lane; x < (end - beg) * b2; x += 32) p.vals[(int64_t)beg * b2 + x] = rowb[x];
+    for (int y = lane; y < b2; y += 32) p.dinv[(int64_t)k * b2 + y] = Lb[y];
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(p.flags + k, p.epoch);
     __syncwarp();
   }
 }
@@ -857,6 +990,7 @@ static int sym_transfer(bsp_precond_s* pc, SymbolicCache& C, bool save) {
   if (save) {
     C.ss_lo = pc->ss_lo;
     C.ss_up = pc->ss_up;
+    C.plan = pc->plan;
     C.h_perm = pc->h_perm;
     C.f_nnzb = pc->f_nnzb;
     C.n_lev_lo = pc->n_lev_lo;
@@ -867,6 +1001,7 @@ static int sym_transfer(bsp_precond_s* pc, SymbolicCache& C, bool save) {
   } else {
     pc->ss_lo = C.ss_lo;
     pc->ss_up = C.ss_up;
+    pc->plan = C.plan;
     pc->h_perm = C.h_perm;
     pc->f_nnzb = C.f_nnzb;
     pc->n_lev_lo = C.n_lev_lo;
@@ -933,11 +1068,43 @@ static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* 
   fp.ticket = pc->ticket.get();
   fp.st = h->ws.status.get();
   fp.spin_limit = h->spin_limit;
-  const size_t smem = (size_t)kFactorWarps * 5 * pc->bs * pc->bs * sizeof(double);
-  BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BSP_CUDA_TRY(cudaMemsetAsync(pc->ticket.get(), 0, sizeof(unsigned), h->stream));
-  const int grid = persistent_grid(h, k_factor, kFactorWarps * 32, smem);
-  bsp::count_launch(), k_factor<<<grid, kFactorWarps * 32, smem, h->stream>>>(fp);
+  // the row-resident kernel when the plan exists and a row fits its staging
+  const FactorPlan* plan = pc->plan.get();
+  const size_t b2 = (size_t)pc->bs * pc->bs;
+  const int depmax = plan ? std::max(plan->max_deps, 4) : 0;
+  const size_t per_warp = plan ? (size_t)(plan->max_row + depmax + 3) * b2 * sizeof(double) : 0;
+  if (mode != FACT_DIAG && plan && pc->bs <= 16 && per_warp <= kFactorRowsSmem && ptr == pc->f_ptr.get()) {
+    FactorRowsP rp;
+    rp.n = n;
+    rp.bs = pc->bs;
+    rp.mode = mode;
+    rp.order = order;
+    rp.ptr = ptr;
+    rp.col = col;
+    rp.diag = diag;
+    rp.pp = plan->pp.get();
+    rp.pairs = plan->pairs.get();
+    rp.vals = vals;
+    rp.dinv = fp.dinv;
+    rp.flags = fp.flags;
+    rp.epoch = fp.epoch;
+    rp.ticket = fp.ticket;
+    rp.st = fp.st;
+    rp.spin_limit = fp.spin_limit;
+    rp.nbmax = plan->max_row;
+    rp.depmax = depmax;
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(8, kFactorRowsSmem / per_warp));
+    const size_t smem = per_warp * warps;
+    BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = persistent_grid(h, k_factor_rows, warps * 32, smem);
+    bsp::count_launch(), k_factor_rows<<<grid, warps * 32, smem, h->stream>>>(rp);
+  } else {
+    const size_t smem = (size_t)kFactorWarps * 5 * pc->bs * pc->bs * sizeof(double);
+    BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = persistent_grid(h, k_factor, kFactorWarps * 32, smem);
+    bsp::count_launch(), k_factor<<<grid, kFactorWarps * 32, smem, h->stream>>>(fp);
+  }
   BSP_CUDA_TRY(cudaPeekAtLastError());
   DevStatus st;
   BSP_TRY(read_status(h, &st));
@@ -1005,6 +1172,63 @@ static int launch_sweep(bsp_handle_s* h, int bs, SweepP<VT, AT> p, unsigned* tic
 }
 
 // ---------------------------------------------------------------- build
+// Elimination plan (FactorPlan) of the row-sorted factor structure.
+static int build_factor_plan(bsp_precond_s* pc, int n, const std::vector<int>& ptr, const std::vector<int>& col,
+                             const std::vector<int>& diag, bool lower_only) {
+  auto plan = std::make_shared<FactorPlan>();
+  const int64_t nf = (int64_t)col.size();
+  std::vector<int> pp(nf + 1, 0);
+  std::vector<int2> pairs;
+  pairs.reserve(nf);
+  // position of column c in the sorted range [a, b) of the factor structure
+  auto find = [&](int a, int b, int c) -> int {
+    const auto it = std::lower_bound(col.begin() + a, col.begin() + b, c);
+    return (it != col.begin() + b && *it == c) ? (int)(it - col.begin()) : -1;
+  };
+  int max_row = 0, max_deps = 0;
+  for (int k = 0; k < n; ++k) {
+    max_row = std::max(max_row, ptr[k + 1] - ptr[k]);
+    for (int e = ptr[k]; e < ptr[k + 1]; ++e) {
+      int deps = 1;
+      if (e < diag[k]) {
+        const int i = col[e];
+        if (!lower_only) {
+          // A_kj -= L_ki U_ij for every later j of row k present in U's row i
+          for (int e2 = e + 1; e2 < ptr[k + 1]; ++e2) {
+            const int pos = find(diag[i] + 1, ptr[i + 1], col[e2]);
+            if (pos >= 0) {
+              pairs.push_back(make_int2(e2, pos));
+              ++deps;
+            }
+          }
+        } else {
+          // A_kj -= L_ki L_ji^T for i < j <= k with (j, i) in the pattern
+          for (int e2 = e + 1; e2 <= diag[k]; ++e2) {
+            const int j = col[e2];
+            if (j == k) {
+              pairs.push_back(make_int2(e2, -1 - e));
+            } else {
+              const int pos = find(ptr[j], diag[j], i);
+              if (pos >= 0) {
+                pairs.push_back(make_int2(e2, pos));
+                ++deps;
+              }
+            }
+          }
+        }
+        max_deps = std::max(max_deps, deps);
+      }
+      pp[e + 1] = (int)pairs.size();
+    }
+  }
+  plan->max_row = max_row;
+  plan->max_deps = max_deps;
+  BSP_TRY(upload(plan->pp, pp));
+  BSP_TRY(upload(plan->pairs, pairs));
+  pc->plan = plan;
+  return BSP_OK;
+}
+
 static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
   const bsp_matrix_s* A = pc->A;
   const int n = A->n_rows;
@@ -1113,7 +1337,7 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
     BSP_TRY(upload(pc->t_row, trow));
     BSP_TRY(upload(pc->t_blk, tblk));
   }
-  return BSP_OK;
+  return build_factor_plan(pc, n, ptr, col, diag, lower_only);
 }
 
 // Factor storage for ILU0 / IChol0: the symbolic part from the matrix's cache

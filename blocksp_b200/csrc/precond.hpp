@@ -4,6 +4,22 @@
 #include "internal.hpp"
 #include "sweep_stream.hpp"
 
+namespace bsp {
+// Elimination plan of a block ILU0 / IChol0 factorisation (pattern only).
+// For every strictly-lower factor entry e (block (k, i)), the updates it makes
+// to later blocks of its own row k, in the reference's order:
+// pairs[pp[e] .. pp[e+1]) = {target factor entry, source}, where source >= 0
+// is a factor entry of another row (U_ij for ILU0: A_kj -= L_ki U_ij; L_ji
+// for IChol0: A_kj -= L_ki L_ji^T) and source < 0 names the entry -1 - source
+// of row k itself (IChol0's diagonal update A_kk -= L_ki L_ki^T).
+struct FactorPlan {
+  DevBuf<int> pp;        // f_nnzb + 1
+  DevBuf<int2> pairs;
+  int max_row = 0;       // blocks of the longest factor row
+  int max_deps = 0;      // largest per-entry dependency count (inverse diagonal + sources)
+};
+}  // namespace bsp
+
 struct bsp_precond_s {
   bsp_handle_t h = nullptr;
   int device = 0;
@@ -55,6 +71,8 @@ struct bsp_precond_s {
   // after every change of the factors
   std::shared_ptr<bsp::StreamSym> ss_lo, ss_up;
   bsp::StreamVals sv_lo[3], sv_up[3];
+  // elimination plan of the factorisation (shared with the matrix's cache)
+  std::shared_ptr<bsp::FactorPlan> plan;
 };
 
 namespace bsp {
