@@ -663,6 +663,46 @@ def run_learned(args):
     print(json.dumps(line), flush=True)
 
 
+def run_apply(args):
+    """The ILU0 application alone (forward + backward streamed sweeps) on the
+    64^3 8x8 system, `steps` times after `warmup`: the kernel the solve's
+    roofline is quoted on, in a short program that profilers can capture."""
+    import torch
+    import blocksp_b200 as bsp
+    from blocksp_b200 import systems
+    stream = torch.cuda.Stream()
+    h = bsp.Handle(0, stream=stream.cuda_stream)
+    s = systems.config1(seed=1, side=args.side)
+    A = bsp.Matrix.from_system(s, h)
+    pc = bsp.ILU0(A)
+    b = torch.tensor(s.b, device="cuda")
+    z = torch.empty_like(b)
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 1)):
+            z.copy_(b)
+            pc(z)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(args.steps):
+            z.copy_(b)
+            e0.record(stream)
+            pc(z)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    peak, kind = read_peaks()
+    nbytes = ilu_apply_bytes(s.n, s.bs, s.nnzb)
+    t = statistics.mean(ms)
+    print(json.dumps({"metric": "ILU0 application (two streamed sweeps) GB/s", "value": nbytes / (t * 1e-3) / 1e9,
+                      "unit": "GB/s", "ms_per_apply": t, "steps": args.steps, "warmup": args.warmup,
+                      "algorithmic_bytes": nbytes, "peak": peak, "peak_source": kind,
+                      "levels": [pc.info()["levels_lower"], pc.info()["levels_upper"]]}), flush=True)
+    pc.close()
+    A.close()
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -676,9 +716,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="plain_f64,mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch", "mixed", "learned"],
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch", "mixed", "learned", "apply"],
                     help="cfg1: the headline line; batch: 256-system batched pCG; mixed: cfg2 precision "
-                         "variants; learned: cfg4 ablation")
+                         "variants; learned: cfg4 ablation; apply: the ILU0 application alone (profiling)")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--learned-side", type=int, default=96)
     ap.add_argument("--learned-seeds", type=int, default=2)
@@ -690,7 +730,7 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": f"the {args.workload} leg reports its CPU "
                               "reference inside its own line"}))
             return
-        {"batch": run_batch, "mixed": run_mixed, "learned": run_learned}[args.workload](args)
+        {"batch": run_batch, "mixed": run_mixed, "learned": run_learned, "apply": run_apply}[args.workload](args)
         return
     world, rank, local = dist_setup(args.dist_backend)
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "

@@ -88,6 +88,70 @@ void pool_free(void* p, size_t cap, int device) {
   if (cur >= 0 && device >= 0 && cur != device) cudaSetDevice(cur);
 }
 
+// ---- pattern registry (see SymbolicSet in internal.hpp) ----
+namespace {
+struct PatternEntry {
+  int device = 0, n_rows = 0, n_cols = 0, bs = 0;
+  int64_t nnzb = 0;
+  uint64_t hash = 0;
+  std::vector<int> row_ptr, col_idx;
+  std::shared_ptr<SymbolicSet> set;
+};
+constexpr size_t kPatternsKept = 4;
+std::mutex g_pat_mu;
+std::vector<PatternEntry>* g_patterns = new std::vector<PatternEntry>;  // most recent last; never destroyed
+
+uint64_t pattern_hash(int n_rows, int64_t nnzb, const int* rp, const int* ci) {
+  uint64_t h = 0x9E3779B97F4A7C15ull ^ ((uint64_t)n_rows << 32) ^ (uint64_t)nnzb;
+  auto mix = [&h](uint32_t v) {
+    h ^= v;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+  };
+  for (int i = 0; i <= n_rows; ++i) mix((uint32_t)rp[i]);
+  for (int64_t t = 0; t < nnzb; ++t) mix((uint32_t)ci[t]);
+  return h;
+}
+}  // namespace
+
+std::shared_ptr<SymbolicSet> symbolic_for_pattern(int device, int n_rows, int n_cols, int bs, int64_t nnzb,
+                                                  const int* row_ptr, const int* col_idx) {
+  const uint64_t h = pattern_hash(n_rows, nnzb, row_ptr, col_idx);
+  std::lock_guard<std::mutex> lk(g_pat_mu);
+  auto& P = *g_patterns;
+  for (size_t k = 0; k < P.size(); ++k) {
+    PatternEntry& e = P[k];
+    if (e.device == device && e.n_rows == n_rows && e.n_cols == n_cols && e.bs == bs && e.nnzb == nnzb &&
+        e.hash == h && std::equal(row_ptr, row_ptr + n_rows + 1, e.row_ptr.begin()) &&
+        std::equal(col_idx, col_idx + nnzb, e.col_idx.begin())) {
+      PatternEntry hit = std::move(e);
+      P.erase(P.begin() + k);
+      std::shared_ptr<SymbolicSet> set = hit.set;
+      P.push_back(std::move(hit));
+      return set;
+    }
+  }
+  PatternEntry e;
+  e.device = device;
+  e.n_rows = n_rows;
+  e.n_cols = n_cols;
+  e.bs = bs;
+  e.nnzb = nnzb;
+  e.hash = h;
+  e.row_ptr.assign(row_ptr, row_ptr + n_rows + 1);
+  e.col_idx.assign(col_idx, col_idx + nnzb);
+  e.set = std::make_shared<SymbolicSet>();
+  std::shared_ptr<SymbolicSet> set = e.set;
+  P.push_back(std::move(e));
+  if (P.size() > kPatternsKept) P.erase(P.begin());
+  return set;
+}
+
+void symbolic_registry_clear() {
+  std::lock_guard<std::mutex> lk(g_pat_mu);
+  g_patterns->clear();
+}
+
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void count_launch_add(int64_t n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
@@ -236,6 +300,7 @@ int bsp_handle_create(int device, void* stream, bsp_handle_t* out) {
 }
 
 int bsp_release_cached_memory(int device) {
+  symbolic_registry_clear();  // its analyses hold device buffers too
   Pool& P = pool();
   std::lock_guard<std::mutex> lk(P.mu);
   pool_trim_locked(P, device);
@@ -290,6 +355,7 @@ static int matrix_create_common(bsp_handle_t h, int n_rows, int n_cols, int bs, 
   A->nnzb = nnzb;
   A->h_row_ptr.assign(row_ptr, row_ptr + n_rows + 1);
   A->h_col_idx.assign(col_idx, col_idx + nnzb);
+  A->sym = symbolic_for_pattern(h->device, n_rows, n_cols, bs, nnzb, row_ptr, col_idx);
   BSP_TRY(A->row_ptr.alloc(n_rows + 1));
   BSP_TRY(A->col_idx.alloc(nnzb > 0 ? nnzb : 1));
   BSP_TRY(A->vals.alloc(nnzb > 0 ? (size_t)nnzb * bs * bs : 1));

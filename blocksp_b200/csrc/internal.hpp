@@ -98,6 +98,17 @@ struct SymbolicCache {
   std::shared_ptr<FactorPlan> plan;
 };
 
+// The analyses of one sparsity pattern.  Matrices created with the same
+// pattern on the same device share one set (a process-wide registry keeps the
+// sets of the last few patterns), so a new matrix with a known pattern —
+// a new time step, a Newton update — skips the host analysis.
+struct SymbolicSet {
+  SymbolicCache ilu, ichol, sor;
+};
+std::shared_ptr<SymbolicSet> symbolic_for_pattern(int device, int n_rows, int n_cols, int bs, int64_t nnzb,
+                                                  const int* row_ptr, const int* col_idx);
+void symbolic_registry_clear();
+
 // Non-owning view of a scratch buffer (handle scratch; see bsp_handle_s).
 template <typename T> struct Span {
   T* p = nullptr;
@@ -179,8 +190,9 @@ struct bsp_matrix_s {
   bsp::DevBuf<int> tr_ptr, tr_row;
   bsp::DevBuf<int64_t> tr_blk;
   bool has_transpose = false;
-  // symbolic analyses for ILU0 (full pattern), IChol0 (lower pattern), SOR/Diag
-  bsp::SymbolicCache sym_ilu, sym_ichol, sym_sor;
+  // symbolic analyses for ILU0 (full pattern), IChol0 (lower pattern), SOR/Diag,
+  // shared with every matrix of the same pattern on this device
+  std::shared_ptr<bsp::SymbolicSet> sym;
   // device memory of destroyed preconditioners of this matrix, handed to the
   // next one built on it (factor copies, inverted diagonals, scratch)
   std::vector<bsp::DevBuf<unsigned char>> bin;

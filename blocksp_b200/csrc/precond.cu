@@ -1343,7 +1343,7 @@ static int analyse_factor_structure(bsp_precond_s* pc, bool lower_only) {
 // Factor storage for ILU0 / IChol0: the symbolic part from the matrix's cache
 // (computed on first use), then A's values gathered into it on the device.
 static int build_factor_structure(bsp_precond_s* pc, bool lower_only) {
-  SymbolicCache& C = lower_only ? pc->A->sym_ichol : pc->A->sym_ilu;
+  SymbolicCache& C = lower_only ? pc->A->sym->ichol : pc->A->sym->ilu;
   if (C.valid) {
     BSP_TRY(sym_transfer(pc, C, false));
   } else {
@@ -1394,7 +1394,7 @@ static int analyse_diag_structure(bsp_precond_s* pc) {
 }
 
 static int build_diag_inverse(bsp_precond_s* pc) {
-  SymbolicCache& C = pc->A->sym_sor;
+  SymbolicCache& C = pc->A->sym->sor;
   const bool sor = pc->kind == BSP_PC_SOR_LU || pc->kind == BSP_PC_SOR_CHOL;
   if (C.valid && (!sor || C.n_task_lo > 0)) {
     BSP_TRY(sym_transfer(pc, C, false));
@@ -1612,7 +1612,10 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
     case BSP_PC_ILU0:
     case BSP_PC_LEARNED_LU: {
       if constexpr (std::is_same<AT, double>::value) {
-        if (pc->ss_lo && pc->ss_up) return apply_streamed<VT>(pc, r, z, sa);
+        // the streamed sweeps read vectors in 16-byte pieces
+        if (pc->ss_lo && pc->ss_up && reinterpret_cast<uintptr_t>(z) % 16 == 0 &&
+            reinterpret_cast<uintptr_t>(r) % 16 == 0)
+          return apply_streamed<VT>(pc, r, z, sa);
       }
       p.ptr = pc->f_ptr.get();
       p.idx = pc->f_col.get();
@@ -1639,7 +1642,10 @@ static int apply_typed(bsp_precond_s* pc, const AT* r, AT* z, const VT* fvals, c
     case BSP_PC_ICHOL0:
     case BSP_PC_LEARNED_LLT: {
       if constexpr (std::is_same<AT, double>::value) {
-        if (pc->ss_lo && pc->ss_up) return apply_streamed<VT>(pc, r, z, sa);
+        // the streamed sweeps read vectors in 16-byte pieces
+        if (pc->ss_lo && pc->ss_up && reinterpret_cast<uintptr_t>(z) % 16 == 0 &&
+            reinterpret_cast<uintptr_t>(r) % 16 == 0)
+          return apply_streamed<VT>(pc, r, z, sa);
       }
       p.ptr = pc->f_ptr.get();
       p.idx = pc->f_col.get();

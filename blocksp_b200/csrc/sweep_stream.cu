@@ -15,12 +15,17 @@
 //     published by its values, so a consumer polls the words it needs
 //     (bounded spin) until they differ from the sentinel;
 //   * a row of another chain of the same CTA is read from that warp's output
-//     rows in shared memory once its published row count says it is there;
+//     rows in shared memory, which are published the same way (sentinel
+//     until written), so neither side needs a memory fence;
 //   * the chain's previous row is passed on in registers;
 //   * every block of the row, its D block and its right-hand side are staged
 //     DEPTH rows ahead into a per-warp shared-memory ring by per-lane cp.async
 //     copies of the contiguous stream (each lane copies exactly the chunks it
-//     reads later, so it only waits for its own copies).
+//     reads later, so it only waits for its own copies); the values of the
+//     row's external dependencies are copied into the ring at the same time,
+//     so a dependency published by then costs no round trip when the row
+//     starts (a copy that still holds the sentinel is polled in global
+//     memory).
 // Lane map: a block of BS x BS values of type VT is 32*P chunks of V values;
 // lane l holds chunk q*32 + l (block row q*RPP + l/CPR, columns c0..c0+V-1,
 // c0 = (l % CPR)*V), so a row's dot products end in a CPR-lane reduction.
@@ -110,13 +115,13 @@ template <int BS, typename VT, bool HAS_D, int W, int DEPTH> struct SSCfg {
   using M = SMap<BS, VT>;
   static constexpr int OFF_D = kStreamEmax * M::BB;
   static constexpr int OFF_R = OFF_D + (HAS_D ? M::BB : 0);
-  static constexpr int SB = OFF_R + 32 * M::P * 8;  // + one rhs value per lane and pass
+  static constexpr int OFF_X = OFF_R + BS * 8;               // + the row's right-hand side
+  static constexpr int SB = OFF_X + kStreamEmax * BS * 8;    // + the staged rows' external x values
   static constexpr size_t RING = (size_t)W * DEPTH * SB;
   static constexpr size_t BUF = (size_t)W * kStreamCmax * BS * 8;   // output rows of each chain
   static constexpr size_t REC = (size_t)W * kStreamCmax * 16;       // row records of each chain
   static constexpr size_t EOF_ = (size_t)W * kStreamCmax * 4;       // entry offsets of each row
-  static constexpr size_t SCR = (size_t)W * BS * 8;                 // per-warp D-product scratch
-  static constexpr size_t kSmem = RING + BUF + REC + EOF_ + SCR;
+  static constexpr size_t kSmem = RING + BUF + REC + EOF_;
 };
 
 __device__ __forceinline__ bool failed(const DevStatus* st) {
@@ -130,7 +135,6 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
   constexpr int V = M::V, P = M::P, CPR = M::CPR, RPP = M::RPP, BB = M::BB, CB = M::CB;
   extern __shared__ __align__(128) unsigned char ss_smem[];
   __shared__ int s_task;
-  __shared__ volatile int s_done[W];
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int c0 = (l % CPR) * V;
   unsigned char* ring = ss_smem + (size_t)w * DEPTH * C::SB;
@@ -138,14 +142,16 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
   double* buf = buf_all + (size_t)w * kStreamCmax * BS;
   int4* rw = reinterpret_cast<int4*>(ss_smem + C::RING + C::BUF) + w * kStreamCmax;
   int* eo = reinterpret_cast<int*>(ss_smem + C::RING + C::BUF + C::REC) + w * kStreamCmax;
-  double* scr = reinterpret_cast<double*>(ss_smem + C::RING + C::BUF + C::REC + C::EOF_) + w * BS;
   const unsigned limit = p.spin_limit;
   DevStatus* const st = p.st;
   double* const xg = p.x;
 
   while (true) {
     if (threadIdx.x == 0) s_task = (int)atomicAdd(p.ticket, 1u);
-    if (l == 0) s_done[w] = 0;
+    // the chain's output rows in shared memory are published by their values,
+    // like the global vector: the sentinel until the row is written
+    for (int x = l; x < kStreamCmax * BS; x += 32)
+      reinterpret_cast<unsigned long long*>(buf)[x] = kSentinel64;
     __syncthreads();
     const int t = s_task;
     if (t >= p.n_super) break;
@@ -191,9 +197,14 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
             for (int q = 0; q < P; ++q) cp_async_n<CB>(dst + C::OFF_D + (q * 32 + l) * CB, ds + (q * 32 + l) * CB);
           }
           const int r = row0 + s * p.dir;
+          if (l < BS / 2) cp_async16(dst + C::OFF_R + l * 16, p.rhs + (int64_t)r * BS + 2 * l);
+          // the external rows' values as they are now: published ones are
+          // final, the others still hold the sentinel and are polled later
+          const int code[kStreamEmax] = {rr.x, rr.y, rr.z};
 #pragma unroll
-          for (int q = 0; q < P; ++q)
-            cp_async_small<8>(dst + C::OFF_R + (q * 32 + l) * 8, p.rhs + (int64_t)r * BS + q * RPP + l / CPR);
+          for (int u = 0; u < kStreamEmax; ++u)
+            if (u < ne && code[u] >= 0 && l < BS / 2)
+              cp_async16(dst + C::OFF_X + u * BS * 8 + l * 16, xg + (int64_t)code[u] * BS + 2 * l);
         }
         cp_async_commit();
       };
@@ -203,6 +214,20 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
       double prev[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) prev[v] = 0.0;
+      // the next row's external values, loaded one row ahead: a dependency
+      // published after the ring copy was made but before this load is
+      // still found without a round trip on the row's path
+      double nx[kStreamEmax][V];
+      auto load_next = [&](int s2) {
+        if (s2 < len) {
+          const int4 r2 = rw[s2];
+          const int c2[kStreamEmax] = {r2.x, r2.y, r2.z};
+#pragma unroll
+          for (int u = 0; u < kStreamEmax; ++u)
+            if (u < r2.w && c2[u] >= 0) ld_vec_cg<V>(xg + (int64_t)c2[u] * BS + c0, nx[u]);
+        }
+      };
+      load_next(0);
       auto poll = [&](int j, double (&xv)[V], int who) {
         bool pend = false;
 #pragma unroll
@@ -222,21 +247,32 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
           for (int v = 0; v < V; ++v) pend |= is_sentinel(xv[v]);
         }
       };
+      // a row of another chain of this CTA: its words in that warp's output
+      // rows, read until they are no longer the sentinel (no fence needed)
       auto local = [&](int slot, double (&xv)[V], int who) {
         const int ww = slot / kStreamCmax, ss = slot - ww * kStreamCmax;
+        const volatile double* src = buf_all + ((size_t)ww * kStreamCmax + ss) * BS + c0;
+        bool pend = false;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          xv[v] = src[v];
+          pend |= is_sentinel(xv[v]);
+        }
         unsigned spins = 0;
-        while (s_done[ww] <= ss) {
+        while (pend) {
           if (++spins > limit) {
             set_status(st, BSP_TIMEOUT, who);
             break;
           }
           if ((spins & 255u) == 0u && failed(st)) break;
           if (spins >= kSpinFree) __nanosleep(32);
-        }
-        __threadfence_block();
-        const double* src = buf_all + ((size_t)ww * kStreamCmax + ss) * BS + c0;
+          pend = false;
 #pragma unroll
-        for (int v = 0; v < V; ++v) xv[v] = src[v];
+          for (int v = 0; v < V; ++v) {
+            xv[v] = src[v];
+            pend |= is_sentinel(xv[v]);
+          }
+        }
       };
       auto fma_chunks = [&](const unsigned char* blk, const double (&xv)[V], double (&acc)[P]) {
 #pragma unroll
@@ -253,16 +289,31 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
         const int4 rr = rw[s];
         const int ne = rr.w;
         cp_async_wait<DEPTH - 1>();
+        __syncwarp();  // the prefetched x values were copied by lanes 0..BS/2-1
         const unsigned char* sl = ring + (s % DEPTH) * C::SB;
         double acc[P];
 #pragma unroll
         for (int q = 0; q < P; ++q) acc[q] = 0.0;
         const int code[kStreamEmax] = {rr.x, rr.y, rr.z};
         double xv[kStreamEmax][V];
-        // every external load first, so their round trips overlap
+        // external rows: the values copied with the row's blocks, else the
+        // ones loaded a row ahead; only a row published after both is polled
 #pragma unroll
         for (int u = 0; u < kStreamEmax; ++u)
-          if (u < ne && code[u] >= 0) ld_vec_cg<V>(xg + (int64_t)code[u] * BS + c0, xv[u]);
+          if (u < ne && code[u] >= 0) {
+            const double* px = reinterpret_cast<const double*>(sl + C::OFF_X + u * BS * 8) + c0;
+            bool ring_ok = true;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              xv[u][v] = px[v];
+              ring_ok &= !is_sentinel(xv[u][v]);
+            }
+            if (!ring_ok) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) xv[u][v] = nx[u][v];
+            }
+          }
+        load_next(s + 1);
 #pragma unroll
         for (int u = 0; u < kStreamEmax; ++u) {
           if (u < ne) {
@@ -292,52 +343,38 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
           }
           fma_chunks(reinterpret_cast<const unsigned char*>(p.vals) + (int64_t)e * BB, xe, acc);
         }
-        // s = rhs_r - sum over the CPR lanes of each block row
-        double sv[P];
+        // x_r = rhs_r - sum (no D), or D_r rhs_r - sum with the blocks
+        // premultiplied by D_r; the CPR lanes of each block row then reduce
         const double* rh = reinterpret_cast<const double*>(sl + C::OFF_R);
-#pragma unroll
-        for (int q = 0; q < P; ++q) sv[q] = rh[q * 32 + l] - row_reduce<CPR>(acc[q], 0xffffffffu);
         double xr[P];
         if constexpr (HAS_D) {
-          // x_r = D_r s: every lane needs s at its columns c0..c0+V-1
-          if (l % CPR == 0) {
-#pragma unroll
-            for (int q = 0; q < P; ++q) scr[q * RPP + l / CPR] = sv[q];
-          }
-          __syncwarp();
-          double sc[V];
-#pragma unroll
-          for (int v = 0; v < V; ++v) sc[v] = scr[c0 + v];
 #pragma unroll
           for (int q = 0; q < P; ++q) {
             double a[V];
             ChunkOps<VT, V>::get(sl + C::OFF_D + (q * 32 + l) * CB, a);
             double o = 0.0;
 #pragma unroll
-            for (int v = 0; v < V; ++v) o = fma(a[v], sc[v], o);
-            xr[q] = row_reduce<CPR>(o, 0xffffffffu);
+            for (int v = 0; v < V; ++v) o = fma(a[v], rh[c0 + v], o);
+            xr[q] = row_reduce<CPR>(o - acc[q], 0xffffffffu);
           }
         } else {
 #pragma unroll
-          for (int q = 0; q < P; ++q) xr[q] = sv[q];
+          for (int q = 0; q < P; ++q) xr[q] = rh[q * RPP + l / CPR] - row_reduce<CPR>(acc[q], 0xffffffffu);
         }
-        // publish row r: global (other CTAs poll its values), shared (this CTA)
+        // publish row r by its values: shared memory first (this CTA's next
+        // chains poll it there), then global memory (other CTAs poll it)
         double* bro = buf + s * BS;
         if (l % CPR == 0) {
 #pragma unroll
-          for (int q = 0; q < P; ++q) {
-            const int rowc = q * RPP + l / CPR;
-            xg[(int64_t)r * BS + rowc] = xr[q];
-            bro[rowc] = xr[q];
-          }
+          for (int q = 0; q < P; ++q) bro[q * RPP + l / CPR] = xr[q];
         }
         __syncwarp();
+        if (l % CPR == 0) {
+#pragma unroll
+          for (int q = 0; q < P; ++q) xg[(int64_t)r * BS + q * RPP + l / CPR] = xr[q];
+        }
 #pragma unroll
         for (int v = 0; v < V; ++v) prev[v] = bro[c0 + v];
-        if (l == 0) {
-          __threadfence_block();
-          s_done[w] = s + 1;
-        }
         issue(s + DEPTH);
       }
       cp_async_wait<0>();
@@ -358,6 +395,30 @@ __global__ void k_stream_gather(int64_t nblk, int bs, const IT* __restrict__ idx
     const int k = (int)(t - e * b2);
     const int a = k / bs, c = k - a * bs;
     const double v = src[(int64_t)idx[e] * b2 + (trans ? c * bs + a : k)];
+    if constexpr (std::is_same<VT, double>::value) dst[t] = v;
+    else if constexpr (std::is_same<VT, float>::value) dst[t] = (float)v;
+    else dst[t] = __float2bfloat16_rn((float)v);
+  }
+}
+
+// dst[e] (VT) = D_r B_e in FP64, r the row of entry e: D = dinv[r] (transposed
+// when trans_d), B_e = src[idx[e]] (transposed when trans).
+template <typename VT>
+__global__ void k_stream_gather_premul(int64_t nblk, int bs, const int64_t* __restrict__ idx,
+                                       const int* __restrict__ ent_q, const int* __restrict__ q_row,
+                                       const double* __restrict__ src, const double* __restrict__ dinv, int trans,
+                                       int trans_d, VT* __restrict__ dst) {
+  const int b2 = bs * bs;
+  const int64_t total = nblk * b2;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / b2;
+    const int k = (int)(t - e * b2);
+    const int a = k / bs, c = k - a * bs;
+    const double* D = dinv + (int64_t)q_row[ent_q[e]] * b2;
+    const double* B = src + (int64_t)idx[e] * b2;
+    double v = 0.0;
+    for (int m = 0; m < bs; ++m)
+      v = fma(trans_d ? D[m * bs + a] : D[a * bs + m], trans ? B[c * bs + m] : B[m * bs + c], v);
     if constexpr (std::is_same<VT, double>::value) dst[t] = v;
     else if constexpr (std::is_same<VT, float>::value) dst[t] = (float)v;
     else dst[t] = __float2bfloat16_rn((float)v);
@@ -429,11 +490,12 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return lvl[a] < lvl[b]; });
   // stream layout in ticket order
-  std::vector<int> super_beg(nsup + 1, 0), codes, q_row(n);
+  std::vector<int> super_beg(nsup + 1, 0), codes, q_row(n), ent_q;
   std::vector<int4> chains, rec(n);
   std::vector<int64_t> src;
   codes.reserve(E.col.size());
   src.reserve(E.col.size());
+  ent_q.reserve(E.col.size());
   chains.reserve(nc);
   int q = 0;
   std::vector<std::pair<int, int64_t>> ext, loc;
@@ -465,6 +527,7 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
         for (auto& e : loc) { codes.push_back(e.first); src.push_back(e.second); }
         if (has_in) { codes.push_back(-1); src.push_back(inchain.second); }
         const int ne = (int)codes.size() - e_first;
+        ent_q.insert(ent_q.end(), ne, q);
         int cc[3] = {0, 0, 0};
         for (int u = 0; u < std::min(ne, 3); ++u) cc[u] = codes[e_first + u];
         rec[q] = make_int4(cc[0], cc[1], cc[2], ne);
@@ -485,6 +548,7 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
   BSP_TRY(upload_vec(S.codes, codes));
   BSP_TRY(upload_vec(S.src_blk, src));
   BSP_TRY(upload_vec(S.q_row, q_row));
+  BSP_TRY(upload_vec(S.ent_q, ent_q));
   return BSP_OK;
 }
 
@@ -503,9 +567,15 @@ static int gather_typed(bsp_handle_s* h, const StreamSym& S, int bs, const doubl
   const int64_t b2 = (int64_t)bs * bs;
   const size_t vb = (size_t)std::max<int64_t>(S.n_ent, 1) * b2 * sizeof(VT);
   if (out.vals.n < vb) BSP_TRY(out.vals.alloc(vb));
-  if (S.n_ent > 0)
-    bsp::count_launch(), k_stream_gather<VT, int64_t><<<grid_for(h, S.n_ent * b2, 256), 256, 0, h->stream>>>(
-        S.n_ent, bs, S.src_blk.get(), fvals, S.trans_blocks ? 1 : 0, reinterpret_cast<VT*>(out.vals.get()));
+  if (S.n_ent > 0) {
+    if (S.has_d)
+      bsp::count_launch(), k_stream_gather_premul<VT><<<grid_for(h, S.n_ent * b2, 256), 256, 0, h->stream>>>(
+          S.n_ent, bs, S.src_blk.get(), S.ent_q.get(), S.q_row.get(), fvals, dinv, S.trans_blocks ? 1 : 0,
+          S.trans_d ? 1 : 0, reinterpret_cast<VT*>(out.vals.get()));
+    else
+      bsp::count_launch(), k_stream_gather<VT, int64_t><<<grid_for(h, S.n_ent * b2, 256), 256, 0, h->stream>>>(
+          S.n_ent, bs, S.src_blk.get(), fvals, S.trans_blocks ? 1 : 0, reinterpret_cast<VT*>(out.vals.get()));
+  }
   if (S.has_d) {
     const size_t db = (size_t)std::max(S.n, 1) * b2 * sizeof(VT);
     if (out.dvals.n < db) BSP_TRY(out.dvals.alloc(db));

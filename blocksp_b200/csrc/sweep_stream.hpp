@@ -17,7 +17,11 @@
 //     chain's previous row (registers), <= -2 a row of another chain of the
 //     same CTA (shared memory);
 //   * the blocks (transposed where the sweep reads B^T) and the D blocks are
-//     stored contiguously in that order, in the precision of the solve.
+//     stored contiguously in that order, in the precision of the solve; in a
+//     sweep with D blocks every block is stored premultiplied by its row's D,
+//     x_r = D_r rhs_r - sum_e (D_r B_e) x_{j_e}, so D_r rhs_r is formed before
+//     the row's dependencies arrive and D leaves the dependency path (the same
+//     operator; the rounding of the two products differs).
 // What a row computes is unchanged; only when it runs and where its inputs
 // come from differ from the reference's loop.
 #pragma once
@@ -42,6 +46,7 @@ struct StreamSym {
   DevBuf<int> codes;       // per entry (rows with more than kStreamEmax entries)
   DevBuf<int64_t> src_blk; // per entry: block index in the factor's value array
   DevBuf<int> q_row;       // per stream row: its block row (D gather)
+  DevBuf<int> ent_q;       // per entry: its stream row (D-premultiplied gather)
 };
 
 // The entries of a sweep in CSR form: row i reads rows col[t] through the

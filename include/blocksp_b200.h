@@ -144,7 +144,11 @@ void* bsp_handle_stream(bsp_handle_t h);
  * reused by later allocations of nearly the same size, so repeated set-up
  * avoids cudaMalloc / cudaFree.  Release returns the cache of `device` (-1:
  * every device) to the driver; the allocator also does so by itself before
- * it reports an allocation failure. */
+ * it reports an allocation failure.  The symbolic analyses of the last four
+ * sparsity patterns (level schedules, sweep layouts, elimination plans) are
+ * kept the same way: a matrix created with a pattern seen before — a new time
+ * step, a Newton update — reuses them instead of analysing it again; release
+ * drops them as well. */
 int bsp_release_cached_memory(int device);
 int bsp_cached_memory(int device, int64_t* bytes);
 /* Failure detection (no counterpart in the reference, which never waits on
