@@ -8,7 +8,8 @@
 // reference's row update.
 //
 // Execution (one persistent launch per sweep):
-//   * a CTA claims a super-task (W consecutive chains) with an atomic ticket,
+//   * a CTA claims a super-task (W chains: a tile of consecutive chains by
+//     chains one plane apart, or W consecutive chains) with an atomic ticket,
 //     in dependency-level order; warp w runs chain w row by row;
 //   * a row of another super-task is read from global memory: the output
 //     vector is pre-filled with a signalling-NaN sentinel and a row is
@@ -31,6 +32,7 @@
 // c0 = (l % CPR)*V), so a row's dot products end in a CPR-lane reduction.
 // Accumulation is FP64 for every storage type (vectors are FP64).
 #include <algorithm>
+#include <map>
 #include <numeric>
 #include "sentinel.cuh"
 #include "stage.cuh"
@@ -430,7 +432,7 @@ int grid_for(const bsp_handle_s* h, int64_t n, int threads);
 // ------------------------------------------------------------------ host: build
 bool stream_supported(int bs) { return bs == 8 || bs == 16; }
 
-int stream_warps(int bs) { return bs >= 16 ? 4 : 8; }
+int stream_warps(int bs) { return bs >= 16 ? 4 : 16; }
 
 template <typename T> static int upload_vec(DevBuf<T>& d, const std::vector<T>& v) {
   BSP_TRY(d.alloc(v.empty() ? 1 : v.size()));
@@ -438,15 +440,11 @@ template <typename T> static int upload_vec(DevBuf<T>& d, const std::vector<T>& 
   return BSP_OK;
 }
 
-int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool trans_blocks, bool has_d,
-                 bool trans_d, StreamSym& S) {
+int stream_plan(int n, bool ascending, int warps, const SweepEntries& E, StreamPlan& S) {
   const int dir = ascending ? 1 : -1;
   S.n = n;
   S.W = warps;
   S.dir = dir;
-  S.trans_blocks = trans_blocks;
-  S.has_d = has_d;
-  S.trans_d = trans_d;
   // chains in sweep order: row r continues the chain of r - dir when it
   // depends on that row and the chain is shorter than kStreamCmax
   std::vector<int> chain_of(n), pos(n), first, clen;
@@ -468,23 +466,85 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
     }
   }
   const int nc = (int)first.size();
-  const int nsup = (nc + warps - 1) / warps;  // W consecutive chains per super-task
-  // super-task levels (creation order is a topological order)
-  std::vector<int> lvl(nsup, 0);
-  int maxl = 0;
-  for (int sp = 0; sp < nsup; ++sp) {
-    int L = 0;
-    for (int c = sp * warps; c < std::min(nc, (sp + 1) * warps); ++c)
-      for (int k = 0; k < clen[c]; ++k) {
-        const int r = first[c] + k * dir;
-        for (int t = E.ptr[r]; t < E.ptr[r + 1]; ++t) {
-          const int so = chain_of[E.col[t]] / warps;
-          if (so != sp) L = std::max(L, lvl[so] + 1);
-        }
-      }
-    lvl[sp] = L;
-    maxl = std::max(maxl, L);
+  // chain dependencies (distinct predecessor chains) and their strides
+  std::vector<std::vector<int>> cdeps(nc);
+  std::map<int, int> stride_count;
+  for (int c = 0; c < nc; ++c) {
+    auto& dc = cdeps[c];
+    for (int k = 0; k < clen[c]; ++k) {
+      const int r = first[c] + k * dir;
+      for (int t = E.ptr[r]; t < E.ptr[r + 1]; ++t)
+        if (chain_of[E.col[t]] != c) dc.push_back(chain_of[E.col[t]]);
+    }
+    std::sort(dc.begin(), dc.end());
+    dc.erase(std::unique(dc.begin(), dc.end()), dc.end());
+    for (int cj : dc)
+      if (c - cj >= 2) stride_count[c - cj]++;
   }
+  // super-tasks: tiles of wy consecutive chains by wz chains strided by d
+  // (the chain's neighbour in the next plane of a grid), so that both
+  // directions across the chains stay inside the CTA; warps in tile order
+  std::vector<int> sup_of(nc), warp_of(nc), lvl;
+  std::vector<std::vector<int>> members, succ;
+  int nsup = 0;
+  auto tile = [&](int d, int wy, int wz) {
+    const int cols = (d + wy - 1) / wy;
+    std::map<int64_t, int> ids;
+    std::vector<int> key_warp(nc);
+    for (int c = 0; c < nc; ++c) {
+      const int a = c / (wz * d), rem = c % (wz * d), zi = rem / d, o = rem % d;
+      const int64_t key = (int64_t)a * cols + o / wy;
+      auto it = ids.find(key);
+      if (it == ids.end()) it = ids.emplace(key, (int)ids.size()).first;
+      sup_of[c] = it->second;
+      key_warp[c] = zi * wy + o % wy;
+    }
+    nsup = (int)ids.size();
+    members.assign(nsup, {});
+    for (int c = 0; c < nc; ++c) members[sup_of[c]].push_back(c);
+    for (auto& m : members) {
+      std::sort(m.begin(), m.end(), [&](int x, int y) { return key_warp[x] < key_warp[y]; });
+      for (int i = 0; i < (int)m.size(); ++i) warp_of[m[i]] = i;
+    }
+    // super-task graph and its longest-path levels (Kahn); false on a cycle
+    succ.assign(nsup, {});
+    std::vector<int> indeg(nsup, 0), queue;
+    for (int c = 0; c < nc; ++c)
+      for (int cj : cdeps[c])
+        if (sup_of[cj] != sup_of[c]) succ[sup_of[cj]].push_back(sup_of[c]);
+    for (auto& v : succ) {
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      for (int b : v) indeg[b]++;
+    }
+    lvl.assign(nsup, 0);
+    for (int a = 0; a < nsup; ++a)
+      if (!indeg[a]) queue.push_back(a);
+    for (size_t h = 0; h < queue.size(); ++h)
+      for (int b : succ[queue[h]]) {
+        lvl[b] = std::max(lvl[b], lvl[queue[h]] + 1);
+        if (--indeg[b] == 0) queue.push_back(b);
+      }
+    return (int)queue.size() == nsup;
+  };
+  int dom = 0, dom_n = 0;
+  for (auto& kv : stride_count)
+    if (kv.second > dom_n) {
+      dom = kv.first;
+      dom_n = kv.second;
+    }
+  int wz = 1;
+  while (wz * wz * 4 <= warps) wz *= 2;  // 16 -> 4 x 4, 8 -> 4 x 2, 4 -> 2 x 2
+  const int wy = warps / wz;
+  S.stride = 0;
+  if (warps > 1 && wz > 1 && dom >= wy && dom_n * 2 >= nc && tile(dom, wy, wz)) {
+    S.stride = dom;
+  } else if (!tile(std::max(nc, 1), warps, 1)) {  // W consecutive chains
+    record_error("streamed sweep: dependency graph is not triangular");
+    return BSP_INVALID;
+  }
+  int maxl = 0;
+  for (int v : lvl) maxl = std::max(maxl, v);
   S.n_levels = maxl + 1;
   std::vector<int> order(nsup);
   std::iota(order.begin(), order.end(), 0);
@@ -503,7 +563,7 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
   for (int t = 0; t < nsup; ++t) {
     const int sp = order[t];
     super_beg[t] = (int)chains.size();
-    for (int c = sp * warps; c < std::min(nc, (sp + 1) * warps); ++c) {
+    for (int c : members[sp]) {
       chains.push_back(make_int4(first[c], clen[c], q, (int)codes.size()));
       for (int k = 0; k < clen[c]; ++k, ++q) {
         const int r = first[c] + k * dir;
@@ -516,8 +576,8 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
           if (cj == c && pos[j] == k - 1) {
             has_in = true;
             inchain = {-1, E.blk[tt]};
-          } else if (cj / warps == sp) {
-            loc.emplace_back(-2 - ((cj - sp * warps) * kStreamCmax + pos[j]), E.blk[tt]);
+          } else if (sup_of[cj] == sp) {
+            loc.emplace_back(-2 - (warp_of[cj] * kStreamCmax + pos[j]), E.blk[tt]);
           } else {
             ext.emplace_back(j, E.blk[tt]);
           }
@@ -541,14 +601,38 @@ int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool t
   }
   S.n_super = nsup;
   S.n_chains = nc;
-  S.n_ent = (int64_t)codes.size();
-  BSP_TRY(upload_vec(S.super_beg, super_beg));
-  BSP_TRY(upload_vec(S.chains, chains));
-  BSP_TRY(upload_vec(S.rec, rec));
-  BSP_TRY(upload_vec(S.codes, codes));
-  BSP_TRY(upload_vec(S.src_blk, src));
-  BSP_TRY(upload_vec(S.q_row, q_row));
-  BSP_TRY(upload_vec(S.ent_q, ent_q));
+  S.super_beg = std::move(super_beg);
+  S.chains = std::move(chains);
+  S.rec = std::move(rec);
+  S.codes = std::move(codes);
+  S.src_blk = std::move(src);
+  S.q_row = std::move(q_row);
+  S.ent_q = std::move(ent_q);
+  return BSP_OK;
+}
+
+int stream_build(int n, bool ascending, int warps, const SweepEntries& E, bool trans_blocks, bool has_d,
+                 bool trans_d, StreamSym& S) {
+  StreamPlan P;
+  BSP_TRY(stream_plan(n, ascending, warps, E, P));
+  S.n = P.n;
+  S.n_super = P.n_super;
+  S.n_chains = P.n_chains;
+  S.W = P.W;
+  S.dir = P.dir;
+  S.n_levels = P.n_levels;
+  S.stride = P.stride;
+  S.n_ent = (int64_t)P.codes.size();
+  S.trans_blocks = trans_blocks;
+  S.has_d = has_d;
+  S.trans_d = trans_d;
+  BSP_TRY(upload_vec(S.super_beg, P.super_beg));
+  BSP_TRY(upload_vec(S.chains, P.chains));
+  BSP_TRY(upload_vec(S.rec, P.rec));
+  BSP_TRY(upload_vec(S.codes, P.codes));
+  BSP_TRY(upload_vec(S.src_blk, P.src_blk));
+  BSP_TRY(upload_vec(S.q_row, P.q_row));
+  BSP_TRY(upload_vec(S.ent_q, P.ent_q));
   return BSP_OK;
 }
 
@@ -616,7 +700,7 @@ static int launch_ss(bsp_handle_s* h, const SSP<VT>& p) {
 // Warps per CTA and ring depth of a configuration: the deepest ring (at most
 // 4 rows) that keeps two CTAs on an SM, else the deepest for one CTA.
 template <int BS, typename VT, bool HAS_D> struct SSPick {
-  static constexpr int W = BS >= 16 ? 4 : 8;  // the layout's grouping depends on BS only
+  static constexpr int W = BS >= 16 ? 4 : 16;  // the layout's grouping depends on BS only
   static constexpr size_t sm(int d) {
     return d == 4 ? SSCfg<BS, VT, HAS_D, W, 4>::kSmem : d == 3 ? SSCfg<BS, VT, HAS_D, W, 3>::kSmem
                                                                  : SSCfg<BS, VT, HAS_D, W, 2>::kSmem;

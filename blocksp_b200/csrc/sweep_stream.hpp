@@ -9,7 +9,11 @@
 // block the sweep reads out once, in the order the device consumes it:
 //   * rows are grouped into chains (runs of consecutive rows, each depending
 //     on the one before; at most kStreamCmax rows), chains into super-tasks of
-//     W consecutive chains (one CTA, one warp per chain);
+//     W chains (one CTA, one warp per chain).  When one chain stride d links
+//     at least half of the chains (the neighbouring plane of a grid), a
+//     super-task is a tile of wy consecutive chains by wz chains d apart, so
+//     both directions across the chains are handed over inside the CTA;
+//     otherwise it is W consecutive chains;
 //   * super-tasks are sorted by dependency level (the ticket order);
 //   * per row the entries are ordered external rows first, rows of the same
 //     super-task next, the chain's previous row last, and each entry carries a
@@ -37,10 +41,10 @@ constexpr int kStreamCmax = 64;  // rows per chain (longer runs are split)
 // Symbolic part of one streamed sweep (depends on the matrix pattern only).
 struct StreamSym {
   int n = 0, n_super = 0, n_chains = 0, W = 0, dir = 1;
-  int n_levels = 0;
+  int n_levels = 0, stride = 0;  // super-task levels; chain stride of the tiles (0: consecutive)
   int64_t n_ent = 0;
   bool trans_blocks = false, has_d = false, trans_d = false;
-  DevBuf<int> super_beg;   // n_super + 1: chains of each super-task (ticket order)
+  DevBuf<int> super_beg;   // n_super + 1: chains of each super-task (ticket order, warp order)
   DevBuf<int4> chains;     // {row0, len, q0 (first stream row), e0 (first entry)}
   DevBuf<int4> rec;        // per stream row: {code0, code1, code2, n_entries}
   DevBuf<int> codes;       // per entry (rows with more than kStreamEmax entries)
@@ -55,6 +59,15 @@ struct SweepEntries {
   std::vector<int> ptr, col;
   std::vector<int64_t> blk;
 };
+
+// The layout of a sweep on the host (the arrays StreamSym holds on the device).
+struct StreamPlan {
+  int n = 0, n_super = 0, n_chains = 0, W = 0, dir = 1, n_levels = 0, stride = 0;
+  std::vector<int> super_beg, codes, q_row, ent_q;
+  std::vector<int4> chains, rec;
+  std::vector<int64_t> src_blk;
+};
+int stream_plan(int n, bool ascending, int warps, const SweepEntries& ent, StreamPlan& P);
 
 // Builds the streamed layout of a sweep over n rows; ascending: forward
 // sweep (dependencies j < i), else backward (j > i).
