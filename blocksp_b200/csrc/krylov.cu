@@ -332,6 +332,20 @@ __device__ __forceinline__ void mgs_barrier(const MgsP& p, unsigned gen) {
   __syncthreads();
 }
 
+// Asks L2 to fetch n doubles at src (a hint: nothing is written; a range
+// that is not 16-byte aligned is skipped).  Called by warp 0 of the CTA:
+// lane k issues the k-th 16 KB piece.
+__device__ __forceinline__ void prefetch_l2(const double* src, int64_t n) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  if (n <= 0 || (a & 15u)) return;
+  const int64_t bytes = (n * 8) & ~int64_t(15);
+  constexpr int64_t kPiece = 16384;
+  for (int64_t o = (int64_t)(threadIdx.x & 31) * kPiece; o < bytes; o += 32 * kPiece) {
+    const unsigned sz = (unsigned)(bytes - o < kPiece ? bytes - o : kPiece);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a + o), "r"(sz) : "memory");
+  }
+}
+
 // Sum of the gridDim.x partials of one pass, in index order (same in every CTA).
 __device__ __forceinline__ double grid_total(const double* part, double* red) {
   if (threadIdx.x < 32) {
@@ -380,6 +394,8 @@ __global__ void __launch_bounds__(kMgsThreads, 1) k_mgs(const MgsP p) {
     }
     a = cta_sum_1024(a, red);
     if (t == 0) p.partials[(size_t)i * gridDim.x + blockIdx.x] = a;
+    // the next basis vector's slice streams into L2 while the grid meets
+    if (t < 32 && i < p.j) prefetch_l2(p.Q[i + 1] + beg, nloc);
     mgs_barrier(p, ++gen);
     h = grid_total(p.partials + (size_t)i * gridDim.x, red);
     if (blockIdx.x == 0 && t == 0) p.H[(size_t)i * p.ldh + p.j] = h;

@@ -258,6 +258,7 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
     model = LearnedModel(h, 8, _lib.BSP_F32, params=init_params(8, seed), form=form)
     t0 = time.time()
     history = []
+    prev, reverts, lr0 = None, 0, lr
     for ep in range(epochs):
         for si, s in enumerate(train_seeds):
             sysm = training_system(dims, s, form)
@@ -266,7 +267,23 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
             Q = training_probes(A, ilu, torch.tensor(sysm.b, device="cuda"), n_probes - n_smooth, n_smooth,
                                 smooth_steps, int(s))
             for _ in range(steps_per_system):
-                loss = model.loss_grad(A, ilu, Q)
+                # a step whose factors break down (zero pivot, not SPD, NaN)
+                # is undone and the learning rate halved
+                try:
+                    loss = model.loss_grad(A, ilu, Q)
+                    ok = np.isfinite(loss)
+                except _lib.BspError as e:
+                    if e.status not in (1, 2, 5):
+                        raise
+                    ok = False
+                if not ok:
+                    if prev is None:
+                        raise RuntimeError("the initial factors break down")
+                    model.set_params(prev)
+                    lr *= 0.5
+                    reverts += 1
+                    continue
+                prev = flatten(model.params(), 8)
                 model.adam_step(lr)
                 history.append(loss)
             ilu.close()
@@ -291,7 +308,8 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
     model.meta = {"bs": 8, "hidden": HIDDEN, "layers": LAYERS, "dims": list(dims), "form": form,
                   "baseline": base.__name__, "beats_baseline": beats,
                   "train_seeds": [int(s) for s in train_seeds], "val_seeds": [int(s) for s in val_seeds],
-                  "steps_per_system": steps_per_system, "epochs": epochs, "n_probes": n_probes, "lr": lr,
+                  "steps_per_system": steps_per_system, "epochs": epochs, "n_probes": n_probes, "lr": lr0,
+                  "lr_final": lr, "reverted_steps": reverts,
                   "n_smooth": n_smooth, "smooth_steps": smooth_steps,
                   "loss_first": history[0] if history else None, "loss_last": history[-1] if history else None,
                   "loss_history": history[:: max(1, len(history) // 200)], "validation": val,

@@ -9,9 +9,9 @@ full-size systems (tests/golden/make_golden.py, ``CONFIG_CASES``):
 * 3D 48^3, 7-point, 16x16 blocks, skew 0.3 (110,592 block rows),
   ILU0_pGMRES(A, 1e-10, 5000, 30, 10).
 
-At these sizes the sweep scheduler runs its full-size shape (190 dependency
-levels and 4,096 chains per sweep at 64^3), which the small fixtures do not
-reach.  Criteria as in tests/parity.py: iteration counts +-1 (+-2 with
+At these sizes the sweep scheduler runs its full-size shape (4,096 chains in
+256 super-tasks of 4 x 4 chains and 31 super-task levels per sweep at 64^3),
+which the small fixtures do not reach.  Criteria as in tests/parity.py: iteration counts +-1 (+-2 with
 deflated restart); pGMRES normalised residual history within 1e-10 absolute
 at every step; pCG history within 1e-10 plus 10x the oracle's own rounding
 envelope (stored in the fixture); solutions within 1e-8 relative (the whole x
