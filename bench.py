@@ -42,7 +42,7 @@ GOLDEN = ROOT / "tests" / "golden"
 # ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one ILU0
 # application at 64^3 with 8x8 FP64 blocks (its two streamed sweeps), from the
 # committed capture summarised in profiles/sweep_stream_ilu0_64cube_bs8.md
-ILU_APPLY_TRAFFIC_64 = None
+ILU_APPLY_TRAFFIC_64 = 1_013_952_512  # 439.6 MB forward + 574.3 MB backward
 
 
 def reference_golden(side: int) -> dict | None:
@@ -184,6 +184,26 @@ def ilu_apply_bytes(n: int, bs: int, nnzb: int, val_bytes: int = 8) -> int:
 
 # --------------------------------------------------------------------- GPU arm
 
+def north_star(results: dict) -> dict | None:
+    """The target comparison: the learned (with its ILU0 fallback) mixed-precision
+    solver against plain FP64 ILU0-pGMRES on the same system, wall time to the
+    FP64 true residual."""
+    from blocksp_b200 import learned
+    if "plain_f64" not in results or "learned_mixed_f32" not in results:
+        return None
+    gate = None
+    if learned.WEIGHTS.exists():
+        gate = bool(json.loads(str(np.load(learned.WEIGHTS)["meta"])).get("beats_ilu0", False))
+    plain, lm = results["plain_f64"]["total_s"], results["learned_mixed_f32"]["total_s"]
+    return {"plain_f64_s": plain, "learned_mixed_f32_s": lm, "speedup": plain / lm,
+            "learned_gate_open": gate, "preconditioner_used": results["learned_mixed_f32"].get("preconditioner")}
+
+
+def pc_name(pc) -> str:
+    from blocksp_b200 import _lib
+    return {_lib.PC_ILU0: "ILU0", _lib.PC_LEARNED_LU: "learned LU"}.get(pc.kind, str(pc.kind))
+
+
 def run_gpu(args, world, rank, local):
     import torch
     import blocksp_b200 as bsp
@@ -205,10 +225,19 @@ def run_gpu(args, world, rank, local):
         e.record(stream)
         return e
 
-    # ---- one solve: ILU0 set-up + refined pGMRES-DR to the true residual ----
-    def solve_once(precision):
+    # the learned preconditioner with its ILU0 fallback (the committed model's
+    # own validation decides which one runs)
+    from blocksp_b200 import learned
+    model = learned.LearnedModel.load(handle=h) if learned.WEIGHTS.exists() else None
+    makers = {"plain_f64": (lambda: bsp.ILU0(A), _lib.PREC_F64),
+              "mixed_f32": (lambda: bsp.ILU0(A), _lib.PREC_F32),
+              "learned_mixed_f32": (lambda: learned.LearnedLU(A, model), _lib.PREC_F32)}
+
+    # ---- one solve: preconditioner set-up + refined pGMRES-DR to the true residual ----
+    def solve_once(name):
+        make_pc, precision = makers[name]
         e0 = ev()
-        pc = bsp.ILU0(A)
+        pc = make_pc()
         e1 = ev()
         x, info, hist = bsp.pGMRES(A, b, TOL, pc, 5000, 30, 10, return_info=True,
                                    stop_rule=_lib.STOP_TRUE_RESIDUAL, precision=precision,
@@ -217,7 +246,7 @@ def run_gpu(args, world, rank, local):
         e2.synchronize()
         pc.close()
         return {"setup_s": e0.elapsed_time(e1) / 1e3, "solve_s": e1.elapsed_time(e2) / 1e3,
-                "total_s": e0.elapsed_time(e2) / 1e3, "iters": info["iters"],
+                "total_s": e0.elapsed_time(e2) / 1e3, "iters": info["iters"], "preconditioner": pc_name(pc),
                 "refinements": info["n_outer"], "restarts": info["n_restarts"],
                 "true_rel_res": info["true_rel_res"], "status": info["status"]}
 
@@ -226,18 +255,17 @@ def run_gpu(args, world, rank, local):
     pc = bsp.ILU0(A)
     _, pinfo, phist = bsp.pGMRES(A, b, TOL, pc, 5000, 30, 10, return_info=True)
     pc.close()
-    variants = {k: v for k, v in {"plain_f64": _lib.PREC_F64, "mixed_f32": _lib.PREC_F32}.items()
-                if k in args.variants.split(",")}
+    variants = {k: makers[k][1] for k in args.variants.split(",") if k in makers}
     results = {}
     launches = 0
     with ClockSampler(local) as clk:
-        for name, prec in variants.items():
+        for name in variants:
             for _ in range(max(args.warmup, 3)):
-                solve_once(prec)
+                solve_once(name)
             torch.cuda.synchronize()
             barrier(world)
             l0 = lib.bsp_launch_count()
-            steps = [solve_once(prec) for _ in range(args.steps)]
+            steps = [solve_once(name) for _ in range(args.steps)]
             launches += lib.bsp_launch_count() - l0
             tot = max_over_ranks(statistics.mean(s["total_s"] for s in steps), world)
             results[name] = {**steps[-1], "total_s": tot,
@@ -274,6 +302,8 @@ def run_gpu(args, world, rank, local):
     best = min(results, key=lambda k: results[k]["total_s"])
     xh = np.zeros_like(sysm.b)
     if args.no_e2e:
+        if model is not None:
+            model.close()
         A.close()
         h.close()
         return {"n": n, "bs": bs, "nnzb": nnzb, "results": results, "best": best, "e2e_s": float("nan"),
@@ -292,7 +322,7 @@ def run_gpu(args, world, rank, local):
         t = [time.perf_counter()]
         A2 = bsp.Matrix(rp_h, ci_h, va_h, bs, handle=h)
         t.append(time.perf_counter())
-        pc2 = bsp.ILU0(A2)
+        pc2 = learned.LearnedLU(A2, model) if best == "learned_mixed_f32" else bsp.ILU0(A2)
         t.append(time.perf_counter())
         out = bsp.pGMRES(A2, b_h, TOL, pc2, 5000, 30, 10, stop_rule=_lib.STOP_TRUE_RESIDUAL,
                          precision=variants[best])
@@ -313,6 +343,8 @@ def run_gpu(args, world, rank, local):
         xh = e2e_call()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
     e2e_parts = {k: v / e2e_steps for k, v in parts.items()}
+    if model is not None:
+        model.close()
     A.close()
     h.close()
     return {
@@ -714,7 +746,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=150.0,
                     help="reference arm: seconds of full CPU solves to run (at least one)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variants", default="plain_f64,mixed_f32")
+    ap.add_argument("--variants", default="plain_f64,mixed_f32,learned_mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch", "mixed", "learned", "apply"],
                     help="cfg1: the headline line; batch: 256-system batched pCG; mixed: cfg2 precision "
@@ -799,6 +831,7 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": f"synthetic (seeded {args.side}^3 7-point block stencil)",
         "config": {**config, "best_variant": r["best"]},
         "variants": r["results"],
+        "north_star": north_star(r["results"]),
         "parity_vs_reference": parity,
         "bsmv": {"kernel": "k_bsmv<8,double,double,1>", "ms": r["bsmv_ms"], "gbs": bsmv_gbs,
                  "frac_of_peak": bsmv_gbs / r["peak"], "algorithmic_bytes": bsmv_bytes(n, bs, nnzb)},
