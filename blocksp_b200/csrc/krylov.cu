@@ -21,6 +21,7 @@
 #include <type_traits>
 #include <vector>
 #include "reduce.cuh"
+#include "stage.cuh"
 #include "sentinel.cuh"
 #include "small_dense.h"
 
@@ -382,15 +383,27 @@ __global__ void __launch_bounds__(kMgsThreads, 1) k_mgs(const MgsP p) {
   for (int i = 0; i <= p.j; ++i) {
     const double* qb = p.Q[i] + beg;
     double a = 0.0;
+    // the axpy with the previous basis vector (its slice in shared memory),
+    // then this vector's slice replaces it: one batch of copies in flight at
+    // once (each thread copies and reads only its own entries)
+    if (i > 0) {
+#pragma unroll
+      for (int k = 0; k < NPT; ++k) {
+        const int o = t + k * kMgsThreads;
+        if (o < nloc) v[k] = fma(-h, qs[o], v[k]);
+      }
+    }
 #pragma unroll
     for (int k = 0; k < NPT; ++k) {
       const int o = t + k * kMgsThreads;
-      if (o < nloc) {
-        if (i > 0) v[k] = fma(-h, qs[o], v[k]);
-        const double q = __ldcs(qb + o);
-        qs[o] = q;
-        a = fma(q, v[k], a);
-      }
+      if (o < nloc) cp_async_small<8>(qs + o, qb + o);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int o = t + k * kMgsThreads;
+      if (o < nloc) a = fma(qs[o], v[k], a);
     }
     a = cta_sum_1024(a, red);
     if (t == 0) p.partials[(size_t)i * gridDim.x + blockIdx.x] = a;
