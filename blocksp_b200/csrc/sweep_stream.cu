@@ -293,6 +293,31 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
         cp_async_wait<DEPTH - 1>();
         __syncwarp();  // the prefetched x values were copied by lanes 0..BS/2-1
         const unsigned char* sl = ring + (s % DEPTH) * C::SB;
+        // the row's staged blocks and its D rhs part do not depend on the
+        // sweep: read from shared memory before any dependency is awaited,
+        // so the waits and these reads overlap
+        double blk[kStreamEmax][P][V];
+#pragma unroll
+        for (int u = 0; u < kStreamEmax; ++u)
+          if (u < ne) {
+#pragma unroll
+            for (int q = 0; q < P; ++q) ChunkOps<VT, V>::get(sl + u * BB + (q * 32 + l) * CB, blk[u][q]);
+          }
+        const double* rh = reinterpret_cast<const double*>(sl + C::OFF_R);
+        double base[P];  // D_r rhs_r partial of this lane (with D), or rhs_r
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          if constexpr (HAS_D) {
+            double a[V];
+            ChunkOps<VT, V>::get(sl + C::OFF_D + (q * 32 + l) * CB, a);
+            double o = 0.0;
+#pragma unroll
+            for (int v = 0; v < V; ++v) o = fma(a[v], rh[c0 + v], o);
+            base[q] = o;
+          } else {
+            base[q] = rh[q * RPP + l / CPR];
+          }
+        }
         double acc[P];
 #pragma unroll
         for (int q = 0; q < P; ++q) acc[q] = 0.0;
@@ -326,7 +351,10 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
             } else {
               local(-code[u] - 2, xv[u], r);
             }
-            fma_chunks(sl + u * BB, xv[u], acc);
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+#pragma unroll
+              for (int v = 0; v < V; ++v) acc[q] = fma(blk[u][q][v], xv[u][v], acc[q]);
           }
         }
         // rows with more entries than are staged: codes and blocks from global memory
@@ -347,21 +375,11 @@ __global__ void __launch_bounds__(W * 32) k_ssweep(const SSP<VT> p) {
         }
         // x_r = rhs_r - sum (no D), or D_r rhs_r - sum with the blocks
         // premultiplied by D_r; the CPR lanes of each block row then reduce
-        const double* rh = reinterpret_cast<const double*>(sl + C::OFF_R);
         double xr[P];
-        if constexpr (HAS_D) {
 #pragma unroll
-          for (int q = 0; q < P; ++q) {
-            double a[V];
-            ChunkOps<VT, V>::get(sl + C::OFF_D + (q * 32 + l) * CB, a);
-            double o = 0.0;
-#pragma unroll
-            for (int v = 0; v < V; ++v) o = fma(a[v], rh[c0 + v], o);
-            xr[q] = row_reduce<CPR>(o - acc[q], 0xffffffffu);
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < P; ++q) xr[q] = rh[q * RPP + l / CPR] - row_reduce<CPR>(acc[q], 0xffffffffu);
+        for (int q = 0; q < P; ++q) {
+          if constexpr (HAS_D) xr[q] = row_reduce<CPR>(base[q] - acc[q], 0xffffffffu);
+          else xr[q] = base[q] - row_reduce<CPR>(acc[q], 0xffffffffu);
         }
         // publish row r by its values: shared memory first (this CTA's next
         // chains poll it there), then global memory (other CTAs poll it)
