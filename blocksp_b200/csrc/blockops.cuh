@@ -21,16 +21,26 @@ __device__ __forceinline__ void warp_copy_out(double* g, const double* s, int ne
   __syncwarp();
 }
 
+// The routines below take the block size as a template argument BS when it
+// is known at compile time (loops unrolled, index arithmetic by shifts) and
+// at run time otherwise (BS = 0); both forms do the same operations in the
+// same order.
+
 // C = A * B (trB = 0) or C = A * B^T (trB = 1); C must not alias A or B.
-__device__ inline void warp_gemm(double* C, const double* A, const double* B, int bs, bool trB) {
+template <int BS = 0>
+__device__ inline void warp_gemm(double* C, const double* A, const double* B, int bs_rt, bool trB) {
+  const int bs = BS > 0 ? BS : bs_rt;
   const int lane = threadIdx.x & 31;
   for (int e = lane; e < bs * bs; e += 32) {
     const int r = e / bs, c = e % bs;
     double acc = 0.0;
-    if (trB)
-      for (int t = 0; t < bs; ++t) acc = fma(A[r * bs + t], B[c * bs + t], acc);
-    else
-      for (int t = 0; t < bs; ++t) acc = fma(A[r * bs + t], B[t * bs + c], acc);
+    if (trB) {
+#pragma unroll
+      for (int t = 0; t < (BS > 0 ? BS : bs); ++t) acc = fma(A[r * bs + t], B[c * bs + t], acc);
+    } else {
+#pragma unroll
+      for (int t = 0; t < (BS > 0 ? BS : bs); ++t) acc = fma(A[r * bs + t], B[t * bs + c], acc);
+    }
     C[e] = acc;
   }
   __syncwarp();
@@ -55,7 +65,9 @@ __device__ inline void warp_gemm_sub_global(double* G, const double* A, const do
 // Inverse by Gauss-Jordan elimination with partial (row) pivoting.
 // M (bs x bs) is destroyed; aug is scratch of bs*2*bs doubles.  Returns false
 // when a pivot is exactly zero or not finite (singular block).
-__device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, int bs) {
+template <int BS = 0>
+__device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, int bs_rt) {
+  const int bs = BS > 0 ? BS : bs_rt;
   const int lane = threadIdx.x & 31;
   const int w = 2 * bs;
   for (int e = lane; e < bs * w; e += 32) {
@@ -119,7 +131,9 @@ __device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, i
 
 // In-place lower Cholesky A = L L^T (upper triangle zeroed), row-oriented
 // (Cholesky-Banachiewicz).  Returns false on a non-positive pivot.
-__device__ inline bool warp_cholesky(double* A, int bs) {
+template <int BS = 0>
+__device__ inline bool warp_cholesky(double* A, int bs_rt) {
+  const int bs = BS > 0 ? BS : bs_rt;
   const int lane = threadIdx.x & 31;
   bool ok = true;
   for (int j = 0; j < bs; ++j) {
@@ -149,7 +163,9 @@ __device__ inline bool warp_cholesky(double* A, int bs) {
 }
 
 // Inverse of a lower-triangular L (bs <= 32): lane c solves column c.
-__device__ inline void warp_lower_inverse(double* X, const double* L, int bs) {
+template <int BS = 0>
+__device__ inline void warp_lower_inverse(double* X, const double* L, int bs_rt) {
+  const int bs = BS > 0 ? BS : bs_rt;
   const int lane = threadIdx.x & 31;
   if (lane < bs) {
     const int c = lane;

@@ -726,15 +726,20 @@ __global__ void __launch_bounds__(kFactorWarps * 32) k_factor(const FactorP p) {
 // triangular inverse formed (IChol0), and the row is written back.  The same
 // operations in the same order as k_factor (bit-identical factors); only the
 // memory traffic on the dependency path changes.
-__device__ inline void warp_gemm_sub_smem(double* T, const double* A, const double* B, int bs, bool trB) {
+template <int BS = 0>
+__device__ inline void warp_gemm_sub_smem(double* T, const double* A, const double* B, int bs_rt, bool trB) {
+  const int bs = BS > 0 ? BS : bs_rt;
   const int lane = threadIdx.x & 31;
   for (int e = lane; e < bs * bs; e += 32) {
     const int r = e / bs, c = e % bs;
     double acc = 0.0;
-    if (trB)
-      for (int t = 0; t < bs; ++t) acc = fma(A[r * bs + t], B[c * bs + t], acc);
-    else
-      for (int t = 0; t < bs; ++t) acc = fma(A[r * bs + t], B[t * bs + c], acc);
+    if (trB) {
+#pragma unroll
+      for (int t = 0; t < (BS > 0 ? BS : bs); ++t) acc = fma(A[r * bs + t], B[c * bs + t], acc);
+    } else {
+#pragma unroll
+      for (int t = 0; t < (BS > 0 ? BS : bs); ++t) acc = fma(A[r * bs + t], B[t * bs + c], acc);
+    }
     T[e] = T[e] - acc;
   }
   __syncwarp();
@@ -758,14 +763,26 @@ struct FactorRowsP {
   int nbmax, depmax;  // row blocks and dependency blocks staged per warp
 };
 
+// Per warp, after the blocks: the row's elimination plan staged from global
+// memory before the dependency waits (at most kFrEnts lower entries and
+// kFrPairs update pairs; longer rows read the plan from global memory).
+constexpr int kFrEnts = 31, kFrPairs = 96;
+constexpr size_t kFrPlanBytes = kFrPairs * sizeof(int2) + 2 * (kFrEnts + 1) * sizeof(int);
+
+template <int BS>
 __global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
   extern __shared__ double fr_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int bs = p.bs, b2 = bs * bs;
-  double* rowb = fr_smem + (size_t)warp * (p.nbmax + p.depmax + 3) * b2;
+  const int bs = BS > 0 ? BS : p.bs, b2 = bs * bs;
+  const size_t warp_bytes = (size_t)(p.nbmax + p.depmax + 3) * b2 * sizeof(double) + kFrPlanBytes;
+  unsigned char* wbase = reinterpret_cast<unsigned char*>(fr_smem) + (size_t)warp * warp_bytes;
+  double* rowb = reinterpret_cast<double*>(wbase);
   double* dep = rowb + (size_t)p.nbmax * b2;
   double* Lb = dep + (size_t)p.depmax * b2;
   double* aug = Lb + b2;
+  int2* prw = reinterpret_cast<int2*>(aug + 2 * b2);
+  int* ppw = reinterpret_cast<int*>(prw + kFrPairs);
+  int* colw = ppw + kFrEnts + 1;
   const bool chol = p.mode == FACT_ICHOL0;
   while (true) {
     int t = 0;
@@ -778,25 +795,41 @@ __global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
     for (int x = lane; x < (end - beg) * b2; x += 32)
       cp_async_small<8>(rowb + x, p.vals + (int64_t)beg * b2 + x);
     cp_async_commit();
-    for (int e = beg; e < dg; ++e) wait_flag(p.flags + __ldg(p.col + e), p.epoch, p.st, k, p.spin_limit);
+    // and its elimination plan (entry offsets, columns, update pairs)
+    const int nl = dg - beg;
+    bool staged = nl <= kFrEnts;
+    if (staged) {
+      if (lane <= nl) ppw[lane] = __ldg(p.pp + beg + lane);
+      if (lane < nl) colw[lane] = __ldg(p.col + beg + lane);
+    }
+    __syncwarp();
+    const int q0 = staged ? ppw[0] : 0;
+    staged = staged && ppw[nl] - q0 <= kFrPairs;
+    if (staged)
+      for (int y = lane; y < ppw[nl] - q0; y += 32) prw[y] = p.pairs[q0 + y];
+    __syncwarp();
+    auto PP = [&](int x) { return staged ? ppw[x - beg] : __ldg(p.pp + x); };
+    auto PR = [&](int q) { return staged ? prw[q - q0] : p.pairs[q]; };
+    auto COL = [&](int x) { return staged ? colw[x - beg] : __ldg(p.col + x); };
+    for (int e = beg; e < dg; ++e) wait_flag(p.flags + COL(e), p.epoch, p.st, k, p.spin_limit);
     int e = beg;
     while (e < dg) {
       // a batch of consecutive lower entries whose dependency blocks fit
       int used = 0, eb = e;
       while (eb < dg) {
         int need = 1;
-        for (int q = __ldg(p.pp + eb); q < __ldg(p.pp + eb + 1); ++q) need += __ldg(&p.pairs[q].y) >= 0;
+        for (int q = PP(eb); q < PP(eb + 1); ++q) need += PR(q).y >= 0;
         if (eb > e && used + need > p.depmax) break;
         used += need;
         ++eb;
       }
       int slot = 0;
       for (int x = e; x < eb; ++x) {
-        const double* src = p.dinv + (int64_t)__ldg(p.col + x) * b2;
+        const double* src = p.dinv + (int64_t)COL(x) * b2;
         for (int y = lane; y < b2; y += 32) cp_async_small<8>(dep + (size_t)slot * b2 + y, src + y);
         ++slot;
-        for (int q = __ldg(p.pp + x); q < __ldg(p.pp + x + 1); ++q) {
-          const int s = __ldg(&p.pairs[q].y);
+        for (int q = PP(x); q < PP(x + 1); ++q) {
+          const int s = PR(q).y;
           if (s < 0) continue;
           for (int y = lane; y < b2; y += 32) cp_async_small<8>(dep + (size_t)slot * b2 + y, p.vals + (int64_t)s * b2 + y);
           ++slot;
@@ -809,12 +842,12 @@ __global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
       for (int x = e; x < eb; ++x) {
         double* Ak = rowb + (size_t)(x - beg) * b2;
         // ILU0: L_ki = A_ki U_ii^{-1};  IChol0: L_ki = A_ki L_ii^{-T}
-        warp_gemm(Lb, Ak, dep + (size_t)slot * b2, bs, chol);
+        warp_gemm<BS>(Lb, Ak, dep + (size_t)slot * b2, bs, chol);
         ++slot;
         for (int y = lane; y < b2; y += 32) Ak[y] = Lb[y];
         __syncwarp();
-        for (int q = __ldg(p.pp + x); q < __ldg(p.pp + x + 1); ++q) {
-          const int2 pr = p.pairs[q];
+        for (int q = PP(x); q < PP(x + 1); ++q) {
+          const int2 pr = PR(q);
           const double* S;
           if (pr.y >= 0) {
             S = dep + (size_t)slot * b2;
@@ -822,7 +855,7 @@ __global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
           } else {
             S = rowb + (size_t)(-1 - pr.y - beg) * b2;
           }
-          warp_gemm_sub_smem(rowb + (size_t)(pr.x - beg) * b2, Lb, S, bs, chol);
+          warp_gemm_sub_smem<BS>(rowb + (size_t)(pr.x - beg) * b2, Lb, S, bs, chol);
         }
       }
       e = eb;
@@ -831,11 +864,11 @@ __global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
     __syncwarp();
     double* Dk = rowb + (size_t)(dg - beg) * b2;
     if (chol) {
-      const bool ok = warp_cholesky(Dk, bs);
+      const bool ok = warp_cholesky<BS>(Dk, bs);
       if (!ok && lane == 0) set_status(p.st, BSP_NOT_SPD, k);
-      warp_lower_inverse(Lb, Dk, bs);
+      warp_lower_inverse<BS>(Lb, Dk, bs);
     } else {
-      const bool ok = warp_inverse(Lb, Dk, aug, bs);  // aug: bs x 2bs scratch
+      const bool ok = warp_inverse<BS>(Lb, Dk, aug, bs);  // aug: bs x 2bs scratch
       if (!ok && lane == 0) set_status(p.st, BSP_ZERO_PIVOT, k);
     }
     for (int x = lane; x < (end - beg) * b2; x += 32) p.vals[(int64_t)beg * b2 + x] = rowb[x];
@@ -1073,7 +1106,7 @@ static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* 
   const FactorPlan* plan = pc->plan.get();
   const size_t b2 = (size_t)pc->bs * pc->bs;
   const int depmax = plan ? std::max(plan->max_deps, 4) : 0;
-  const size_t per_warp = plan ? (size_t)(plan->max_row + depmax + 3) * b2 * sizeof(double) : 0;
+  const size_t per_warp = plan ? (size_t)(plan->max_row + depmax + 3) * b2 * sizeof(double) + kFrPlanBytes : 0;
   if (mode != FACT_DIAG && plan && pc->bs <= 16 && per_warp <= kFactorRowsSmem && ptr == pc->f_ptr.get()) {
     FactorRowsP rp;
     rp.n = n;
@@ -1096,9 +1129,16 @@ static int run_factor(bsp_precond_s* pc, int mode, const int* order, const int* 
     rp.depmax = depmax;
     const int warps = (int)std::max<size_t>(1, std::min<size_t>(8, kFactorRowsSmem / per_warp));
     const size_t smem = per_warp * warps;
-    BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = persistent_grid(h, k_factor_rows, warps * 32, smem);
-    bsp::count_launch(), k_factor_rows<<<grid, warps * 32, smem, h->stream>>>(rp);
+    auto launch = [&](auto kern) -> int {
+      BSP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const int grid = persistent_grid(h, kern, warps * 32, smem);
+      bsp::count_launch(), kern<<<grid, warps * 32, smem, h->stream>>>(rp);
+      return BSP_OK;
+    };
+    if (pc->bs == 8) BSP_TRY(launch(k_factor_rows<8>));
+    else if (pc->bs == 16) BSP_TRY(launch(k_factor_rows<16>));
+    else if (pc->bs == 4) BSP_TRY(launch(k_factor_rows<4>));
+    else BSP_TRY(launch(k_factor_rows<0>));
   } else {
     const size_t smem = (size_t)kFactorWarps * 5 * pc->bs * pc->bs * sizeof(double);
     BSP_CUDA_TRY(cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1969,7 +2009,6 @@ int bsp_precond_export(bsp_precond_t pc, double* vals_host, int64_t capacity) {
   if (!pc || !vals_host) return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(pc->device));
   const int b2 = pc->bs * pc->bs;
-  bsp_handle_s* h = pc->h;
   if (pc->kind == BSP_PC_ILU0 || pc->kind == BSP_PC_ICHOL0 || pc->kind == BSP_PC_LEARNED_LU ||
       pc->kind == BSP_PC_LEARNED_LLT) {
     // blocks in the caller's layout: ILU0 / learned LU in A's block order; IChol0 in the
@@ -1995,7 +2034,6 @@ int bsp_precond_export(bsp_precond_t pc, double* vals_host, int64_t capacity) {
     if (capacity < (int64_t)pc->n * b2) return BSP_INVALID;
     BSP_CUDA_TRY(cudaMemcpy(vals_host, pc->dinv.get(), (size_t)pc->n * b2 * sizeof(double), cudaMemcpyDeviceToHost));
   }
-  (void)h;
   return BSP_OK;
 }
 
