@@ -369,6 +369,12 @@ __global__ void __launch_bounds__(kMgsThreads, 1) k_mgs(const MgsP p) {
   const int t = threadIdx.x;
   const int64_t beg = (int64_t)blockIdx.x * p.slice;
   const int nloc = (int)((beg + p.slice < p.len ? beg + p.slice : p.len) - beg);  // may be <= 0
+  // the first two basis vectors' slices start streaming into L2 now; later
+  // ones two passes ahead of their use
+  if (t < 32) {
+    prefetch_l2(p.Q[0] + beg, nloc);
+    if (p.j >= 1) prefetch_l2(p.Q[1] + beg, nloc);
+  }
   double v[NPT];
   {
     const double* vb = p.v + beg;
@@ -407,8 +413,8 @@ __global__ void __launch_bounds__(kMgsThreads, 1) k_mgs(const MgsP p) {
     }
     a = cta_sum_1024(a, red);
     if (t == 0) p.partials[(size_t)i * gridDim.x + blockIdx.x] = a;
-    // the next basis vector's slice streams into L2 while the grid meets
-    if (t < 32 && i < p.j) prefetch_l2(p.Q[i + 1] + beg, nloc);
+    // a later basis vector's slice streams into L2 while the grid meets
+    if (t < 32 && i + 2 <= p.j) prefetch_l2(p.Q[i + 2] + beg, nloc);
     mgs_barrier(p, ++gen);
     h = grid_total(p.partials + (size_t)i * gridDim.x, red);
     if (blockIdx.x == 0 && t == 0) p.H[(size_t)i * p.ldh + p.j] = h;
@@ -646,16 +652,49 @@ __global__ void __launch_bounds__(32) k_gm_deflate(GPtrs g, int k_req, int max_k
 
 // Qout[0..k] <- Qn[0..m1-1] P_{k+1} (deflated_restart.hpp:250-258), written to
 // spare vectors; the host then swaps the pointer tables.
-__global__ void k_gm_qn_update(int64_t len, double* const* __restrict__ Q, double* const* __restrict__ Qout,
-                               const double* __restrict__ P, int ldp, const KHead* __restrict__ head,
-                               int m1) {
+// Qout[c] = sum_i Q[i] P[i][c] for c <= keff: each thread reads its entry of
+// the m1 basis vectors once (in chunks of 32, in registers) and forms every
+// output column from them, summing in basis order; P sits in shared memory.
+// Up to kQnCols output columns; wider restarts take the column-by-column loop.
+constexpr int kQnCols = 16;
+__global__ void __launch_bounds__(256) k_gm_qn_update(int64_t len, double* const* __restrict__ Q,
+                                                      double* const* __restrict__ Qout, const double* __restrict__ P,
+                                                      int ldp, const KHead* __restrict__ head, int m1) {
+  extern __shared__ double ps[];  // m1 x kQnCols
   const int kp1 = head->keff + 1;  // <= the spare count, checked by k_gm_deflate
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
-    for (int c = 0; c < kp1; ++c) {
-      double s = 0.0;
-      for (int i = 0; i < m1; ++i) s += Q[i][e] * P[i * ldp + c];
-      Qout[c][e] = s;
+  if (kp1 > kQnCols) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
+      for (int c = 0; c < kp1; ++c) {
+        double s = 0.0;
+        for (int i = 0; i < m1; ++i) s += Q[i][e] * P[i * ldp + c];
+        Qout[c][e] = s;
+      }
     }
+    return;
+  }
+  for (int t = threadIdx.x; t < m1 * kQnCols; t += blockDim.x) {
+    const int i = t / kQnCols, c = t % kQnCols;
+    ps[t] = c < kp1 ? P[i * ldp + c] : 0.0;
+  }
+  __syncthreads();
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
+    double s[kQnCols];
+#pragma unroll
+    for (int c = 0; c < kQnCols; ++c) s[c] = 0.0;
+    for (int i0 = 0; i0 < m1; i0 += 32) {
+      double qv[32];
+#pragma unroll
+      for (int t = 0; t < 32; ++t) qv[t] = i0 + t < m1 ? __ldcs(Q[i0 + t] + e) : 0.0;
+#pragma unroll
+      for (int t = 0; t < 32; ++t)
+        if (i0 + t < m1) {
+#pragma unroll
+          for (int c = 0; c < kQnCols; ++c) s[c] += qv[t] * ps[(i0 + t) * kQnCols + c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kQnCols; ++c)
+      if (c < kp1) Qout[c][e] = s[c];
   }
 }
 
@@ -1065,7 +1104,8 @@ int pgmres_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const doub
         bsp::count_launch(), k_gm_pure_restart<<<1, 1, 0, h->stream>>>(gp);
       } else {
         bsp::count_launch(), k_gm_deflate<<<1, 32, defl_smem, h->stream>>>(gp, k_req, n_spare, defl_smem > 0);
-        bsp::count_launch(), k_gm_qn_update<<<g, 256, 0, h->stream>>>(len, dq.get(), dspare.get(), gp.P, m + 1, hd, st.j + 1);
+        bsp::count_launch(), k_gm_qn_update<<<g, 256, (size_t)(st.j + 1) * kQnCols * sizeof(double), h->stream>>>(
+            len, dq.get(), dspare.get(), gp.P, m + 1, hd, st.j + 1);
       }
       BSP_CUDA_TRY(cudaPeekAtLastError());
       BSP_TRY(read_head(h, hd, &st));
