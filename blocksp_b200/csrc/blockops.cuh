@@ -62,11 +62,76 @@ __device__ inline void warp_gemm_sub_global(double* G, const double* A, const do
   __syncwarp();
 }
 
+// Gauss-Jordan inverse with the augmented matrix [M | I] held by columns in
+// registers: lane c (c < 2 BS) keeps column c.  The same pivots, divisions
+// and FMAs as the shared-memory form below, without its shared-memory round
+// trips and warp barriers per step.
+template <int BS>
+__device__ inline bool warp_inverse_cols(double* Inv, const double* M) {
+  const int lane = threadIdx.x & 31;
+  constexpr int W2 = 2 * BS;
+  double col[BS];
+#pragma unroll
+  for (int r = 0; r < BS; ++r)
+    col[r] = lane < BS ? M[r * BS + lane] : (lane < W2 && lane - BS == r ? 1.0 : 0.0);
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < BS; ++k) {
+    // pivot: the largest |aug[r][k]| over r >= k, the lowest row on ties, a
+    // NaN never chosen over a number (lane k scans its column)
+    double best = -1.0;
+    int bidx = k;
+#pragma unroll
+    for (int r = k; r < BS; ++r) {
+      double v = fabs(col[r]);
+      if (v != v) v = -0.5;
+      if (v > best) {
+        best = v;
+        bidx = r;
+      }
+    }
+    best = __shfl_sync(0xffffffffu, best, k);
+    bidx = __shfl_sync(0xffffffffu, bidx, k);
+    if (!(best > 0.0) || !isfinite(best)) ok = false;
+    if (bidx != k) {  // rows k and bidx swap in every column
+      double tb = 0.0;
+#pragma unroll
+      for (int r = k + 1; r < BS; ++r)
+        if (r == bidx) tb = col[r];
+#pragma unroll
+      for (int r = k + 1; r < BS; ++r)
+        if (r == bidx) col[r] = col[k];
+      col[k] = tb;
+    }
+    const double piv = __shfl_sync(0xffffffffu, col[k], k);
+    col[k] = col[k] / piv;
+    // eliminate column k from the other rows with the multipliers aug[r][k]
+#pragma unroll
+    for (int r = 0; r < BS; ++r) {
+      if (r == k) continue;
+      const double mult = __shfl_sync(0xffffffffu, col[r], k);
+      if (lane != k) col[r] = fma(-mult, col[k], col[r]);
+    }
+    if (lane == k) {
+#pragma unroll
+      for (int r = 0; r < BS; ++r)
+        if (r != k) col[r] = 0.0;
+    }
+  }
+  if (lane >= BS && lane < W2) {
+#pragma unroll
+    for (int r = 0; r < BS; ++r) Inv[r * BS + (lane - BS)] = col[r];
+  }
+  __syncwarp();
+  return ok;
+}
+
 // Inverse by Gauss-Jordan elimination with partial (row) pivoting.
 // M (bs x bs) is destroyed; aug is scratch of bs*2*bs doubles.  Returns false
 // when a pivot is exactly zero or not finite (singular block).
 template <int BS = 0>
 __device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, int bs_rt) {
+  if constexpr (BS > 0 && BS <= 16) return warp_inverse_cols<BS>(Inv, M);
   const int bs = BS > 0 ? BS : bs_rt;
   const int lane = threadIdx.x & 31;
   const int w = 2 * bs;
@@ -85,10 +150,14 @@ __device__ inline bool warp_inverse(double* Inv, const double* M, double* aug, i
       if (best != best) best = -0.5;  // NaN never wins the comparison below
       bidx = lane;
     }
+    // the candidates sit in lanes 0..bs-1: a butterfly over the smallest
+    // power-of-two segment that holds them (the whole warp when bs is known
+    // only at run time)
+    constexpr int SEG = BS <= 0 ? 32 : BS <= 4 ? 4 : BS <= 8 ? 8 : BS <= 16 ? 16 : 32;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+    for (int o = SEG / 2; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o, SEG);
+      const int oi = __shfl_xor_sync(0xffffffffu, bidx, o, SEG);
       if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
     }
     // Every lane must take the same pivot: the row swap below is a branch that

@@ -770,7 +770,7 @@ constexpr int kFrEnts = 31, kFrPairs = 96;
 constexpr size_t kFrPlanBytes = kFrPairs * sizeof(int2) + 2 * (kFrEnts + 1) * sizeof(int);
 
 template <int BS>
-__global__ void __launch_bounds__(256) k_factor_rows(const FactorRowsP p) {
+__global__ void __launch_bounds__(256, 1) k_factor_rows(const FactorRowsP p) {
   extern __shared__ double fr_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bs = BS > 0 ? BS : p.bs, b2 = bs * bs;
