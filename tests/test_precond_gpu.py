@@ -122,3 +122,38 @@ def test_missing_diagonal_block_is_reported(handle):
     with pytest.raises(bsp.BspError) as e:
         bsp.ILU0(A)
     assert e.value.status == 1
+
+
+def long_row_system(n, bs, band, seed):
+    """Block rows holding every block column in [i - band, i + 2] (clipped):
+    rows past `band` have more lower entries than the factorisation stages per
+    row, so both the staged and the global-memory elimination plans run.
+    Diagonal blocks dominate, so ILU0 exists and is well conditioned."""
+    from blocksp_b200.systems import BSRSystem
+    rng = np.random.default_rng(seed)
+    rp, ci, vs = [0], [], []
+    for i in range(n):
+        cols = list(range(max(0, i - band), min(n, i + 3)))
+        blocks = {j: rng.uniform(-1, 1, (bs, bs)) / (bs * len(cols)) for j in cols if j != i}
+        blocks[i] = np.eye(bs) * 2.0 + rng.uniform(-0.1, 0.1, (bs, bs))
+        for j in cols:
+            ci.append(j)
+            vs.append(blocks[j])
+        rp.append(len(ci))
+    return BSRSystem(n=n, bs=bs, row_ptr=np.array(rp, dtype=np.int32), col_idx=np.array(ci, dtype=np.int32),
+                     vals=np.array(vs).reshape(-1, bs, bs), b=rng.uniform(-1, 1, n * bs), name=f"band{band}")
+
+
+@pytest.mark.parametrize("bs", [4, 8, 16])
+def test_ilu0_long_rows(handle, bs):
+    """Rows with 40 lower blocks (more than the staged plan holds) against the oracle."""
+    import blocksp_b200 as bsp
+    s = long_row_system(72, bs, 40, seed=bs)
+    A = bsp.Matrix.from_system(s, handle)
+    pc = bsp.ILU0(A)
+    ref = O.ILU0(O.BSR.from_system(s))
+    assert rel(pc.export(), ref.LU.vals) <= 1e-12
+    r = np.random.default_rng(3).uniform(-1, 1, s.n * bs)
+    assert rel(pc.apply_host(r), ref(r)) <= 1e-11
+    pc.close()
+    A.close()
