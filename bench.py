@@ -459,6 +459,24 @@ def batch_cpu_sample(specs, iters, budget_s: float = 25.0) -> dict | None:
 
 
 def run_batch(args):
+    print(json.dumps(batch_measure(args, args.steps, max(args.warmup, 3), not args.no_cpu_baseline)), flush=True)
+
+
+def batch_summary(args) -> dict:
+    """cfg3 inside the default line: one warm-up and one timed batched solve
+    (the standalone `--workload batch` run is the full measurement)."""
+    line = batch_measure(args, 1, 1, False)
+    it = line["iterations"]
+    return {"metric": line["metric"], "value": line["value"], "unit": "s", "steps": 1, "warmup": 1,
+            "systems": line["config"]["systems"], "rhs": line["config"]["rhs"],
+            "iterations_max": it["max"], "converged_pairs": it["converged_pairs"], "pairs": it["pairs"],
+            "achieved_gbs": line["roofline"]["achieved"], "frac_of_peak": line["roofline"]["frac"],
+            "e2e_s": line["e2e"]["value"], "gpu_launches": line["gpu_launches"],
+            "launch": "one CUDA graph launch per solve; its device-side while node replays one pCG "
+                      "iteration of every block-size group (several kernels) until every pair converges"}
+
+
+def batch_measure(args, steps: int, warmup: int, with_cpu: bool) -> dict:
     import torch
     import blocksp_b200 as bsp
     from blocksp_b200 import _lib, systems
@@ -485,20 +503,20 @@ def run_batch(args):
         return e
 
     first = None
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(warmup):
         x, info = B.pcg(bd, R, TOL, 2000)
         first = first or info
     torch.cuda.synchronize()
     with ClockSampler(0) as clk:
         l0 = lib.bsp_launch_count()
         e0 = ev()
-        for _ in range(args.steps):
+        for _ in range(steps):
             x, info = B.pcg(bd, R, TOL, 2000)
         e1 = ev()
         e1.synchronize()
         launches = lib.bsp_launch_count() - l0
     clocks = clk.summary()
-    solve_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    solve_s = e0.elapsed_time(e1) / 1e3 / steps
     res = B.results()
     # algorithmic bytes: every system active for (its slowest pair's iterations + 1)
     total_bytes = 0
@@ -511,7 +529,7 @@ def run_batch(args):
     e2e_s = time.perf_counter() - t0
     tun = B.tuning()
     cpu = None
-    if not args.no_cpu_baseline:
+    if with_cpu:
         cs = batch_cpu_sample(specs, res["iters"])
         if cs is not None and all(bs in cs for bs in (4, 8)):
             est = 0.0
@@ -529,7 +547,7 @@ def run_batch(args):
     nnzb = int(sum(s.nnzb for s in sl))
     line = {
         "metric": BATCH_METRIC, "value": solve_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "dtype": "f64",
+        "steps": steps, "warmup": warmup, "ms_per_step": solve_s * 1e3, "dtype": "f64",
         "data": "synthetic (seeded 2D 5-point block stencils)", "vs_baseline": None, "scaling": "weak",
         "config": {"workload": f"{len(sl)} SPD 2D block systems, sides log-uniform 32..256, bs 4/8 by seed, "
                                f"{R} RHS each; batched pCG + block IChol0, FP64, tol 1e-10",
@@ -546,11 +564,11 @@ def run_batch(args):
                      "traffic": None, "peak_source": peak_kind,
                      "algorithmic_bytes": total_bytes},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": bh.nbytes, "d2h_bytes_per_step": bh.nbytes},
-        "gpu_launches": launches // args.steps, "clocks": clocks, "cpu_baseline": cpu,
+        "gpu_launches": launches // steps, "clocks": clocks, "cpu_baseline": cpu,
     }
     B.close()
     h.close()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ----------------------------------------------------------------- mixed / learned workloads
@@ -748,6 +766,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default="plain_f64,mixed_f32,learned_mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="leave the cfg3 batch summary out of the default line")
     ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch", "mixed", "learned", "apply"],
                     help="cfg1: the headline line; batch: 256-system batched pCG; mixed: cfg2 precision "
                          "variants; learned: cfg4 ablation; apply: the ILU0 application alone (profiling)")
@@ -848,6 +867,8 @@ def main():
         "clocks": r["clocks"],
         "cpu_baseline": cpu,
     }
+    if not args.no_batch and args.gpus == 1:
+        line["batch"] = batch_summary(args)
     print(json.dumps(line), flush=True)
 
 
