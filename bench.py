@@ -191,12 +191,14 @@ def north_star(results: dict) -> dict | None:
     from blocksp_b200 import learned
     if "plain_f64" not in results or "learned_mixed_f32" not in results:
         return None
-    gate = None
-    if learned.WEIGHTS.exists():
-        gate = bool(json.loads(str(np.load(learned.WEIGHTS)["meta"])).get("beats_ilu0", False))
+    meta = json.loads(str(np.load(learned.WEIGHTS)["meta"])) if learned.WEIGHTS.exists() else {}
     plain, lm = results["plain_f64"]["total_s"], results["learned_mixed_f32"]["total_s"]
     return {"plain_f64_s": plain, "learned_mixed_f32_s": lm, "speedup": plain / lm,
-            "learned_gate_open": gate, "preconditioner_used": results["learned_mixed_f32"].get("preconditioner")}
+            "plain_f64_iters": results["plain_f64"]["iters"],
+            "learned_mixed_f32_iters": results["learned_mixed_f32"]["iters"],
+            "learned_gate_open": meta.get("beats_ilu0"), "learned_relax": meta.get("relax"),
+            "learned_network_used": meta.get("network_used"),
+            "preconditioner_used": results["learned_mixed_f32"].get("preconditioner")}
 
 
 def pc_name(pc) -> str:
@@ -573,9 +575,9 @@ def batch_measure(args, steps: int, warmup: int, with_cpu: bool) -> dict:
 
 # ----------------------------------------------------------------- mixed / learned workloads
 
-def _solve_variant(bsp, _lib, A, b, stream, make_pc, precision):
-    """One timed solve: preconditioner set-up + refined pGMRES(30, k=10) to the
-    FP64 true relative residual 1e-10."""
+def _solve_variant(bsp, _lib, A, b, stream, make_pc, precision, solver="pgmres"):
+    """One timed solve: preconditioner set-up + refined pGMRES(30, k=10) (or
+    pCG) to the FP64 true relative residual 1e-10."""
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -583,8 +585,12 @@ def _solve_variant(bsp, _lib, A, b, stream, make_pc, precision):
     e0.record(stream)
     pc = make_pc()
     e1.record(stream)
-    x, info, _ = bsp.pGMRES(A, b, TOL, pc, 20000, 30, 10, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL,
-                            precision=precision, inner_tol=1e-6)
+    if solver == "pcg":
+        x, info, _ = bsp.pCG(A, b, TOL, pc, 20000, return_info=True, stop_rule=_lib.STOP_TRUE_RESIDUAL,
+                             precision=precision, inner_tol=1e-6)
+    else:
+        x, info, _ = bsp.pGMRES(A, b, TOL, pc, 20000, 30, 10, return_info=True,
+                                stop_rule=_lib.STOP_TRUE_RESIDUAL, precision=precision, inner_tol=1e-6)
     e2.record(stream)
     e2.synchronize()
     kind = pc.kind
@@ -713,6 +719,81 @@ def run_learned(args):
     print(json.dumps(line), flush=True)
 
 
+def llt_measure(args, warmup: int, steps: int) -> dict:
+    """The learned L L^T preconditioner against block IChol0: held-out SPD 3D
+    diffusion systems (8x8 blocks, log-normal conductivity), pCG to the FP64
+    true relative residual 1e-10; per variant the mean set-up + solve time over
+    `steps` timed solves after `warmup`, on each seed."""
+    import torch
+    import blocksp_b200 as bsp
+    from blocksp_b200 import _lib, learned, systems
+    stream = torch.cuda.Stream()
+    h = bsp.Handle(0, stream=stream.cuda_stream)
+    model = learned.LearnedModel.load(learned.WEIGHTS_LLT, handle=h) if learned.WEIGHTS_LLT.exists() else None
+    seeds = [30200 + i for i in range(args.learned_seeds)]
+    dims = (args.llt_side,) * 3
+    variants = (("ichol0_f64", lambda A: bsp.IChol0(A), _lib.PREC_F64),
+                ("ichol0_f32", lambda A: bsp.IChol0(A, _lib.PREC_F32), _lib.PREC_F32),
+                ("learned_llt_f64", lambda A: learned.LearnedLLT(A, model), _lib.PREC_F64),
+                ("learned_llt_f32", lambda A: learned.LearnedLLT(A, model, _lib.PREC_F32), _lib.PREC_F32))
+    per = []
+    launches = 0
+    lib = _lib.load()
+    with ClockSampler(0) as clk:
+        for sd in seeds:
+            s = systems.convection_diffusion_system(dims, 8, sd, speed=0.0)
+            A = bsp.Matrix.from_system(s, h)
+            b = torch.tensor(s.b, device="cuda")
+            row = {"seed": sd}
+            for vname, mk, prec in variants:
+                for _ in range(warmup):
+                    _solve_variant(bsp, _lib, A, b, stream, lambda: mk(A), prec, "pcg")
+                l0 = lib.bsp_launch_count()
+                runs = [_solve_variant(bsp, _lib, A, b, stream, lambda: mk(A), prec, "pcg")[1] for _ in range(steps)]
+                launches += lib.bsp_launch_count() - l0
+                row[vname] = {**runs[-1], "total_s": float(np.mean([r["total_s"] for r in runs])),
+                              "setup_s": float(np.mean([r["setup_s"] for r in runs])),
+                              "solve_s": float(np.mean([r["solve_s"] for r in runs]))}
+            per.append(row)
+            A.close()
+    names = [v[0] for v in variants]
+    summary = {k: {"total_s": float(np.mean([r[k]["total_s"] for r in per])),
+                   "setup_s": float(np.mean([r[k]["setup_s"] for r in per])),
+                   "iters": float(np.mean([r[k]["iters"] for r in per])),
+                   "max_true_rel_res": float(max(r[k]["true_rel_res"] for r in per))} for k in names}
+    gate = bool(model is not None and model.meta.get("beats_baseline", False))
+    out = {"metric": "learned L L^T vs block IChol0: pCG time to FP64 true relative residual 1e-10",
+           "value": summary["learned_llt_f32"]["total_s"], "unit": "s", "higher_is_better": False,
+           "speedup_vs_ichol0_f64": summary["ichol0_f64"]["total_s"] / summary["learned_llt_f32"]["total_s"],
+           "iteration_ratio_f64": summary["learned_llt_f64"]["iters"] / summary["ichol0_f64"]["iters"],
+           "seeds": seeds, "side": dims[0], "steps": steps, "warmup": warmup, "gate_open": gate,
+           "relax": model.relax if model is not None else None,
+           "network_used": model.meta.get("network_used") if model is not None else None,
+           "summary": summary, "per_seed": per, "gpu_launches": launches, "clocks": clk.summary()}
+    if model is not None:
+        model.close()
+    h.close()
+    return out
+
+
+def run_learned_llt(args):
+    m = llt_measure(args, max(args.warmup, 3), args.steps)
+    line = {**m, "n_gpus": 1, "dtype": "f64 (f32 storage variants marked)", "vs_baseline": None,
+            "data": f"synthetic held-out seeds {m['seeds']} (training used 10000-10099, relaxation fit "
+                    "15000-15003, validation 20000-20003)",
+            "config": {"workload": f"SPD 3D {m['side']}^3 diffusion, 8x8 blocks, pCG + IChol0 / learned L L^T"}}
+    print(json.dumps(line), flush=True)
+
+
+def llt_summary(args) -> dict:
+    """The learned L L^T comparison inside the default line: one warm-up and
+    one timed solve per variant and seed (`--workload learned_llt` is the full
+    measurement)."""
+    m = llt_measure(args, 1, 1)
+    return {k: m[k] for k in ("metric", "value", "unit", "speedup_vs_ichol0_f64", "iteration_ratio_f64", "seeds",
+                              "side", "gate_open", "relax", "network_used", "summary", "gpu_launches")}
+
+
 def run_apply(args):
     """The ILU0 application alone (forward + backward streamed sweeps) on the
     64^3 8x8 system, `steps` times after `warmup`: the kernel the solve's
@@ -767,9 +848,14 @@ def main():
     ap.add_argument("--variants", default="plain_f64,mixed_f32,learned_mixed_f32")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="leave the cfg3 batch summary out of the default line")
-    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "batch", "mixed", "learned", "apply"],
+    ap.add_argument("--no-llt", action="store_true",
+                    help="leave the learned L L^T vs IChol0 summary out of the default line")
+    ap.add_argument("--workload", default="cfg1",
+                    choices=["cfg1", "batch", "mixed", "learned", "learned_llt", "apply"],
                     help="cfg1: the headline line; batch: 256-system batched pCG; mixed: cfg2 precision "
-                         "variants; learned: cfg4 ablation; apply: the ILU0 application alone (profiling)")
+                         "variants; learned: cfg4 ablation; learned_llt: learned L L^T vs IChol0 with pCG; "
+                         "apply: the ILU0 application alone (profiling)")
+    ap.add_argument("--llt-side", type=int, default=64)
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--learned-side", type=int, default=96)
     ap.add_argument("--learned-seeds", type=int, default=2)
@@ -781,7 +867,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": f"the {args.workload} leg reports its CPU "
                               "reference inside its own line"}))
             return
-        {"batch": run_batch, "mixed": run_mixed, "learned": run_learned, "apply": run_apply}[args.workload](args)
+        {"batch": run_batch, "mixed": run_mixed, "learned": run_learned, "learned_llt": run_learned_llt,
+         "apply": run_apply}[args.workload](args)
         return
     world, rank, local = dist_setup(args.dist_backend)
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "
@@ -869,6 +956,8 @@ def main():
     }
     if not args.no_batch and args.gpus == 1:
         line["batch"] = batch_summary(args)
+    if not args.no_llt and args.gpus == 1:
+        line["learned_llt"] = llt_summary(args)
     print(json.dumps(line), flush=True)
 
 

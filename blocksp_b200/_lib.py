@@ -112,6 +112,8 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_learned_create": (_I, [_P, _I, _I, C.POINTER(_P)]),
     "bsp_learned_destroy": (_I, [_P]),
     "bsp_learned_set_form": (_I, [_P, _I]),
+    "bsp_learned_set_relax": (_I, [_P, C.c_double]),
+    "bsp_learned_get_relax": (_I, [_P, C.POINTER(C.c_double)]),
     "bsp_learned_param_count": (_I, [_P, C.POINTER(_I64)]),
     "bsp_learned_set_params": (_I, [_P, _P, _I64]),
     "bsp_learned_get_params": (_I, [_P, _P, _I64]),

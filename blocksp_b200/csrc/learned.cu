@@ -657,6 +657,8 @@ struct ModelBase {
   virtual int adam(bsp_handle_s* h, double lr, double b1, double b2, double eps) = 0;
   virtual int get(double* out, int64_t cnt, int which) = 0;
   virtual int set(const double* in, int64_t cnt) = 0;
+  // true while both decoders are exactly zero (the network's output dF is zero)
+  virtual bool decoders_zero() const = 0;
 };
 
 }  // namespace
@@ -666,6 +668,7 @@ struct bsp_learned_s {
   int device = 0;
   int bs = 0, dtype = 0;
   int form = BSP_LEARNED_LU;  // factor form the network emits
+  double relax = 0.0;        // off-diagonal factor blocks scaled by 1 + relax
   int64_t n_params = 0;
   std::vector<ParamSlot> slots;
   std::unique_ptr<ModelBase> impl;
@@ -735,6 +738,7 @@ template <typename T> struct Model : ModelBase {
   bsp_learned_s* M;
   DevBuf<T> p, g, m, v, part;
   int64_t step = 0;
+  bool dec_zero = true;  // parameters start at zero
   // per-matrix cache
   GraphBuf G;
   const bsp_matrix_s* cachedA = nullptr;
@@ -836,6 +840,7 @@ template <typename T> struct Model : ModelBase {
       work->precision = BSP_PREC_F64;
       BSP_TRY(precond_learned_init(work.get()));
     }
+    work->relax = M->relax;
     BSP_TRY(precond_learned_refresh(work.get(), ilu, dF.get()));
     for (DevBuf<double>* b : {&lz, &lw, &llam, &ly}) BSP_TRY(ensure(*b, (size_t)N * K));
     BSP_TRY(ensure(lu, (size_t)N));
@@ -937,6 +942,7 @@ template <typename T> struct Model : ModelBase {
 
   int adam(bsp_handle_s* h, double lr, double b1, double b2, double eps) override {
     ++step;
+    dec_zero = false;
     const double c1 = 1.0 - std::pow(b1, (double)step), c2 = 1.0 - std::pow(b2, (double)step);
     bsp::count_launch(), k_adam<T><<<grid_for(h, M->n_params, 256), 256, 0, h->stream>>>(
         M->n_params, p.get(), g.get(), m.get(), v.get(), (T)lr, (T)b1, (T)b2, (T)eps, (T)c1, (T)c2);
@@ -954,12 +960,15 @@ template <typename T> struct Model : ModelBase {
   int set(const double* in, int64_t cnt) override {
     if (cnt != M->n_params) return BSP_INVALID;
     std::vector<T> tmp(in, in + cnt);
+    // the decoders (Wo, bo, Wd, bd) are the last slots
+    dec_zero = std::all_of(tmp.begin() + M->slots[2 + 2 * kLayers].off, tmp.end(), [](T x) { return x == T(0); });
     BSP_CUDA_TRY(cudaMemcpy(p.get(), tmp.data(), cnt * sizeof(T), cudaMemcpyHostToDevice));
     BSP_CUDA_TRY(cudaMemset(m.get(), 0, cnt * sizeof(T)));
     BSP_CUDA_TRY(cudaMemset(v.get(), 0, cnt * sizeof(T)));
     step = 0;
     return BSP_OK;
   }
+  bool decoders_zero() const override { return dec_zero; }
 };
 
 }  // namespace
@@ -1004,6 +1013,18 @@ int bsp_learned_destroy(bsp_learned_t M) {
   if (!M) return BSP_OK;
   cudaSetDevice(M->device);
   delete M;
+  return BSP_OK;
+}
+
+int bsp_learned_set_relax(bsp_learned_t M, double relax) {
+  if (!M || !(relax > -1.0 && relax < 4.0)) return BSP_INVALID;
+  M->relax = relax;
+  return BSP_OK;
+}
+
+int bsp_learned_get_relax(bsp_learned_t M, double* relax) {
+  if (!M || !relax) return BSP_INVALID;
+  *relax = M->relax;
   return BSP_OK;
 }
 
@@ -1127,9 +1148,12 @@ int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int pre
   if (!h || !M || !A || !out || A->bs != M->bs || A->n_rows != A->n_cols) return BSP_INVALID;
   *out = nullptr;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
+  // zero decoders give dF = 0 exactly: the factors are the (relaxed) baseline's
   DevBuf<double> dF;
-  BSP_TRY(dF.alloc((size_t)A->nnzb * A->bs * A->bs));
-  BSP_TRY(M->impl->forward(h, A, dF.get()));
+  if (!M->impl->decoders_zero()) {
+    BSP_TRY(dF.alloc((size_t)A->nnzb * A->bs * A->bs));
+    BSP_TRY(M->impl->forward(h, A, dF.get()));
+  }
   auto pc = std::make_unique<bsp_precond_s>();
   pc->h = h;
   pc->device = h->device;
@@ -1138,6 +1162,7 @@ int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int pre
   pc->n = A->n_rows;
   pc->bs = A->bs;
   pc->precision = precision;
+  pc->relax = M->relax;
   if (precision != BSP_PREC_F64)
     BSP_TRY(bsp_matrix_make_lowp(A, precision == BSP_PREC_F32 ? BSP_F32 : BSP_BF16));
   BSP_TRY(precond_build_learned(pc.get(), dF.get()));

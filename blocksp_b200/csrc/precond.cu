@@ -1515,9 +1515,34 @@ __global__ void k_add_perm(int64_t nblk, int b2, const int64_t* __restrict__ per
     f[e] += dF[perm[e / b2] * b2 + e % b2];
 }
 
+// f_b += relax * f0_b on every off-diagonal block b of the factor (strictly
+// lower blocks of an L L^T factor, both triangles of an LU factor): the
+// relaxation of the learned factors.  One warp per factor row; f0 may be f.
+__global__ void k_relax_offdiag(int n, int b2, const int* __restrict__ f_ptr, const int* __restrict__ f_diag,
+                                double relax, const double* f0, double* f) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < n; i += warps) {
+    const int d = f_diag[i];
+    for (int b = f_ptr[i]; b < f_ptr[i + 1]; ++b)
+      if (b != d)
+        for (int o = lane; o < b2; o += 32) f[(int64_t)b * b2 + o] += relax * f0[(int64_t)b * b2 + o];
+  }
+}
+
+static int relax_offdiag(bsp_precond_s* pc, const double* f0) {
+  if (pc->relax == 0.0 || pc->n == 0) return BSP_OK;
+  const int grid = (int)std::min<int64_t>(((int64_t)pc->n * 32 + 255) / 256, (int64_t)pc->h->num_sms * 16);
+  bsp::count_launch(), k_relax_offdiag<<<grid, 256, 0, pc->h->stream>>>(
+      pc->n, pc->bs * pc->bs, pc->f_ptr.get(), pc->f_diag.get(), pc->relax, f0, pc->f_vals.get());
+  BSP_CUDA_TRY(cudaPeekAtLastError());
+  return BSP_OK;
+}
+
 // Learned factors: the block-ILU0 factors (LU form) or the block-IChol0 factor
-// (L L^T form) plus a correction dF given in A's block order; the diagonal
-// inverses are recomputed from the corrected U_ii / L_ii (general inverses).
+// (L L^T form), off-diagonal blocks scaled by 1 + relax, plus a correction dF
+// given in A's block order (null: none); the diagonal inverses are recomputed
+// from the corrected U_ii / L_ii (general inverses).
 int precond_build_learned(bsp_precond_s* pc, const double* dF) {
   const int n = pc->n, b2 = pc->bs * pc->bs;
   stream_invalidate(pc);
@@ -1530,12 +1555,18 @@ int precond_build_learned(bsp_precond_s* pc, const double* dF) {
   BSP_TRY(build_factor_structure(pc, llt));
   BSP_TRY(run_factor(pc, llt ? FACT_ICHOL0 : FACT_ILU0, pc->order_lo.get(), pc->f_ptr.get(), pc->f_col.get(),
                      pc->f_diag.get(), pc->f_vals.get(), n));
-  const int64_t tot = pc->f_nnzb * b2;
-  if (tot > 0)
-    bsp::count_launch(), k_add_perm<<<grid_for(pc->h, tot, 256), 256, 0, pc->h->stream>>>(
-        pc->f_nnzb, b2, pc->d_perm.get(), dF, pc->f_vals.get());
-  BSP_CUDA_TRY(cudaPeekAtLastError());
-  BSP_TRY(run_factor(pc, FACT_DIAG, nullptr, pc->f_ptr.get(), pc->f_col.get(), pc->f_diag.get(), pc->f_vals.get(), n));
+  BSP_TRY(relax_offdiag(pc, pc->f_vals.get()));
+  // dF null: no correction, so the diagonal blocks and the factorisation's own
+  // inverses of them stand
+  if (dF) {
+    const int64_t tot = pc->f_nnzb * b2;
+    if (tot > 0)
+      bsp::count_launch(), k_add_perm<<<grid_for(pc->h, tot, 256), 256, 0, pc->h->stream>>>(
+          pc->f_nnzb, b2, pc->d_perm.get(), dF, pc->f_vals.get());
+    BSP_CUDA_TRY(cudaPeekAtLastError());
+    BSP_TRY(run_factor(pc, FACT_DIAG, nullptr, pc->f_ptr.get(), pc->f_col.get(), pc->f_diag.get(),
+                       pc->f_vals.get(), n));
+  }
   return make_lowp_copies(pc);
 }
 
@@ -1841,7 +1872,8 @@ int precond_learned_init(bsp_precond_s* pc) {
   return build_factor_structure(pc, pc->kind == BSP_PC_LEARNED_LLT);
 }
 
-// work's factors = ilu's factors + dF (A order); work shares ilu's structure
+// work's factors = ilu's factors + dF (A order) + work->relax * ilu's off-diagonal
+// factor blocks; work shares ilu's structure
 // (both built on the same matrix) and gets fresh diagonal inverses.
 int precond_learned_refresh(bsp_precond_s* work, const bsp_precond_s* ilu, const double* dF) {
   if (work->f_nnzb != ilu->f_nnzb || work->n != ilu->n || work->bs != ilu->bs) return BSP_INVALID;
@@ -1852,6 +1884,7 @@ int precond_learned_refresh(bsp_precond_s* work, const bsp_precond_s* ilu, const
     bsp::count_launch(), k_copy_add_perm<<<grid_for(work->h, tot, 256), 256, 0, work->h->stream>>>(
         work->f_nnzb, b2, work->d_perm.get(), ilu->f_vals.get(), dF, work->f_vals.get());
   BSP_CUDA_TRY(cudaPeekAtLastError());
+  BSP_TRY(relax_offdiag(work, ilu->f_vals.get()));
   return run_factor(work, FACT_DIAG, nullptr, work->f_ptr.get(), work->f_col.get(), work->f_diag.get(),
                     work->f_vals.get(), work->n);
 }

@@ -26,6 +26,9 @@ struct bsp_precond_s {
   bsp_matrix_t A = nullptr;
   int kind = 0, n = 0, bs = 0, precision = 0;
   double w = 1.6;
+  // learned factors: off-diagonal factor blocks scaled by (1 + relax) before the
+  // network's correction is added
+  double relax = 0.0;
   int nu = 3, type = 0;
   // factor storage (ILU0: every block of A; IChol0: A.lowTri()), columns sorted
   bsp::DevBuf<int> f_ptr, f_col, f_diag;
@@ -83,7 +86,8 @@ int precond_check_status(bsp_precond_s* pc);
 // out = M^-T g for an ILU0 / learned-LU preconditioner (FP64); w receives U^-T g.
 int precond_apply_transposed(bsp_precond_s* pc, const double* g, double* w, double* out);
 // learned LU: structure only (no factorisation), then
-// f = ilu's factors + dF (A's block order) with dinv recomputed
+// f = ilu's factors (off-diagonal blocks scaled by 1 + work->relax) + dF
+// (A's block order) with dinv recomputed
 int precond_learned_init(bsp_precond_s* pc);
 int precond_learned_refresh(bsp_precond_s* work, const bsp_precond_s* ilu, const double* dF);
 }  // namespace bsp

@@ -11,6 +11,11 @@ loop, and the preconditioners it builds, in two factor forms:
 * L L^T form (``LearnedLLT``, pCG on SPD systems): corrects the block-IChol0
   factor; falls back to block IChol0 the same way.
 
+Both forms first scale the baseline factors' off-diagonal blocks by 1 + relax,
+a scalar of the model fitted to the training systems' iteration counts (a
+compensation for the fill-in that the incomplete factorisation drops, in the
+spirit of modified ILU), and add the network's correction to that.
+
 No reference counterpart (the reference's preconditioners end at IChol0,
 blocksp_preconditioners.hpp:364-538); the produced factors keep A's sparsity
 and are applied by the same triangular sweeps as ILU0 (ILU0::invmul order).
@@ -90,6 +95,7 @@ class LearnedModel:
         self.n_params = cnt.value
         self.meta = dict(meta or {})
         self.set_params(params if params is not None else init_params(bs))
+        self.set_relax(float(self.meta.get("relax", 0.0)))
 
     # -------------------------------------------------------------- parameters
     def set_params(self, params) -> None:
@@ -98,6 +104,17 @@ class LearnedModel:
         if flat.size != self.n_params:
             raise ValueError(f"expected {self.n_params} parameters, got {flat.size}")
         check(self.handle.lib.bsp_learned_set_params(self.m, _ptr(flat), flat.size), "bsp_learned_set_params")
+
+    def set_relax(self, relax: float) -> None:
+        """Scale the off-diagonal blocks of the baseline factors by 1 + relax
+        before the network's correction is added (0 keeps them as they are)."""
+        check(self.handle.lib.bsp_learned_set_relax(self.m, float(relax)), "bsp_learned_set_relax")
+
+    @property
+    def relax(self) -> float:
+        r = C.c_double()
+        check(self.handle.lib.bsp_learned_get_relax(self.m, C.byref(r)), "bsp_learned_get_relax")
+        return r.value
 
     def params(self) -> dict[str, np.ndarray]:
         flat = np.zeros(self.n_params)
@@ -244,19 +261,70 @@ def training_system(dims, seed: int, form: str = "lu"):
     return systems.convection_diffusion_system(dims, 8, int(seed), speed=0.0 if form == "llt" else 0.5)
 
 
+RELAX_GRID = tuple(round(0.05 * i, 2) for i in range(17))  # 0, 0.05, ..., 0.8
+
+
+def fit_relax(model: LearnedModel, seeds, dims, form: str = "lu", grid=RELAX_GRID, log=print,
+              margin: float = 0.1):
+    """Fit the model's relaxation to systems: the grid value with the fewest
+    total solver iterations to the FP64 true residual 1e-10 (ties: the smaller
+    value).  A value whose factors break down or miss 1e-10 on any system is
+    out, and so is every value within ``margin`` below one that is out: the
+    iteration count falls up to the point where the relaxed factors stop
+    converging, and unseen systems may reach that point a little earlier.
+    Leaves the model at the chosen value; returns it and the table."""
+    h = model.handle
+    table = {float(r): 0 for r in grid}
+    for sd in seeds:
+        sysm = training_system(dims, sd, form)
+        A = Matrix.from_system(sysm, h)
+        row = {}
+        for r in grid:
+            if table[float(r)] is None:
+                continue
+            model.set_relax(r)
+            try:
+                lp = model.precond(A)
+            except _lib.BspError as e:
+                if e.status not in (1, 2, 5):
+                    raise
+                table[float(r)] = None
+                continue
+            it, res = solve_iters(A, sysm.b, lp, form=form)
+            lp.close()
+            row[float(r)] = it
+            table[float(r)] = table[float(r)] + it if res <= 1e-10 else None
+        A.close()
+        log(f"relaxation fit seed {sd}: " + " ".join(f"{r:g}:{it}" for r, it in row.items()))
+    bad = [r for r, t in table.items() if t is None]
+    ok = {r: t for r, t in table.items() if t is not None and not any(r < q <= r + margin + 1e-9 for q in bad)}
+    best = min(ok, key=lambda r: (ok[r], r)) if ok else 0.0
+    model.set_relax(best)
+    return best, table
+
+
 def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, epochs: int = 1,
           n_probes: int = 16, lr: float = 1e-4, handle: Handle | None = None, seed: int = 0,
-          n_smooth: int = 8, smooth_steps: int = 20, log=print, form: str = "lu") -> LearnedModel:
+          n_smooth: int = 8, smooth_steps: int = 20, log=print, form: str = "lu", fit_seeds=(),
+          relax_grid=RELAX_GRID) -> LearnedModel:
     """Train on convection-diffusion systems (LU form; SPD diffusion for the L L^T
-    form) with the GPU kernels; then validate against the baseline (ILU0 /
-    IChol0) on held-out seeds and record whether the model beats its iteration
-    count (the fallback gate)."""
+    form) with the GPU kernels: first fit the relaxation of the baseline
+    factors on ``fit_seeds`` (none: relaxation 0), then train the network with
+    that relaxation in place, and keep the network only if it lowers the
+    iteration count on the fit systems (else its decoders are zeroed); then
+    validate against the baseline (ILU0 / IChol0) on held-out seeds, with the
+    relaxation alone and with the whole model, and record whether the model
+    beats the baseline's iteration count (the fallback gate)."""
     import torch
     from .api import IChol0, ILU0
     h = handle or default_handle()
     base = IChol0 if form == "llt" else ILU0
     model = LearnedModel(h, 8, _lib.BSP_F32, params=init_params(8, seed), form=form)
     t0 = time.time()
+    relax, relax_table = 0.0, {}
+    if len(fit_seeds):
+        relax, relax_table = fit_relax(model, fit_seeds, dims, form, relax_grid, log)
+        log(f"relaxation {relax:g} ({time.time() - t0:.0f}s)")
     history = []
     prev, reverts, lr0 = None, 0, lr
     for ep in range(epochs):
@@ -290,23 +358,54 @@ def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, 
             A.close()
             if si % 20 == 0:
                 log(f"epoch {ep} system {si} loss {history[-1]:.6e} ({time.time() - t0:.0f}s)")
+    # the relaxation alone: zero decoders, so the network adds nothing
+    relax_only = LearnedModel(h, 8, _lib.BSP_F32, params=init_params(8, seed), meta={"relax": relax}, form=form)
+    # keep the network only if it lowers the iteration count on the fit systems
+    # (training data); otherwise zero its decoders (the relaxation alone)
+    network_fit = None
+    if len(fit_seeds) and history:
+        tot = [0, 0]
+        for sd in fit_seeds:
+            sysm = training_system(dims, sd, form)
+            A = Matrix.from_system(sysm, h)
+            for k, mm in enumerate((relax_only, model)):
+                try:
+                    pc = mm.precond(A)
+                    it, res = solve_iters(A, sysm.b, pc, form=form)
+                    pc.close()
+                except _lib.BspError as e:
+                    if e.status not in (1, 2, 5):
+                        raise
+                    it, res = 10**9, np.inf
+                tot[k] += it if res <= 1e-10 else 10**9
+            A.close()
+        network_fit = {"relax_only_iters": tot[0], "with_network_iters": tot[1]}
+        log(f"fit systems: relaxation only {tot[0]} iterations, with the network {tot[1]}")
+        if tot[1] >= tot[0]:
+            model.set_params(init_params(8, seed))
+    network_used = network_fit is not None and network_fit["with_network_iters"] < network_fit["relax_only_iters"]
     val = []
     for s in val_seeds:
         sysm = training_system(dims, s, form)
         A = Matrix.from_system(sysm, h)
         ilu = base(A)
         it0, r0 = solve_iters(A, sysm.b, ilu, form=form)
+        rp = relax_only.precond(A)
+        itr, rr = solve_iters(A, sysm.b, rp, form=form)
         lp = model.precond(A)
         it1, r1 = solve_iters(A, sysm.b, lp, form=form)
-        val.append({"seed": int(s), "ilu0_iters": it0, "learned_iters": it1, "ilu0_res": r0, "learned_res": r1})
-        lp.close()
-        ilu.close()
-        A.close()
-        log(f"validation seed {s}: {base.__name__} {it0} iterations, learned {it1}")
+        val.append({"seed": int(s), "ilu0_iters": it0, "learned_iters": it1, "ilu0_res": r0, "learned_res": r1,
+                    "relax_only_iters": itr, "relax_only_res": rr})
+        for o in (rp, lp, ilu, A):
+            o.close()
+        log(f"validation seed {s}: {base.__name__} {it0} iterations, relaxation only {itr}, learned {it1}")
+    relax_only.close()
     beats = bool(val) and sum(v["learned_iters"] for v in val) < sum(v["ilu0_iters"] for v in val) and \
         all(v["learned_res"] <= 1e-10 for v in val)
     model.meta = {"bs": 8, "hidden": HIDDEN, "layers": LAYERS, "dims": list(dims), "form": form,
-                  "baseline": base.__name__, "beats_baseline": beats,
+                  "baseline": base.__name__, "beats_baseline": beats, "relax": relax,
+                  "relax_fit": {"seeds": [int(s) for s in fit_seeds], "grid_total_iters": relax_table},
+                  "network_used": bool(network_used), "network_fit": network_fit,
                   "train_seeds": [int(s) for s in train_seeds], "val_seeds": [int(s) for s in val_seeds],
                   "steps_per_system": steps_per_system, "epochs": epochs, "n_probes": n_probes, "lr": lr0,
                   "lr_final": lr, "reverted_steps": reverts,
@@ -330,12 +429,14 @@ if __name__ == "__main__":  # pragma: no cover - the training run itself
     ap.add_argument("--smooth", type=int, default=8)
     ap.add_argument("--smooth-steps", type=int, default=20)
     ap.add_argument("--form", default="lu", choices=["lu", "llt"])
+    ap.add_argument("--fit", type=int, default=4, help="systems the relaxation is fitted on")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
     tr = [10_000 + i for i in range(a.train)]
     va = [20_000 + i for i in range(a.val)]
+    fit = [15_000 + i for i in range(a.fit)]
     m = train(tr, va, (a.side,) * 3, a.steps, a.epochs, a.probes, a.lr, n_smooth=a.smooth,
-              smooth_steps=a.smooth_steps, form=a.form)
+              smooth_steps=a.smooth_steps, form=a.form, fit_seeds=fit)
     a.out = a.out or str(WEIGHTS_LLT if a.form == "llt" else WEIGHTS)
     m.save(a.out)
     print(json.dumps({k: v for k, v in m.meta.items() if k != "loss_history"}))

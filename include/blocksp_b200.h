@@ -341,6 +341,13 @@ int bsp_learned_create(bsp_handle_t h, int bs, int dtype, bsp_learned_t* out);
  * ILU0.  No counterpart in the reference. */
 enum bsp_learned_form { BSP_LEARNED_LU = 0, BSP_LEARNED_LLT = 1 };
 int bsp_learned_set_form(bsp_learned_t M, int form);
+/* Relaxation of the learned factors (default 0): the off-diagonal blocks of the
+ * block-ILU0 / block-IChol0 factors are scaled by 1 + relax before the
+ * network's correction is added (a modified-incomplete-factorisation-like
+ * compensation), in bsp_learned_loss_grad and bsp_learned_precond alike.
+ * relax must lie in (-1, 4).  No counterpart in the reference. */
+int bsp_learned_set_relax(bsp_learned_t M, double relax);
+int bsp_learned_get_relax(bsp_learned_t M, double* relax);
 int bsp_learned_destroy(bsp_learned_t M);
 int bsp_learned_param_count(bsp_learned_t M, int64_t* count);
 int bsp_learned_set_params(bsp_learned_t M, const double* params, int64_t count);

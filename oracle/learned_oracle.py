@@ -23,7 +23,9 @@ with c_k = sqrt(s_i s_j) for an upper block (j > i, the scale of U_ij ~ A_ij)
 and c_k = sqrt(s_i / s_j) for a lower block (j < i, the scale of
 L_ij ~ A_ij U_jj^-1).
 The preconditioner is M = L U with L = unit lower + strict-lower blocks and U
-the upper blocks (diagonal included) of F = F_ILU0 + dF (A's pattern).
+the upper blocks (diagonal included) of F = R(F_ILU0) + dF (A's pattern), where
+R scales every off-diagonal block by 1 + relax (a fixed scalar of the model,
+fitted to the training systems' iteration counts; 0 leaves F_ILU0 as it is).
 
 Loss over orthonormal probe vectors q_1..q_K (Arnoldi vectors of the
 ILU0-preconditioned operator, generated by the solver): the distance of the
@@ -269,25 +271,34 @@ def _factor_loss(form: str):
     return loss_and_factor_grad_llt if form == "llt" else loss_and_factor_grad
 
 
+def relaxed(g: Graph, F0: np.ndarray, relax: float) -> np.ndarray:
+    """The baseline factors with every off-diagonal block scaled by 1 + relax
+    (the learned factors' relaxation; F0's upper blocks are zero in the L L^T
+    form).  The learned factors are relaxed(F0) + dF."""
+    F = F0 * (1.0 + relax)
+    F[g.diag_pos] = F0[g.diag_pos]
+    return F
+
+
 def loss_fn(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3,
-            form: str = "lu") -> float:
+            form: str = "lu", relax: float = 0.0) -> float:
     dF, _ = forward(p, g, vals, L, form)
-    return _factor_loss(form)(g, vals, F0 + dF, Q)[0]
+    return _factor_loss(form)(g, vals, relaxed(g, F0, relax) + dF, Q)[0]
 
 
 def loss_and_grads(p: dict, g: Graph, vals: np.ndarray, F0: np.ndarray, Q: np.ndarray, L: int = 3,
-                   form: str = "lu"):
+                   form: str = "lu", relax: float = 0.0):
     dF, cache = forward(p, g, vals, L, form)
-    loss, gF = _factor_loss(form)(g, vals, F0 + dF, Q)
+    loss, gF = _factor_loss(form)(g, vals, relaxed(g, F0, relax) + dF, Q)
     return loss, backward(p, g, cache, gF, L)
 
 
 def finite_difference(p: dict, g: Graph, vals, F0, Q, name: str, idx: tuple, h: float = 1e-6,
-                      L: int = 3, form: str = "lu") -> float:
+                      L: int = 3, form: str = "lu", relax: float = 0.0) -> float:
     """Central difference of the loss in one parameter entry."""
     q = {k: v.copy() for k, v in p.items()}
     q[name][idx] += h
-    lp = loss_fn(q, g, vals, F0, Q, L, form)
+    lp = loss_fn(q, g, vals, F0, Q, L, form, relax)
     q[name][idx] -= 2 * h
-    lm = loss_fn(q, g, vals, F0, Q, L, form)
+    lm = loss_fn(q, g, vals, F0, Q, L, form, relax)
     return (lp - lm) / (2 * h)

@@ -7,7 +7,8 @@
   (the triangular solves of the loss are FP64 in both);
 * probes: orthonormal Arnoldi vectors of the ILU0-preconditioned operator,
   equal to the oracle's Arnoldi process within 1e-9;
-* zero decoders reproduce block ILU0 bit for bit;
+* zero decoders reproduce block ILU0 bit for bit; with a relaxation they give
+  ILU0's factors with the off-diagonal blocks scaled by 1 + relax;
 * training steps lower the loss and the trained factors still solve;
 * LearnedLU falls back to ILU0 when a model has not beaten it.
 """
@@ -52,8 +53,9 @@ def test_forward_matches_oracle(handle, case, dtype, tol):
     m.close()
 
 
+@pytest.mark.parametrize("relax", [0.0, 0.4])
 @pytest.mark.parametrize("dtype,ltol,gtol", [(_lib.BSP_F64, 1e-10, 1e-9), (_lib.BSP_F32, 1e-4, 2e-3)])
-def test_loss_and_gradients_match_oracle(handle, case, torch_cuda, dtype, ltol, gtol):
+def test_loss_and_gradients_match_oracle(handle, case, torch_cuda, dtype, ltol, gtol, relax):
     torch = torch_cuda
     s, A, _, ilu_o, g, p = case
     import blocksp_b200 as bsp
@@ -63,9 +65,10 @@ def test_loss_and_gradients_match_oracle(handle, case, torch_cuda, dtype, ltol, 
     rng = np.random.default_rng(6)
     Qh = np.linalg.qr(rng.standard_normal((s.n * 8, 3)))[0].T.copy()
     Q = torch.tensor(Qh, device="cuda")
-    m = learned.LearnedModel(handle, 8, dtype, params=p)
+    m = learned.LearnedModel(handle, 8, dtype, params=p, meta={"relax": relax})
+    assert m.relax == relax
     loss = m.loss_grad(A, ilu, Q)
-    ref_loss, ref_g = LO.loss_and_grads(p, g, s.vals, F0.cpu().numpy(), Qh)
+    ref_loss, ref_g = LO.loss_and_grads(p, g, s.vals, F0.cpu().numpy(), Qh, relax=relax)
     assert abs(loss - ref_loss) <= ltol * abs(ref_loss)
     gr = m.grads()
     for k in ref_g:
@@ -113,6 +116,32 @@ def test_zero_decoders_reproduce_ilu0(handle, case, torch_cuda):
     lp.close()
     ilu.close()
     m.close()
+
+
+@pytest.mark.parametrize("relax", [0.25, 0.6])
+def test_relaxation_scales_the_off_diagonal_factors(handle, case, torch_cuda, relax):
+    """Zero decoders with a relaxation: the learned factors are ILU0's with
+    every off-diagonal block scaled by 1 + relax (diagonal blocks bit for bit),
+    and the preconditioner applies them like the oracle's ILU0 on those factors."""
+    torch = torch_cuda
+    s, A, Ao, _, g, _ = case
+    import blocksp_b200 as bsp
+    m = learned.LearnedModel(handle, 8, _lib.BSP_F32, meta={"relax": relax})
+    lp = m.precond(A)
+    ilu = bsp.ILU0(A)
+    f1, f0 = lp.export(), ilu.export()
+    rows = np.repeat(np.arange(s.n), np.diff(s.row_ptr))
+    off = s.col_idx != rows
+    assert np.array_equal(f1[~off], f0[~off])
+    assert rel(f1[off], f0[off] * (1 + relax)) <= 1e-15
+    ref = O.ILU0(Ao)
+    ref.LU.vals[:] = LO.relaxed(g, ref.LU.vals, relax)
+    r = np.random.default_rng(7).uniform(-1, 1, s.n * 8)
+    assert rel(lp.apply_host(r), ref(r)) <= 1e-11
+    for o in (lp, ilu, m):
+        o.close()
+    with pytest.raises(_lib.BspError):
+        learned.LearnedModel(handle, 8, _lib.BSP_F32, meta={"relax": -1.0})
 
 
 def test_training_lowers_the_loss(handle, torch_cuda):

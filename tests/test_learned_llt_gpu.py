@@ -46,8 +46,9 @@ def test_llt_forward_matches_oracle(handle, spd_case, dtype, tol):
     m.close()
 
 
+@pytest.mark.parametrize("relax", [0.0, 0.4])
 @pytest.mark.parametrize("dtype,ltol,gtol", [(_lib.BSP_F64, 1e-10, 1e-9), (_lib.BSP_F32, 1e-4, 2e-3)])
-def test_llt_loss_and_gradients_match_oracle(handle, spd_case, torch_cuda, dtype, ltol, gtol):
+def test_llt_loss_and_gradients_match_oracle(handle, spd_case, torch_cuda, dtype, ltol, gtol, relax):
     torch = torch_cuda
     s, A, g, p = spd_case
     import blocksp_b200 as bsp
@@ -56,9 +57,9 @@ def test_llt_loss_and_gradients_match_oracle(handle, spd_case, torch_cuda, dtype
     assert rel(F0, ichol0_in_a_order(s)) <= 1e-13
     rng = np.random.default_rng(16)
     Qh = np.linalg.qr(rng.standard_normal((s.n * 8, 3)))[0].T.copy()
-    m = learned.LearnedModel(handle, 8, dtype, params=p, form="llt")
+    m = learned.LearnedModel(handle, 8, dtype, params=p, form="llt", meta={"relax": relax})
     loss = m.loss_grad(A, ic, torch.tensor(Qh, device="cuda"))
-    ref_loss, ref_g = LO.loss_and_grads(p, g, s.vals, F0, Qh, form="llt")
+    ref_loss, ref_g = LO.loss_and_grads(p, g, s.vals, F0, Qh, form="llt", relax=relax)
     assert abs(loss - ref_loss) <= ltol * abs(ref_loss)
     gr = m.grads()
     for k in ref_g:

@@ -5,6 +5,8 @@ and of the convection-diffusion generator it trains on.
   (relative error <= 1e-5 on sampled entries of every parameter);
 * with zero decoders the network's correction is exactly zero (the initial
   preconditioner is block ILU0) and the loss is ILU0's;
+* the relaxation scales exactly the off-diagonal factor blocks, and the
+  gradients stay exact (finite differences) with it in place;
 * the generator follows its stated conventions (velocity magnitude, harmonic
   edge conductivities, upwind blocks, SPD coupling, unit-variance field).
 """
@@ -140,3 +142,36 @@ def test_llt_form_keeps_the_factor_lower_and_spd():
     # with zero decoders the factor is IChol0's: L L^T = the reference's IC(0)
     dF0, _ = LO.forward(LO.init_params(8, seed=2), g, s.vals, form="llt")
     assert not np.any(dF0)
+
+
+# ---- the relaxation of the baseline factors ----
+
+def test_relaxed_scales_off_diagonal_blocks_only():
+    for s, g, F0 in (small_case(), small_spd_case()):
+        rows = np.repeat(np.arange(s.n), np.diff(s.row_ptr))
+        off = s.col_idx != rows
+        R = LO.relaxed(g, F0, 0.35)
+        assert np.array_equal(R[~off], F0[~off])
+        assert np.array_equal(R[off], F0[off] * 1.35)
+        assert np.array_equal(LO.relaxed(g, F0, 0.0), F0)
+    # the L L^T factor stays lower: its upper blocks are zero before and after
+    s, g, F0 = small_spd_case()
+    rows = np.repeat(np.arange(s.n), np.diff(s.row_ptr))
+    assert not np.any(LO.relaxed(g, F0, 0.5)[s.col_idx > rows])
+
+
+def test_gradients_with_relaxation_match_finite_differences():
+    rng = np.random.default_rng(12)
+    for form, (s, g, F0) in (("lu", small_case()), ("llt", small_spd_case())):
+        p = LO.init_params(8, seed=13)
+        for k in p:
+            p[k] = p[k] + (0.005 if k in ("Wo", "bo", "Wd", "bd") else 0.05) * rng.standard_normal(p[k].shape)
+        Q = np.linalg.qr(rng.standard_normal((s.n * 8, 3)))[0].T
+        _, gr = LO.loss_and_grads(p, g, s.vals, F0, Q, form=form, relax=0.4)
+        worst = 0.0
+        for name in p:
+            idx = tuple(int(rng.integers(0, d)) for d in p[name].shape)
+            fd = LO.finite_difference(p, g, s.vals, F0, Q, name, idx, h=1e-5, form=form, relax=0.4)
+            an = gr[name][idx]
+            worst = max(worst, abs(fd - an) / max(1e-8, abs(fd) + abs(an)))
+        assert worst <= 1e-5, (form, worst)
