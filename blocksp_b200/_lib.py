@@ -81,6 +81,8 @@ SIGNATURES: dict[str, tuple] = {
     "bsp_release_cached_memory": (_I, [_I]),
     "bsp_cached_memory": (_I, [_I, C.POINTER(_I64)]),
     "bsp_matrix_create": (_I, [_P, _I, _I, _I, _I64, _P, _P, _P, C.POINTER(_P)]),
+    "bsp_matrix_create_complex": (_I, [_P, _I, _I, _I, _I64, _P, _P, _P, C.POINTER(_P)]),
+    "bsp_matrix_complex_bs": (_I, [_P, C.POINTER(_I)]),
     "bsp_matrix_create_dev": (_I, [_P, _I, _I, _I, _I64, _P, _P, _P, C.POINTER(_P)]),
     "bsp_matrix_destroy": (_I, [_P]),
     "bsp_matrix_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I64)]),

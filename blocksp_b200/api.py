@@ -102,7 +102,14 @@ def default_handle() -> Handle:
 
 
 class Matrix:
-    """A BSR matrix resident on the GPU (the packed form of BlockSp<T,N>)."""
+    """A BSR matrix resident on the GPU (the packed form of BlockSp<T,N>).
+
+    A complex matrix (``Matrix.from_complex``, T = std::complex<double>) is held
+    as its real embedding: ``bs`` is twice the complex block size
+    ``complex_bs``, and complex vectors (numpy complex128) are passed to the
+    library as their interleaved (re, im) doubles."""
+
+    complex_bs = 0
 
     def __init__(self, row_ptr, col_idx, vals, bs: int, n_cols: int | None = None,
                  handle: Handle | None = None):
@@ -124,7 +131,26 @@ class Matrix:
 
     @classmethod
     def from_system(cls, s, handle: Handle | None = None) -> "Matrix":
+        if np.iscomplexobj(s.vals):
+            return cls.from_complex(s.row_ptr, s.col_idx, s.vals, handle=handle)
         return cls(s.row_ptr, s.col_idx, s.vals, s.bs, handle=handle)
+
+    @classmethod
+    def from_complex(cls, row_ptr, col_idx, vals, n_cols: int | None = None,
+                     handle: Handle | None = None) -> "Matrix":
+        """A complex block matrix: vals complex128 [nnzb, bs, bs] row-major."""
+        handle = handle or default_handle()
+        row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        col_idx = np.ascontiguousarray(col_idx, dtype=np.int32)
+        vals = np.ascontiguousarray(vals, dtype=np.complex128)
+        n = int(row_ptr.shape[0] - 1)
+        cbs = int(vals.shape[1]) if vals.ndim == 3 else 1
+        m = C.c_void_p()
+        check(handle.lib.bsp_matrix_create_complex(handle.h, n, int(n_cols if n_cols is not None else n), cbs,
+                                                   int(col_idx.shape[0]), _ptr(row_ptr), _ptr(col_idx),
+                                                   _ptr(vals), C.byref(m)),
+              "bsp_matrix_create_complex", handle.h)
+        return cls._wrap(m, handle)
 
     @classmethod
     def _wrap(cls, m: C.c_void_p, handle: Handle) -> "Matrix":
@@ -134,6 +160,9 @@ class Matrix:
         n, nc, bs, nnzb = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
         check(handle.lib.bsp_matrix_info(m, C.byref(n), C.byref(nc), C.byref(bs), C.byref(nnzb)), "bsp_matrix_info")
         obj.n_rows, obj.n_cols, obj.bs, obj.nnzb = n.value, nc.value, bs.value, nnzb.value
+        cb = C.c_int()
+        check(handle.lib.bsp_matrix_complex_bs(m, C.byref(cb)), "bsp_matrix_complex_bs")
+        obj.complex_bs = cb.value
         obj.m = m
         handle.adopt(obj)
         return obj
@@ -217,17 +246,26 @@ def bsmv(A: Matrix, x: np.ndarray, b: np.ndarray | None = None, nrhs: int = 1,
     ``bsmv(A, x)`` returns A x (blocksp_multiply.hpp:377-390); with ``b`` given
     it accumulates into b like the void overloads ``bsmv(b, A, x)``.
     """
-    x = np.ascontiguousarray(x, dtype=np.float64)
+    cplx = bool(A.complex_bs)
+    x = _as_real(x, cplx)
     m = (A.n_cols if transpose else A.n_rows) * A.bs * nrhs
     if b is None:
         y = np.zeros(m)
         beta = 0.0
     else:
-        y = b
+        y = b.view(np.float64) if cplx else b
         beta = 1.0
     check(A.handle.lib.bsp_bsmv(A.handle.h, A.m, nrhs, int(transpose), 1.0, _ptr(x), beta, _ptr(y)),
           "bsp_bsmv", A.handle.h)
-    return y
+    return y.view(np.complex128) if cplx else y
+
+
+def _as_real(v, cplx: bool) -> np.ndarray:
+    """A host vector as the doubles the library reads: complex vectors as their
+    interleaved (re, im) doubles."""
+    if cplx:
+        return np.ascontiguousarray(v, dtype=np.complex128).view(np.float64)
+    return np.ascontiguousarray(v, dtype=np.float64)
 
 
 def dot_dev(handle: Handle, x, y) -> float:
@@ -274,10 +312,11 @@ class Precond:
               "bsp_precond_apply_dev", self.handle.h)
 
     def apply_host(self, r: np.ndarray) -> np.ndarray:
-        out = np.array(r, dtype=np.float64, copy=True)
+        cplx = bool(self.A.complex_bs)
+        out = _as_real(r, cplx).copy()
         check(self.handle.lib.bsp_precond_apply(self.handle.h, self.p, _ptr(out)),
               "bsp_precond_apply", self.handle.h)
-        return out
+        return out.view(np.complex128) if cplx else out
 
     def info(self) -> dict:
         kind, lo, up, nnz = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
@@ -357,10 +396,12 @@ def _solve(fn_dev, fn_host, A: Matrix, b, pc, opts: SolveOpts, return_info: bool
         st = getattr(lib, fn_dev)(A.handle.h, A.m, pcp, _ptr(b), _ptr(x), C.byref(opts), _ptr(hist),
                                   cap, C.byref(info))
     else:
-        bb = np.ascontiguousarray(b, dtype=np.float64)
+        bb = _as_real(b, bool(A.complex_bs))
         x = np.zeros_like(bb)
         st = getattr(lib, fn_host)(A.handle.h, A.m, pcp, _ptr(bb), _ptr(x), C.byref(opts), _ptr(hist),
                                    cap, C.byref(info))
+        if A.complex_bs:
+            x = x.view(np.complex128)
     if st not in (_lib.BSP_OK, 4, 3, 5):  # MAXIT / BREAKDOWN / NAN still return x
         check(st, fn_dev, A.handle.h)
     if return_info:

@@ -177,6 +177,8 @@ struct bsp_matrix_s {
   bsp_handle_t h = nullptr;  // creating handle; must outlive every compute call on A
   int device = 0;
   int n_rows = 0, n_cols = 0, bs = 0;
+  // complex matrix held as its real embedding (bs = 2 cbs); 0 for a real one
+  int cbs = 0;
   int64_t nnzb = 0;
   bsp::DevBuf<int> row_ptr, col_idx;
   bsp::DevBuf<double> vals;

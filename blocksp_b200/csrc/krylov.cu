@@ -1255,6 +1255,11 @@ int refine_solve(bool gmres, bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc
 // ================================================================== C ABI
 using namespace bsp;
 
+namespace bsp {
+int pgmres_complex_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, const double* b, double* x,
+                         const bsp_solve_opts* o, double* hist, int hist_cap, bsp_solve_info* info);
+}  // namespace bsp
+
 static int solve_common(bool gmres, bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc,
                         const double* b, double* x, const bsp_solve_opts* opts, double* hist,
                         int hist_cap, bsp_solve_info* info) {
@@ -1262,6 +1267,14 @@ static int solve_common(bool gmres, bsp_handle_t h, bsp_matrix_t A, bsp_precond_
   if (A->n_rows != A->n_cols) return BSP_INVALID;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
   if (info) *info = bsp_solve_info{};
+  if (A->cbs) {
+    // complex T: pGMRES only (no complex pCG in the reference, solvers.hpp:55)
+    if (!gmres) {
+      record_error("pCG is not defined for complex matrices");
+      return BSP_INVALID;
+    }
+    return pgmres_complex_solve(h, A, pc, b, x, opts, hist, hist_cap, info);
+  }
   if (opts->precision != BSP_PREC_F64 || opts->stop_rule == BSP_STOP_TRUE_RESIDUAL)
     return refine_solve(gmres, h, A, pc, b, x, opts, hist, hist_cap, info);
   return gmres ? pgmres_solve(h, A, pc, b, x, opts, hist, hist_cap, info)

@@ -1145,7 +1145,7 @@ int bsp_learned_smooth(bsp_handle_t h, bsp_matrix_t A, bsp_precond_t pc, int K, 
 }
 
 int bsp_learned_precond(bsp_handle_t h, bsp_learned_t M, bsp_matrix_t A, int precision, bsp_precond_t* out) {
-  if (!h || !M || !A || !out || A->bs != M->bs || A->n_rows != A->n_cols) return BSP_INVALID;
+  if (!h || !M || !A || !out || A->bs != M->bs || A->n_rows != A->n_cols || A->cbs) return BSP_INVALID;
   *out = nullptr;
   BSP_CUDA_TRY(cudaSetDevice(h->device));
   // zero decoders give dF = 0 exactly: the factors are the (relaxed) baseline's

@@ -1967,6 +1967,11 @@ int bsp_precond_create(bsp_handle_t h, bsp_matrix_t A, const bsp_precond_params*
     record_error("preconditioners support block sizes up to 32");
     return BSP_INVALID;
   }
+  if (A->cbs && params->kind == BSP_PC_ICHOL0) {
+    // the reference's IChol0 is real only (blocksp_solvers.hpp:485)
+    record_error("IChol0 is not defined for complex matrices");
+    return BSP_INVALID;
+  }
   BSP_CUDA_TRY(cudaSetDevice(h->device));
   auto pc = std::make_unique<bsp_precond_s>();
   pc->h = h;

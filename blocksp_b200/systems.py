@@ -211,6 +211,35 @@ def gaussian_field(rng: np.random.Generator, dims: tuple[int, ...], corr_len: fl
     return w.reshape(-1)
 
 
+def complex_system(dims: tuple[int, ...], bs: int, seed: int, skew: float = 0.3, imag: float = 0.3,
+                   name: str = "") -> BSRSystem:
+    """A complex block system (T = std::complex<double>): the real block stencil
+    system of ``grid_system(dims, bs, seed, skew)`` plus i * imag times a second
+    one of the same pattern (seed + 7919), and the right-hand side
+    b + i * b'.  vals is complex128 [nnzb, bs, bs]; b is complex128 [n * bs]."""
+    re = grid_system(dims, bs, seed, skew=skew)
+    im = grid_system(dims, bs, seed + 7919, skew=skew)
+    vals = re.vals + 1j * imag * im.vals
+    b = re.b + 1j * im.b
+    return BSRSystem(n=re.n, bs=bs, row_ptr=re.row_ptr, col_idx=re.col_idx, vals=vals, b=b,
+                     name=name or f"complex_{len(dims)}d_bs{bs}_s{seed}")
+
+
+def complex_embedding(vals: np.ndarray) -> np.ndarray:
+    """The real 2bs x 2bs blocks of complex bs x bs blocks: complex entry
+    a = ar + i ai at (r, c) becomes [[ar, -ai], [ai, ar]] at rows 2r, 2r+1 and
+    columns 2c, 2c+1, so a complex vector stored as interleaved (re, im)
+    doubles is the real vector the embedded blocks act on."""
+    v = np.asarray(vals, dtype=np.complex128)
+    nb, bs, _ = v.shape
+    out = np.empty((nb, bs, 2, bs, 2))
+    out[:, :, 0, :, 0] = v.real
+    out[:, :, 0, :, 1] = -v.imag
+    out[:, :, 1, :, 0] = v.imag
+    out[:, :, 1, :, 1] = v.real
+    return out.reshape(nb, 2 * bs, 2 * bs)
+
+
 @dataclass
 class ConvDiffSpec:
     """Per-system data of a convection-diffusion block system: cell

@@ -179,6 +179,22 @@ int bsp_matrix_create(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nn
 int bsp_matrix_create_dev(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
                           const int* d_row_ptr, const int* d_col_idx, const double* d_vals,
                           bsp_matrix_t* out);
+/* Complex T = std::complex<double> (BlockSp<std::complex<double>, N>): vals
+ * holds nnzb complex bs x bs row-major blocks as interleaved (re, im) doubles.
+ * The matrix is kept as its real embedding (complex entry ar + i ai ->
+ * [[ar, -ai], [ai, ar]]), so bsp_matrix_info reports block size 2 bs, and a
+ * complex vector (interleaved doubles, the std::complex<double> layout) is a
+ * vector of 2 n bs doubles for every call on it: bsmv computes the complex
+ * product; Diag / SOR / ILU0 preconditioners are the complex ones; pGMRES
+ * (bsp_pgmres, bsp_pgmres_dev) runs in complex arithmetic, FP64 with the
+ * reference's stopping rule.  IChol0, pCG and the learned preconditioner are
+ * real only (BSP_INVALID), as in the reference (blocksp_solvers.hpp:55, 485).
+ * bs <= 16. */
+int bsp_matrix_create_complex(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
+                              const int* row_ptr, const int* col_idx, const double* vals,
+                              bsp_matrix_t* out);
+/* complex block size of a complex matrix, 0 for a real one */
+int bsp_matrix_complex_bs(bsp_matrix_t A, int* complex_bs);
 int bsp_matrix_destroy(bsp_matrix_t A);
 int bsp_matrix_info(bsp_matrix_t A, int* n_rows, int* n_cols, int* bs, int64_t* nnzb);
 /* Device pointers of the packed matrix (row_ptr, col_idx, FP64 vals). */
