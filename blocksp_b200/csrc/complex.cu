@@ -46,7 +46,6 @@ namespace {
 using namespace bsp;
 using Cx = std::complex<double>;
 using namespace bsp::cd;
-constexpr double kEpsC = std::numeric_limits<double>::epsilon();
 
 // ------------------------------------------------------------------ kernels
 // Reduction body: (re, im) of sum conj(x_c) y_c over complex elements c.
