@@ -11,7 +11,9 @@
 // Names, template parameters, constructor defaults and solve() signatures are
 // those of blocksp_solvers.hpp:344-649 (solver structs and ez::), :51-105
 // (pCG), :156-295 (pGMRES), blocksp_preconditioners.hpp:75-538
-// (preconditioners) and blocksp_multiply.hpp:364-404 (bsmv).  T is double.
+// (preconditioners) and blocksp_multiply.hpp:364-404 (bsmv).  T is double, or
+// std::complex<double> for bsmv, Diag / SOR / ILU0 and pGMRES (the reference's
+// complex set: no complex pCG or IChol0, blocksp_solvers.hpp:55, 411, 485).
 // The matrix is uploaded once, when a preconditioner or solver struct is
 // constructed (the reference's structs build their preconditioner in the
 // constructor too); solve() uploads b and returns x by value.  Errors that the
@@ -22,7 +24,9 @@
 #pragma once
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <memory>
+#include <type_traits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -30,6 +34,14 @@
 #include "blocksp_b200.h"
 
 namespace blocksp_b200 {
+
+// ScalarType_t of the reference (blocksp_utility.hpp): the real type under T.
+template <typename T> struct scalar_of { using type = T; };
+template <typename U> struct scalar_of<std::complex<U>> { using type = U; };
+template <typename T> using Scalar = typename scalar_of<T>::type;
+template <typename T> constexpr bool is_cplx = !std::is_same_v<T, Scalar<T>>;
+// doubles per element of T in the library's vectors (complex: re, im)
+template <typename T> constexpr int kWords = is_cplx<T> ? 2 : 1;
 
 struct error : std::runtime_error {
   int status;
@@ -66,6 +78,8 @@ class DeviceMatrix {
  public:
   template <class BlockSpT>
   DeviceMatrix(const BlockSpT& A, int N, std::shared_ptr<Handle> h = Handle::shared()) : h_(std::move(h)) {
+    using V = std::remove_cv_t<std::remove_pointer_t<decltype(A.get_data(0)[0].data())>>;
+    constexpr int W = kWords<V>;
     std::vector<int> row_ptr{0}, col_idx;
     std::vector<double> vals;
     for (int i = 0; i < A.m(); ++i) {
@@ -73,14 +87,20 @@ class DeviceMatrix {
       const auto& cols = A.get_colIndex(i);
       for (size_t t = 0; t < blocks.size(); ++t) {
         col_idx.push_back(cols[t]);
-        const double* p = blocks[t].data();  // row-major TinyMatrix<T,N,N>
-        vals.insert(vals.end(), p, p + N * N);
+        // row-major TinyMatrix<T,N,N>; complex as interleaved (re, im)
+        const double* p = reinterpret_cast<const double*>(blocks[t].data());
+        vals.insert(vals.end(), p, p + W * N * N);
       }
       row_ptr.push_back((int)col_idx.size());
     }
-    check(bsp_matrix_create(h_->get(), A.m(), A.n(), N, (int64_t)col_idx.size(), row_ptr.data(),
-                            col_idx.data(), vals.data(), &m_),
-          "bsp_matrix_create", h_->get());
+    if constexpr (W == 2)
+      check(bsp_matrix_create_complex(h_->get(), A.m(), A.n(), N, (int64_t)col_idx.size(), row_ptr.data(),
+                                      col_idx.data(), vals.data(), &m_),
+            "bsp_matrix_create_complex", h_->get());
+    else
+      check(bsp_matrix_create(h_->get(), A.m(), A.n(), N, (int64_t)col_idx.size(), row_ptr.data(),
+                              col_idx.data(), vals.data(), &m_),
+            "bsp_matrix_create", h_->get());
   }
   ~DeviceMatrix() { bsp_matrix_destroy(m_); }
   DeviceMatrix(const DeviceMatrix&) = delete;
@@ -97,17 +117,29 @@ class DeviceMatrix {
 // element access x(i, d)(b), since the container's data() is not usable
 // through a non-const reference).
 template <typename T, int B, int D> std::vector<double> flat(const BlockSp::solArray<T, B, D>& x) {
-  std::vector<double> v((size_t)x.len() * B * D);
+  std::vector<double> v((size_t)x.len() * B * D * kWords<T>);
   for (int i = 0; i < x.len(); ++i)
     for (int d = 0; d < D; ++d)
-      for (int b = 0; b < B; ++b) v[((size_t)i * D + d) * B + b] = x(i, d)(b);
+      for (int b = 0; b < B; ++b) {
+        const size_t e = ((size_t)i * D + d) * B + b;
+        if constexpr (is_cplx<T>) {
+          v[2 * e] = std::real(x(i, d)(b));
+          v[2 * e + 1] = std::imag(x(i, d)(b));
+        } else {
+          v[e] = x(i, d)(b);
+        }
+      }
   return v;
 }
 template <typename T, int B, int D> BlockSp::solArray<T, B, D> unflat(const std::vector<double>& v, int n) {
   BlockSp::solArray<T, B, D> x(n);
   for (int i = 0; i < n; ++i)
     for (int d = 0; d < D; ++d)
-      for (int b = 0; b < B; ++b) x(i, d)(b) = v[((size_t)i * D + d) * B + b];
+      for (int b = 0; b < B; ++b) {
+        const size_t e = ((size_t)i * D + d) * B + b;
+        if constexpr (is_cplx<T>) x(i, d)(b) = T(v[2 * e], v[2 * e + 1]);
+        else x(i, d)(b) = v[e];
+      }
   return x;
 }
 
@@ -118,7 +150,7 @@ template <typename T, int B, int D>
 BlockSp::solArray<T, B, D> bsmv(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& x) {
   DeviceMatrix M(A, B * D);
   const std::vector<double> xv = flat(x);
-  std::vector<double> yv((size_t)A.m() * B * D);
+  std::vector<double> yv((size_t)A.m() * B * D * kWords<T>);
   check(bsp_bsmv(M.handle(), M.get(), 1, 0, 1.0, xv.data(), 0.0, yv.data()), "bsp_bsmv", M.handle());
   return unflat<T, B, D>(yv, A.m());
 }
@@ -179,10 +211,11 @@ template <typename T, int B, int D = 1> struct SORChol : DevicePrecond<T, B, D> 
 // pCG<T,B,D>(A, b, tol, preCond, maxIters, printIters) (solvers.hpp:51-105);
 // the preconditioner carries the device copy of A.
 template <typename T, int B, int D>
-BlockSp::solArray<T, B, D> pCG(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& b, T tol,
+BlockSp::solArray<T, B, D> pCG(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& b, Scalar<T> tol,
                                const DevicePrecond<T, B, D>& preCond, int maxIters = 1000, bool printIters = false,
                                bsp_solve_info* info = nullptr) {
   (void)A;
+  static_assert(!is_cplx<T>, "pCG is defined for real T only (blocksp_solvers.hpp:55)");
   const std::vector<double> bv = flat(b);
   std::vector<double> xv(bv.size());
   bsp_solve_opts o{tol, maxIters, -1, -1, printIters ? 1 : 0, BSP_STOP_REFERENCE, BSP_PREC_F64, 1e-6, 50};
@@ -196,7 +229,7 @@ BlockSp::solArray<T, B, D> pCG(const BlockSp::BlockSp<T, B * D>& A, const BlockS
 // pGMRES<T,B,D>(A, b, tol, preCond, maxIters, restart, k, printIters,
 // printEigInfo) (solvers.hpp:156-295).
 template <typename T, int B, int D>
-BlockSp::solArray<T, B, D> pGMRES(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& b, T tol,
+BlockSp::solArray<T, B, D> pGMRES(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& b, Scalar<T> tol,
                                   const DevicePrecond<T, B, D>& preCond, int maxIters = 500, int restart = -1,
                                   int k = -1, bool printIters = false, bool printEigInfo = false,
                                   bsp_solve_info* info = nullptr) {
@@ -216,10 +249,10 @@ BlockSp::solArray<T, B, D> pGMRES(const BlockSp::BlockSp<T, B * D>& A, const Blo
 template <typename T, int B, int D = 1>
 struct ILU0_pGMRES {
   preConditioners::ILU0<T, B, D> ILU0_pre;
-  T tol;
+  Scalar<T> tol;
   int maxIters, restart, k;
   bool printIters, printEigInfo;
-  ILU0_pGMRES(const BlockSp::BlockSp<T, B * D>& A, T tol = 1.0e-8, int maxIters = 5000, int restart = -1, int k = -1,
+  ILU0_pGMRES(const BlockSp::BlockSp<T, B * D>& A, Scalar<T> tol = 1.0e-8, int maxIters = 5000, int restart = -1, int k = -1,
               bool printIters = false, bool printEigInfo = false)
       : ILU0_pre(A), tol(tol), maxIters(maxIters), restart(restart), k(k), printIters(printIters),
         printEigInfo(printEigInfo) {}
@@ -231,10 +264,10 @@ struct ILU0_pGMRES {
 template <typename T, int B, int D = 1>
 struct IChol0_pCG {
   preConditioners::IChol0<T, B, D> IChol0_pre;
-  T tol;
+  Scalar<T> tol;
   int maxIters;
   bool printIters;
-  IChol0_pCG(const BlockSp::BlockSp<T, B * D>& A, T tol = 1.0e-8, int maxIters = 5000, bool printIters = false)
+  IChol0_pCG(const BlockSp::BlockSp<T, B * D>& A, Scalar<T> tol = 1.0e-8, int maxIters = 5000, bool printIters = false)
       : IChol0_pre(A), tol(tol), maxIters(maxIters), printIters(printIters) {}
   BlockSp::solArray<T, B, D> solve(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& b) const {
     return pCG<T, B, D>(A, b, tol, IChol0_pre, maxIters, printIters);
@@ -244,10 +277,10 @@ struct IChol0_pCG {
 template <typename T, int B, int D = 1>
 struct SOR_pGMRES {
   preConditioners::SORLU<T, B, D> SOR_pre;
-  T tol;
+  Scalar<T> tol;
   int maxIters, restart, k;
   bool printIters, printEigInfo;
-  SOR_pGMRES(const BlockSp::BlockSp<T, B * D>& A, T w = 1.6, int nu = 3, int SORtype = 0, T tol = 1.0e-8,
+  SOR_pGMRES(const BlockSp::BlockSp<T, B * D>& A, Scalar<T> w = 1.6, int nu = 3, int SORtype = 0, Scalar<T> tol = 1.0e-8,
              int maxIters = 5000, int restart = -1, int k = -1, bool printIters = false, bool printEigInfo = false)
       : SOR_pre(A, w, nu, SORtype), tol(tol), maxIters(maxIters), restart(restart), k(k), printIters(printIters),
         printEigInfo(printEigInfo) {}
@@ -259,10 +292,10 @@ struct SOR_pGMRES {
 template <typename T, int B, int D = 1>
 struct SOR_pCG {
   preConditioners::SORChol<T, B, D> SOR_pre;
-  T tol;
+  Scalar<T> tol;
   int maxIters;
   bool printIters;
-  SOR_pCG(const BlockSp::BlockSp<T, B * D>& A, T w = 1.6, int nu = 3, T tol = 1.0e-8, int maxIters = 5000,
+  SOR_pCG(const BlockSp::BlockSp<T, B * D>& A, Scalar<T> w = 1.6, int nu = 3, Scalar<T> tol = 1.0e-8, int maxIters = 5000,
           bool printIters = false)
       : SOR_pre(A, w, nu, 0), tol(tol), maxIters(maxIters), printIters(printIters) {}
   BlockSp::solArray<T, B, D> solve(const BlockSp::BlockSp<T, B * D>& A, const BlockSp::solArray<T, B, D>& b) const {

@@ -5,9 +5,11 @@
 // headers); run by tests/test_dropin_gpu.py.
 //
 // usage: dropin_test <system.bsps> B D
+//        dropin_test <system.bspc> B 1     (T = std::complex<double>)
 // output: "CHECK <solver> <rel max-norm x difference> <ref iters> <gpu iters>"
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -158,6 +160,86 @@ int run(const Sys& s) {
   return 0;
 }
 
+// ---- T = std::complex<double>: a "BSPC" file (values as (re, im) doubles)
+struct CSys {
+  int n = 0, bs = 0;
+  long long nnzb = 0;
+  std::vector<int> row_ptr, col_idx;
+  std::vector<std::complex<double>> vals, b;
+};
+
+CSys read_csys(const char* path) {
+  CSys s;
+  std::ifstream f(path, std::ios::binary);
+  char magic[4];
+  int ver = 0, nrhs = 1;
+  f.read(magic, 4);
+  f.read((char*)&ver, 4);
+  f.read((char*)&s.n, 4);
+  f.read((char*)&s.bs, 4);
+  f.read((char*)&s.nnzb, 8);
+  f.read((char*)&nrhs, 4);
+  s.row_ptr.resize(s.n + 1);
+  s.col_idx.resize(s.nnzb);
+  s.vals.resize((size_t)s.nnzb * s.bs * s.bs);
+  s.b.resize((size_t)s.n * s.bs);
+  f.read((char*)s.row_ptr.data(), 4 * (s.n + 1));
+  f.read((char*)s.col_idx.data(), 4 * s.nnzb);
+  f.read((char*)s.vals.data(), 16 * s.vals.size());
+  f.read((char*)s.b.data(), 16 * s.b.size());
+  return s;
+}
+
+template <int B>
+double crel_diff(const BlockSp::solArray<std::complex<double>, B, 1>& x,
+                 const BlockSp::solArray<std::complex<double>, B, 1>& y) {
+  double num = 0.0, den = 0.0;
+  for (int i = 0; i < x.len(); ++i)
+    for (int b = 0; b < B; ++b) {
+      num = std::fmax(num, std::abs(x(i, 0)(b) - y(i, 0)(b)));
+      den = std::fmax(den, std::abs(y(i, 0)(b)));
+    }
+  return num / den;
+}
+
+template <int B>
+int run_complex(const CSys& s) {
+  using C = std::complex<double>;
+  BlockSp::BlockSp<C, B> A(s.n);
+  for (int i = 0; i < s.n; ++i)
+    for (int t = s.row_ptr[i]; t < s.row_ptr[i + 1]; ++t) {
+      blitz::TinyMatrix<C, B, B> m;
+      for (int e = 0; e < B * B; ++e) m.data()[e] = s.vals[(size_t)t * B * B + e];
+      A(i, s.col_idx[t]) = m;
+    }
+  BlockSp::solArray<C, B, 1> b(s.n);
+  for (int i = 0; i < s.n; ++i)
+    for (int k = 0; k < B; ++k) b(i, 0)(k) = s.b[(size_t)i * B + k];
+  {
+    auto y_ref = BlockSp::bsmv(A, b);
+    auto y_gpu = blocksp_b200::bsmv<C, B, 1>(A, b);
+    std::printf("CHECK c_bsmv %.3e 0 0\n", crel_diff(y_gpu, y_ref));
+  }
+  const double tol = 1e-10;
+  {
+    BlockSp::solArray<C, B, 1> xr, xg;
+    const std::string ro = capture([&] { xr = BlockSp::ILU0_pGMRES<C, B, 1>(A, tol, 5000, 30, 10, true).solve(A, b); });
+    const std::string go = capture([&] {
+      xg = blocksp_b200::ILU0_pGMRES<C, B, 1>(A, tol, 5000, 30, 10, true).solve(A, b);
+    });
+    std::printf("CHECK c_ilu0_pgmres_dr %.3e %d %d\n", crel_diff(xg, xr), iters_of(ro), iters_of(go));
+  }
+  {
+    BlockSp::solArray<C, B, 1> xr, xg;
+    const std::string ro = capture([&] { xr = BlockSp::SOR_pGMRES<C, B, 1>(A, 1.2, 2, 0, tol, 5000, -1, -1, true).solve(A, b); });
+    const std::string go = capture([&] {
+      xg = blocksp_b200::SOR_pGMRES<C, B, 1>(A, 1.2, 2, 0, tol, 5000, -1, -1, true).solve(A, b);
+    });
+    std::printf("CHECK c_sor_pgmres %.3e %d %d\n", crel_diff(xg, xr), iters_of(ro), iters_of(go));
+  }
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -165,8 +247,25 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "usage: dropin_test <system.bsps> B D\n");
     return 2;
   }
-  const Sys s = read_sys(argv[1]);
   const int B = std::atoi(argv[2]), D = std::atoi(argv[3]);
+  {
+    char magic[4] = {0, 0, 0, 0};
+    std::ifstream f(argv[1], std::ios::binary);
+    f.read(magic, 4);
+    if (std::memcmp(magic, "BSPC", 4) == 0) {
+      const CSys cs = read_csys(argv[1]);
+      try {
+        if (B == 2 && D == 1) return run_complex<2>(cs);
+        if (B == 4 && D == 1) return run_complex<4>(cs);
+      } catch (const blocksp_b200::error& e) {
+        std::printf("ERROR %d %s\n", e.status, e.what());
+        return 1;
+      }
+      std::fprintf(stderr, "unsupported complex B\n");
+      return 2;
+    }
+  }
+  const Sys s = read_sys(argv[1]);
   try {
     if (B == 2 && D == 2) return run<2, 2>(s);
     if (B == 4 && D == 2) return run<4, 2>(s);

@@ -6,15 +6,22 @@ BlockSp::<solver> (the reference, CPU) and blocksp_b200::<solver> (this
 library, GPU) — the same names, template arguments and call shapes — and
 prints how far apart the answers are.  Criteria: bsmv <= 1e-14 relative;
 solutions within 1e-8 relative; iteration counts within +-2 (the reference's
-own printed counts, "pGMRES iters N" / "pCG iters N").
+own printed counts, "pGMRES iters N" / "pCG iters N").  A complex system
+(T = std::complex<double>) runs bsmv, ILU0_pGMRES(30, 10) and SOR_pGMRES with
+the same criteria.
 """
 import os
 import subprocess
+import sys
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from blocksp_b200 import systems
+
+sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+from make_golden_complex import write_complex_system  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
@@ -22,8 +29,12 @@ EXE = ROOT / "oracle" / "_ref" / "dropin_test"
 
 
 def run(tmp_path, s, B, D, spd):
-    f = tmp_path / "sys.bsps"
-    systems.write_bsr(f, s)
+    if np.iscomplexobj(s.vals):
+        f = tmp_path / "sys.bspc"
+        write_complex_system(f, s)
+    else:
+        f = tmp_path / "sys.bsps"
+        systems.write_bsr(f, s)
     env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
     if spd:
         env["DROPIN_SPD"] = "1"
@@ -64,5 +75,14 @@ def test_dropin_nonsymmetric_3d(tmp_path):
     assert out["bsmv"][0] <= 1e-14
     check_algebra(out)
     for name in ("ilu0_pgmres_dr", "sor_pgmres"):
+        d, ir, ig = out[name]
+        assert d <= 1e-8 and abs(ir - ig) <= 2, (name, out[name])
+
+
+@pytest.mark.parametrize("dims,B", [((6, 6, 6), 4), ((10, 10), 2)])
+def test_dropin_complex(tmp_path, dims, B):
+    out = run(tmp_path, systems.complex_system(dims, B, 63 + B), B, 1, False)
+    assert out["c_bsmv"][0] <= 1e-14
+    for name in ("c_ilu0_pgmres_dr", "c_sor_pgmres"):
         d, ir, ig = out[name]
         assert d <= 1e-8 and abs(ir - ig) <= 2, (name, out[name])
