@@ -794,6 +794,75 @@ def llt_summary(args) -> dict:
                               "side", "gate_open", "relax", "network_used", "summary", "gpu_launches")}
 
 
+def run_complex(args):
+    """The complex solve path (T = std::complex<double>): 3D side^3 7-point
+    complex 4x4 block system (the real embedding is 8x8), block ILU0 +
+    pGMRES(30, k=10) with the reference's stopping rule 1e-10, host vectors in
+    and out; per step the ILU0 set-up and the solve.  The reference's own
+    complex build (oracle/_ref/ref_complex_hist, single-threaded) times one
+    full solve of the same system on the host."""
+    import torch
+    import blocksp_b200 as bsp
+    from blocksp_b200 import _lib, systems
+    side = args.complex_side
+    s = systems.complex_system((side,) * 3, 4, 5)
+    stream = torch.cuda.Stream()
+    h = bsp.Handle(0, stream=stream.cuda_stream)
+    lib = _lib.load()
+    A = bsp.Matrix.from_system(s, h)
+
+    def one():
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        pc = bsp.ILU0(A)
+        e[1].record(stream)
+        x, info, hist = bsp.pGMRES(A, s.b, TOL, pc, 5000, 30, 10, return_info=True)
+        e[2].record(stream)
+        e[2].synchronize()
+        pc.close()
+        return x, info, hist, e[0].elapsed_time(e[1]) / 1e3, e[1].elapsed_time(e[2]) / 1e3
+    with ClockSampler(0) as clk:
+        for _ in range(max(args.warmup, 3)):
+            one()
+        l0 = lib.bsp_launch_count()
+        runs = [one() for _ in range(args.steps)]
+        launches = lib.bsp_launch_count() - l0
+    x, info, hist, _, _ = runs[-1]
+    setup = float(np.mean([r[3] for r in runs]))
+    solve = float(np.mean([r[4] for r in runs]))
+    cpu = None
+    ref_iters = None
+    exe = ROOT / "oracle" / "_ref" / "ref_complex_hist"
+    if exe.exists() and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as td:
+            f = Path(td) / "c.bspc"
+            systems.write_complex_bsr(f, s)
+            t0 = time.perf_counter()
+            out = subprocess.run([str(exe), str(f), "--B", "4", "--solver", "ilu0_pgmres", "--restart", "30",
+                                  "--k", "10", "--tol", repr(TOL)], capture_output=True, text=True,
+                                 env=dict(os.environ, OPENBLAS_NUM_THREADS="1"), timeout=1800).stdout
+            wall = time.perf_counter() - t0
+        t = {ln.split()[1]: float(ln.split()[2]) for ln in out.splitlines() if ln.startswith("TIME ")}
+        ref_iters = next((int(ln.split()[2]) for ln in out.splitlines() if ln.startswith("pGMRES iters")), None)
+        cpu = {"value": t.get("setup_s", 0.0) + t.get("solve_s", 0.0), "unit": "s", "cores": 1, "kind": "reference",
+               "sample": f"one full reference ILU0_pGMRES<std::complex<double>,4,1>(A, 1e-10, 5000, 30, 10) solve of "
+                         f"the same system ({ref_iters} iterations): set-up {t.get('setup_s', 0):.2f} s + solve "
+                         f"{t.get('solve_s', 0):.2f} s, timed inside the reference build (process wall {wall:.1f} s)"}
+    line = {"metric": "complex ILU0-pGMRES(30, k=10): time to relative preconditioned residual 1e-10",
+            "value": setup + solve, "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "dtype": "complex f64", "vs_baseline": None,
+            "data": f"synthetic (seeded {side}^3 7-point complex block stencil)",
+            "config": {"workload": f"complex T: 3D {side}^3, 4x4 complex blocks (8x8 real embedding), ILU0 + "
+                                   "pGMRES(30, k=10), reference stopping rule", "n_block_rows": s.n,
+                       "nnzb": int(s.row_ptr[-1])},
+            "setup_s": setup, "solve_s": solve, "iters": info["iters"], "reference_iters": ref_iters,
+            "restarts": info["n_restarts"], "true_rel_res": info["true_rel_res"],
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu}
+    A.close()
+    h.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_apply(args):
     """The ILU0 application alone (forward + backward streamed sweeps) on the
     64^3 8x8 system, `steps` times after `warmup`: the kernel the solve's
@@ -851,11 +920,12 @@ def main():
     ap.add_argument("--no-llt", action="store_true",
                     help="leave the learned L L^T vs IChol0 summary out of the default line")
     ap.add_argument("--workload", default="cfg1",
-                    choices=["cfg1", "batch", "mixed", "learned", "learned_llt", "apply"],
+                    choices=["cfg1", "batch", "mixed", "learned", "learned_llt", "complex", "apply"],
                     help="cfg1: the headline line; batch: 256-system batched pCG; mixed: cfg2 precision "
                          "variants; learned: cfg4 ablation; learned_llt: learned L L^T vs IChol0 with pCG; "
                          "apply: the ILU0 application alone (profiling)")
     ap.add_argument("--llt-side", type=int, default=64)
+    ap.add_argument("--complex-side", type=int, default=48)
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--learned-side", type=int, default=96)
     ap.add_argument("--learned-seeds", type=int, default=2)
@@ -868,7 +938,7 @@ def main():
                               "reference inside its own line"}))
             return
         {"batch": run_batch, "mixed": run_mixed, "learned": run_learned, "learned_llt": run_learned_llt,
-         "apply": run_apply}[args.workload](args)
+         "complex": run_complex, "apply": run_apply}[args.workload](args)
         return
     world, rank, local = dist_setup(args.dist_backend)
     workload = (f"pGMRES(30, deflated restart k=10) + block ILU0 to FP64 true relative residual "

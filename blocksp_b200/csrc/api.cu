@@ -342,9 +342,11 @@ int bsp_handle_sync(bsp_handle_t h) {
 
 void* bsp_handle_stream(bsp_handle_t h) { return h ? (void*)h->stream : nullptr; }
 
+// pre_vals: the value buffer, already allocated (and being filled) by the
+// caller; null: allocate it here.
 static int matrix_create_common(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nnzb,
                                 const int* row_ptr, const int* col_idx, bsp_matrix_t* out,
-                                std::unique_ptr<bsp_matrix_s>& A) {
+                                std::unique_ptr<bsp_matrix_s>& A, DevBuf<double>* pre_vals = nullptr) {
   BSP_TRY(validate_structure(n_rows, n_cols, bs, nnzb, row_ptr, col_idx));
   A = std::make_unique<bsp_matrix_s>();
   A->h = h;
@@ -358,7 +360,8 @@ static int matrix_create_common(bsp_handle_t h, int n_rows, int n_cols, int bs, 
   A->sym = symbolic_for_pattern(h->device, n_rows, n_cols, bs, nnzb, row_ptr, col_idx);
   BSP_TRY(A->row_ptr.alloc(n_rows + 1));
   BSP_TRY(A->col_idx.alloc(nnzb > 0 ? nnzb : 1));
-  BSP_TRY(A->vals.alloc(nnzb > 0 ? (size_t)nnzb * bs * bs : 1));
+  if (pre_vals) A->vals = std::move(*pre_vals);
+  else BSP_TRY(A->vals.alloc(nnzb > 0 ? (size_t)nnzb * bs * bs : 1));
   BSP_CUDA_TRY(cudaMemcpy(A->row_ptr.get(), row_ptr, (n_rows + 1) * sizeof(int), cudaMemcpyHostToDevice));
   if (nnzb > 0)
     BSP_CUDA_TRY(cudaMemcpy(A->col_idx.get(), col_idx, nnzb * sizeof(int), cudaMemcpyHostToDevice));
@@ -372,12 +375,25 @@ int bsp_matrix_create(bsp_handle_t h, int n_rows, int n_cols, int bs, int64_t nn
   if (!h || !out) return BSP_INVALID;
   *out = nullptr;
   DeviceGuard g(h->device);
+  if (n_rows < 0 || bs < 1 || bs > 64 || nnzb < 0 || nnzb > INT32_MAX || (nnzb > 0 && !vals)) {
+    record_error("matrix: bad sizes or null values");
+    return BSP_INVALID;
+  }
+  // The values travel (asynchronously from pinned memory) while the host
+  // validates and registers the structure.
+  DevBuf<double> dv;
+  BSP_TRY(dv.alloc(nnzb > 0 ? (size_t)nnzb * bs * bs : 1));
+  if (nnzb > 0)
+    BSP_CUDA_TRY(cudaMemcpyAsync(dv.get(), vals, (size_t)nnzb * bs * bs * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
   std::unique_ptr<bsp_matrix_s> A;
-  BSP_TRY(matrix_create_common(h, n_rows, n_cols, bs, nnzb, row_ptr, col_idx, out, A));
-  if (nnzb > 0) {
-    if (!vals) return BSP_INVALID;
-    BSP_CUDA_TRY(cudaMemcpy(A->vals.get(), vals, (size_t)nnzb * bs * bs * sizeof(double),
-                            cudaMemcpyHostToDevice));
+  const int st = matrix_create_common(h, n_rows, n_cols, bs, nnzb, row_ptr, col_idx, out, A, &dv);
+  // the copy ends before any buffer is released or handed out
+  const cudaError_t se = cudaStreamSynchronize(h->stream);
+  if (st != BSP_OK) return st;
+  if (se != cudaSuccess) {
+    record_error(std::string("matrix upload: ") + cudaGetErrorString(se));
+    return BSP_CUDA_ERROR;
   }
   *out = A.release();
   return BSP_OK;

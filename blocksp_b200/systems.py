@@ -13,6 +13,8 @@ identically to the CPU oracle, to the reference build and to the GPU:
 * ``batch_specs(seed, count)`` — the uneven-size batch of 2D systems.
 * ``convection_diffusion_system(...)`` — the 3D convection-diffusion family
   used to train and evaluate the learned preconditioner.
+* ``complex_system(dims, bs, seed)`` — a complex (std::complex<double>) block
+  system: a grid system plus i times a second one of the same pattern.
 
 Randomness: one Philox4x64-10 stream per system, keyed by the seed
 (``numpy.random.Philox(key=seed)``, counter from 0), read as uniform doubles
@@ -383,6 +385,18 @@ def write_bsr(path: str | Path, s: BSRSystem) -> None:
         f.write(np.ascontiguousarray(s.col_idx, dtype="<i4").tobytes())
         f.write(np.ascontiguousarray(s.vals, dtype="<f8").tobytes())
         f.write(np.ascontiguousarray(s.b, dtype="<f8").tobytes())
+
+
+def write_complex_bsr(path: str | Path, s: BSRSystem) -> None:
+    """The exchange format with magic BSPC: blocks and right-hand side as
+    complex (re, im) doubles."""
+    with open(path, "wb") as f:
+        f.write(b"BSPC")
+        f.write(struct.pack("<iiiqi", 1, s.n, s.bs, int(s.row_ptr[-1]), 1))
+        f.write(np.ascontiguousarray(s.row_ptr, dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(s.col_idx, dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(s.vals, dtype="<c16").tobytes())
+        f.write(np.ascontiguousarray(s.b, dtype="<c16").tobytes())
 
 
 def read_bsr(path: str | Path) -> BSRSystem:

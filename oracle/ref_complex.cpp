@@ -11,8 +11,10 @@
 //   options: --tol t --maxit m --restart r --k k --w w --nu nu --sortype t --x out.vec
 // The system file is the real exchange format with magic "BSPC": every value
 // (blocks, right-hand side) is a complex number stored as (re, im) doubles.
-// Output lines: "RES0 ..", "RES it res" (history build), "ITERS n"; --x writes
+// Output lines: "RES0 ..", "RES it res" (history build), "pGMRES iters n",
+// "TIME setup_s v" / "TIME solve_s v" (ilu0_pgmres); --x writes
 // the result vector as interleaved (re, im) doubles.
+#include <chrono>
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -137,9 +139,15 @@ int run(const Sys& s, const Opts& o) {
     x = b;
     pre(x);
   } else if (sv == "ilu0_pgmres") {
+    auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    const double t0 = now();
     ILU0_pGMRES<C, N, 1> solver(A, o.tol, o.maxit, o.restart, o.k, true);
+    const double t1 = now();
     print_res0(b, solver.access_ILU0_pre());
+    const double t2 = now();
     x = solver.solve(A, b);
+    const double t3 = now();
+    std::cout << "TIME setup_s " << (t1 - t0) << "\nTIME solve_s " << (t3 - t2) << "\n";
   } else if (sv == "sor_pgmres") {
     SOR_pGMRES<C, N, 1> solver(A, o.w, o.nu, o.sortype, o.tol, o.maxit, o.restart, o.k, true);
     print_res0(b, solver.access_SOR_pre());

@@ -49,17 +49,6 @@ CASES = {
 }
 
 
-def write_complex_system(path: Path, s) -> None:
-    """The exchange format with magic BSPC: values as (re, im) doubles."""
-    with open(path, "wb") as f:
-        f.write(b"BSPC")
-        f.write(struct.pack("<iiiqi", 1, s.n, s.bs, int(s.row_ptr[-1]), 1))
-        f.write(np.asarray(s.row_ptr, dtype=np.int32).tobytes())
-        f.write(np.asarray(s.col_idx, dtype=np.int32).tobytes())
-        f.write(np.ascontiguousarray(s.vals, dtype=np.complex128).tobytes())
-        f.write(np.ascontiguousarray(s.b, dtype=np.complex128).tobytes())
-
-
 def read_complex_vec(path: Path) -> np.ndarray:
     raw = path.read_bytes()
     m = struct.unpack("<q", raw[:8])[0]
@@ -70,7 +59,7 @@ def run_case(name, spec, tmp: Path) -> dict:
     dims, bs, seed, solver, extra = spec
     s = systems.complex_system(dims, bs, seed)
     f = tmp / f"{name}.bspc"
-    write_complex_system(f, s)
+    systems.write_complex_bsr(f, s)
     xo = tmp / f"{name}.x"
     cmd = [str(EXE), str(f), "--B", str(bs), "--solver", solver, "--x", str(xo), *extra]
     out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout

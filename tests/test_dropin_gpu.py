@@ -12,7 +12,6 @@ the same criteria.
 """
 import os
 import subprocess
-import sys
 from pathlib import Path
 
 import numpy as np
@@ -20,8 +19,6 @@ import pytest
 
 from blocksp_b200 import systems
 
-sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
-from make_golden_complex import write_complex_system  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
@@ -31,7 +28,7 @@ EXE = ROOT / "oracle" / "_ref" / "dropin_test"
 def run(tmp_path, s, B, D, spd):
     if np.iscomplexobj(s.vals):
         f = tmp_path / "sys.bspc"
-        write_complex_system(f, s)
+        systems.write_complex_bsr(f, s)
     else:
         f = tmp_path / "sys.bsps"
         systems.write_bsr(f, s)
