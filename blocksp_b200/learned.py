@@ -296,11 +296,19 @@ def fit_relax(model: LearnedModel, seeds, dims, form: str = "lu", grid=RELAX_GRI
             table[float(r)] = table[float(r)] + it if res <= 1e-10 else None
         A.close()
         log(f"relaxation fit seed {sd}: " + " ".join(f"{r:g}:{it}" for r, it in row.items()))
-    bad = [r for r, t in table.items() if t is None]
-    ok = {r: t for r, t in table.items() if t is not None and not any(r < q <= r + margin + 1e-9 for q in bad)}
-    best = min(ok, key=lambda r: (ok[r], r)) if ok else 0.0
+    best = choose_relax(table, margin)
     model.set_relax(best)
     return best, table
+
+
+def choose_relax(table: dict, margin: float = 0.1) -> float:
+    """The fit's rule on a table {relax: total iterations, or None where some
+    system broke down or missed the tolerance}: the value with the fewest
+    iterations among those with no failing value in (relax, relax + margin];
+    ties go to the smaller value; 0 when nothing qualifies."""
+    bad = [r for r, t in table.items() if t is None]
+    ok = {r: t for r, t in table.items() if t is not None and not any(r < q <= r + margin + 1e-9 for q in bad)}
+    return min(ok, key=lambda r: (ok[r], r)) if ok else 0.0
 
 
 def train(train_seeds, val_seeds, dims=(64, 64, 64), steps_per_system: int = 4, epochs: int = 1,

@@ -175,3 +175,22 @@ def test_gradients_with_relaxation_match_finite_differences():
             an = gr[name][idx]
             worst = max(worst, abs(fd - an) / max(1e-8, abs(fd) + abs(an)))
         assert worst <= 1e-5, (form, worst)
+
+
+def test_relaxation_choice_rule():
+    # the committed L L^T fit: 0.7 has the fewest iterations but 0.8 fails
+    # within the margin, so 0.65 is chosen
+    table = {0.0: 891, 0.5: 469, 0.6: 398, 0.65: 374, 0.7: 372, 0.75: 428, 0.8: None}
+    assert learned.choose_relax(table) == 0.65
+    # without failures the minimum wins; ties go to the smaller value
+    assert learned.choose_relax({0.0: 10, 0.1: 8, 0.2: 8, 0.3: 9}) == 0.1
+    # everything failing but 0 -> 0; a fully failing table -> 0
+    assert learned.choose_relax({0.0: 5, 0.05: None, 0.1: None}) == 0.0
+    assert learned.choose_relax({0.0: None}) == 0.0
+    # the committed weights record their own fit consistently
+    import json
+    import numpy as np
+    for w in (learned.WEIGHTS, learned.WEIGHTS_LLT):
+        meta = json.loads(str(np.load(w)["meta"]))
+        tab = {float(k): v for k, v in meta["relax_fit"]["grid_total_iters"].items()}
+        assert learned.choose_relax(tab) == meta["relax"]
