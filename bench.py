@@ -184,7 +184,7 @@ def ilu_apply_bytes(n: int, bs: int, nnzb: int, val_bytes: int = 8) -> int:
 
 # --------------------------------------------------------------------- GPU arm
 
-def north_star(results: dict) -> dict | None:
+def target_comparison(results: dict) -> dict | None:
     """The target comparison: the learned (with its ILU0 fallback) mixed-precision
     solver against plain FP64 ILU0-pGMRES on the same system, wall time to the
     FP64 true residual."""
@@ -1007,7 +1007,7 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": f"synthetic (seeded {args.side}^3 7-point block stencil)",
         "config": {**config, "best_variant": r["best"]},
         "variants": r["results"],
-        "north_star": north_star(r["results"]),
+        "target_comparison": target_comparison(r["results"]),
         "parity_vs_reference": parity,
         "bsmv": {"kernel": "k_bsmv<8,double,double,1>", "ms": r["bsmv_ms"], "gbs": bsmv_gbs,
                  "frac_of_peak": bsmv_gbs / r["peak"], "algorithmic_bytes": bsmv_bytes(n, bs, nnzb)},
