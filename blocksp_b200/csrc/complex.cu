@@ -39,6 +39,7 @@ int precond_apply(bsp_precond_s* pc, int precision, const void* r, void* z);
 int precond_check_status(bsp_precond_s* pc);
 int true_residual(bsp_handle_s* h, bsp_matrix_s* A, const double* b, const double* x, double* work,
                   double* rel);
+void print_eigs(const double* wr, const double* wi, int n, bool harmonic, bool info, bool vals);
 }  // namespace bsp
 
 namespace {
@@ -314,6 +315,34 @@ int pgmres_complex_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, co
   if (o->print_iters) {
     printf("pGMRES iters %d\n", tot);
     if (tot > max_iters) printf("maximum pGMRES iterations reached\n");
+  }
+  if (o->print_eig_info && H.c > 0 && H.r == H.c + 1) {
+    // eigenvalues of the final H's square part, harmonic Ritz values after a
+    // deflated restart (blocksp_solvers.hpp:272-288; Eigenvalues_Arr, complex
+    // branch, blocksp_dense_solvers.hpp:919-965)
+    const int n = H.c;
+    CMat Hs(n, n), HsH(n, n), Z(n, n);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        Hs(i, j) = H(i, j);
+        HsH(j, i) = std::conj(H(i, j));
+      }
+    if (restarted) {
+      std::vector<Cx> e(n, Cx(0.0));
+      e[n - 1] = 1.0;
+      const std::vector<Cx> wv = lu_solve(HsH, e);
+      const Cx hmn = H(n, n - 1);
+      for (int i = 0; i < n; ++i) Hs(i, n - 1) += std::conj(hmn) * hmn * wv[i];
+    }
+    for (int i = 0; i < n; ++i) Z(i, i) = 1.0;
+    if (schur(Hs, Z)) {
+      std::vector<double> wr(n), wi(n);
+      for (int i = 0; i < n; ++i) {
+        wr[i] = Hs(i, i).real();
+        wi[i] = Hs(i, i).imag();
+      }
+      print_eigs(wr.data(), wi.data(), n, restarted, true, false);
+    }
   }
   return status;
 }

@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(32) k_ritz(const double* __restrict__ H, int l
 }
 
 // printEigInfo / printEigVals text of Eigenvalues_Arr (dense_solvers.hpp:973-990).
-static void print_eigs(const double* wr, const double* wi, int n, bool harmonic, bool info, bool vals) {
+void print_eigs(const double* wr, const double* wi, int n, bool harmonic, bool info, bool vals) {
   if (n < 1) return;
   std::vector<double> wm(n);
   for (int i = 0; i < n; ++i) wm[i] = std::sqrt(wr[i] * wr[i] + wi[i] * wi[i]);
