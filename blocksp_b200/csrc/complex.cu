@@ -320,26 +320,13 @@ int pgmres_complex_solve(bsp_handle_s* h, bsp_matrix_s* A, bsp_precond_s* pc, co
     // eigenvalues of the final H's square part, harmonic Ritz values after a
     // deflated restart (blocksp_solvers.hpp:272-288; Eigenvalues_Arr, complex
     // branch, blocksp_dense_solvers.hpp:919-965)
-    const int n = H.c;
-    CMat Hs(n, n), HsH(n, n), Z(n, n);
-    for (int i = 0; i < n; ++i)
-      for (int j = 0; j < n; ++j) {
-        Hs(i, j) = H(i, j);
-        HsH(j, i) = std::conj(H(i, j));
-      }
-    if (restarted) {
-      std::vector<Cx> e(n, Cx(0.0));
-      e[n - 1] = 1.0;
-      const std::vector<Cx> wv = lu_solve(HsH, e);
-      const Cx hmn = H(n, n - 1);
-      for (int i = 0; i < n; ++i) Hs(i, n - 1) += std::conj(hmn) * hmn * wv[i];
-    }
-    for (int i = 0; i < n; ++i) Z(i, i) = 1.0;
-    if (schur(Hs, Z)) {
+    std::vector<Cx> ev;
+    if (ritz_values(H, restarted, ev)) {
+      const int n = (int)ev.size();
       std::vector<double> wr(n), wi(n);
       for (int i = 0; i < n; ++i) {
-        wr[i] = Hs(i, i).real();
-        wi[i] = Hs(i, i).imag();
+        wr[i] = ev[i].real();
+        wi[i] = ev[i].imag();
       }
       print_eigs(wr.data(), wi.data(), n, restarted, true, false);
     }

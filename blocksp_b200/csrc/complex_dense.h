@@ -328,5 +328,32 @@ inline int deflate_complex(const CMat& H, const std::vector<Cx>& res_vec, int k,
   return 0;
 }
 
+// Ritz values of an Arnoldi H ((n+1) x n): the eigenvalues of its square part
+// H_n, or with harmonic the harmonic Ritz values, the eigenvalues of
+// H_n + |h_mn|^2 H_n^-H e_n e_n^T (Eigenvalues_Arr's complex branch,
+// blocksp_dense_solvers.hpp:919-965).  False if the Schur iteration failed.
+inline bool ritz_values(const CMat& H, bool harmonic, std::vector<Cx>& ev) {
+  const int n = H.c;
+  ev.clear();
+  if (n < 1 || H.r < n + 1) return false;
+  CMat Hs(n, n), HsH(n, n), Z(n, n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      Hs(i, j) = H(i, j);
+      HsH(j, i) = std::conj(H(i, j));
+    }
+  if (harmonic) {
+    std::vector<Cx> e(n, Cx(0.0));
+    e[n - 1] = 1.0;
+    const std::vector<Cx> w = lu_solve(HsH, e);
+    const Cx hmn = H(n, n - 1);
+    for (int i = 0; i < n; ++i) Hs(i, n - 1) += std::conj(hmn) * hmn * w[i];
+  }
+  for (int i = 0; i < n; ++i) Z(i, i) = 1.0;
+  if (!schur(Hs, Z)) return false;
+  for (int i = 0; i < n; ++i) ev.push_back(Hs(i, i));
+  return true;
+}
+
 }  // namespace cd
 }  // namespace bsp

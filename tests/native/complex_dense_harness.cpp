@@ -50,4 +50,13 @@ int cd_deflate(const double* H, int n, const double* res_vec, int k, double* Pk1
   return 0;
 }
 
+// Ritz (harmonic: harmonic Ritz) values of H ((n+1) x n); returns the count
+int cd_ritz(const double* H, int n, int harmonic, double* ev) {
+  CMat h = load(H, n + 1, n);
+  std::vector<Cx> e;
+  if (!ritz_values(h, harmonic != 0, e)) return -1;
+  std::memcpy(ev, e.data(), sizeof(double) * 2 * e.size());
+  return (int)e.size();
+}
+
 }  // extern "C"

@@ -4,6 +4,7 @@ for the host by g++).
 * complex Schur form of general and Arnoldi-like matrices: Z unitary,
   Z T Z^H = A, T upper triangular, eigenvalues equal to numpy's;
 * Householder least squares against numpy's lstsq;
+* Ritz and harmonic Ritz values of an Arnoldi H (printEigInfo) against numpy;
 * the deflated restart: the oracle's complex pGMRES run with the C++
   deflate_complex in place of its LAPACK one reproduces the reference's
   residual histories (tests/golden/c_*_dr_*.npz) within 1e-10 and its
@@ -38,6 +39,7 @@ def cd():
     lib.cd_schur.argtypes = [P, C.c_int, P, P]
     lib.cd_lstsq.argtypes = [P, C.c_int, C.c_int, P, P]
     lib.cd_deflate.argtypes = [P, C.c_int, P, C.c_int, P, P, P, C.POINTER(C.c_int)]
+    lib.cd_ritz.argtypes = [P, C.c_int, C.c_int, P]
     return lib
 
 
@@ -106,3 +108,19 @@ def test_cpp_deflate_reproduces_reference(cd, name):
     n = min(len(h), len(g))
     assert np.abs(h[:n] - g[:n]).max() <= 1e-10
     assert rel(res.x, x) <= 1e-8
+
+
+@pytest.mark.parametrize("n,harmonic", [(1, 0), (6, 0), (6, 1), (20, 1)])
+def test_complex_ritz_values(cd, n, harmonic):
+    rng = np.random.default_rng(40 + n)
+    H = np.triu(crand(rng, n + 1, n), -1) + np.vstack([2 * np.eye(n), np.zeros((1, n))])
+    H = np.ascontiguousarray(H)
+    ev = np.zeros(n, complex)
+    assert cd.cd_ritz(ptr(H), n, harmonic, ptr(ev)) == n
+    Hs = H[:n, :n].copy()
+    if harmonic:
+        e = np.zeros(n, complex)
+        e[-1] = 1.0
+        Hs[:, -1] += abs(H[n, n - 1]) ** 2 * np.linalg.solve(Hs.conj().T, e)
+    ref = np.sort_complex(np.linalg.eigvals(Hs))
+    assert np.abs(np.sort_complex(ev) - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
